@@ -1,0 +1,123 @@
+/*
+ * psr_b200 — C ABI of the B200-native screened-Poisson reconstruction library.
+ *
+ * Every entry point returns an int status (PSR_OK = 0).  Pointers named "device" are CUDA
+ * device pointers (torch tensors, Warp arrays or anything exposing
+ * __cuda_array_interface__); sizes are element counts; `stream` is a cudaStream_t (NULL =
+ * legacy default stream).  Work is stream-ordered; the only host synchronisations are the
+ * element-count reads that size data-dependent buffers, as in the reference.  A result is
+ * thread-compatible, not thread-safe.  psr_last_error() returns the calling thread's last
+ * message.
+ *
+ * Interfaces replaced (warp-psr, file:line):
+ *   psr_reconstruct       <- warp_psr.reconstruct            src/warp_psr/reconstruction.py:137-349
+ *   psr_result_info       <- Reconstruction.iso_value/.metadata reconstruction.py:119-134,303-344
+ *   psr_result_arrays     <- LevelField keys/coefficients/cumulative  src/warp_psr/field.py:122-148
+ *   psr_evaluate          <- Reconstruction.evaluate / LevelField.evaluate  field.py:150-184,395-421
+ *   psr_device_field      <- Reconstruction.device_field / _device_field  device_field.py:19-28,115-142
+ *   psr_free              <- (Python garbage collection of the Reconstruction)
+ *   psr_relax_sliced      <- relaxation.relax_sliced         src/warp_psr/relaxation.py:189-210
+ *   psr_isovalue          <- reconstruction._compute_isovalue src/warp_psr/reconstruction.py:101-116
+ */
+#ifndef PSR_B200_H
+#define PSR_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  PSR_OK = 0,
+  PSR_EINVAL = 1,      /* invalid argument (raised before any allocation, like the reference's ValueError) */
+  PSR_ECUDA = 2,       /* CUDA runtime error */
+  PSR_EDATA = 3,       /* degenerate input: nonfinite positions, zero extent, no accepted samples */
+  PSR_ETIMEOUT = 4,    /* a bounded device-side wait gave up (dependency scheduler) */
+  PSR_ENOMEM = 5
+};
+
+enum { PSR_FLOAT32 = 0, PSR_FLOAT64 = 1 };
+
+/* Solve precision.  PSR_PRECISION_INPUT follows the input dtype exactly like the reference
+ * (float32 in, float32 solve; float64 in, float64 solve).  PSR_PRECISION_MIXED keeps
+ * float32 operator storage and runs the vector arithmetic of the ordered relaxation in
+ * float64 (see DESIGN notes in the package). */
+enum { PSR_PRECISION_INPUT = 0, PSR_PRECISION_MIXED = 1 };
+
+/* reconstruct() keyword arguments (reconstruction.py:137-153); all fields required. */
+typedef struct psr_params {
+  int32_t depth, full_depth, base_depth, solve_depth, kernel_depth;
+  double samples_per_node, scale, point_weight, cg_accuracy;
+  int32_t exact_interpolation, iters, base_v_cycles;
+  int32_t precision;
+  int32_t keep_stages; /* nonzero: keep intermediate stage arrays for psr_result_stage (tests) */
+} psr_params;
+
+typedef struct psr_result psr_result;
+
+/* Summary of one reconstruction. */
+typedef struct psr_info {
+  int32_t dtype;            /* PSR_FLOAT32 / PSR_FLOAT64 of coefficients and queries */
+  int32_t depth;
+  int64_t total;            /* coefficients over all levels */
+  int64_t groups;           /* accepted leaf sample groups */
+  int64_t basis_counts[16]; /* active basis functions per depth (0 beyond depth) */
+  int64_t support_counts[16];
+  double iso_value;
+  double cube_to_model[16]; /* row-major 4x4 (transforms.py:255-280, first matrix) */
+  double model_to_cube[16]; /* row-major 4x4 (second matrix) */
+  double stage_ms[8];       /* samples, density, normal_field, tree, assembly_and_solve, field, isovalue, total */
+} psr_info;
+
+/* Device arrays owned by the result (valid until psr_free). */
+typedef struct psr_arrays {
+  const int64_t* keys;          /* d<<48 | x<<32 | y<<16 | z, sorted, all levels */
+  const void* coefficients;     /* per-level corrections, dtype */
+  const void* cumulative;       /* cumulative coefficients (field.py:187-210), dtype */
+  const int64_t* level_offsets; /* host array, depth+2 entries */
+  const int64_t* support_keys[16]; /* signed tree keys of each depth's non-ghost support (device) */
+} psr_arrays;
+
+/* Zero-copy handle mirroring warp-psr's DeviceField struct (device_field.py:19-28). */
+typedef struct psr_field_handle {
+  const int64_t* keys;
+  const void* coefficients;
+  const void* cumulative;
+  int64_t count;
+  double linear[9];         /* model -> unit cube, row-major */
+  double translation[3];
+  int32_t depth;
+  int32_t dtype;
+  double iso_value;
+} psr_field_handle;
+
+int psr_reconstruct(const void* positions, const void* normals, int64_t n, int32_t dtype, const psr_params* params,
+                    void* stream, psr_result** out);
+int psr_result_info(const psr_result* result, psr_info* info);
+int psr_result_arrays(const psr_result* result, psr_arrays* arrays);
+int psr_evaluate(const psr_result* result, const void* queries, int64_t nq, void* values, void* gradients,
+                 int32_t* valid, void* stream);
+int psr_device_field(const psr_result* result, psr_field_handle* handle);
+int psr_free(psr_result* result);
+int psr_last_error(char* buffer, size_t length);
+
+/* Ordered sliced Gauss-Seidel of one level on a caller-supplied CSR operator (device
+ * pointers; rows = basis keys of `depth`).  Result bitwise identical to the reference's
+ * sequential slice/colour order. */
+int psr_relax_sliced(int32_t dtype, const int64_t* keys, int64_t n, int32_t depth, const int32_t* offsets,
+                     const int32_t* columns, const void* values, const void* b, void* x, int32_t iters, void* stream);
+
+/* Device pointer, element count and element size of an intermediate array kept when
+ * params.keep_stages was set (names: group_keys, group_sums, group_normal_sums,
+ * group_weights, group_first, transform, depths_and_weights, normal_keys, normal_values,
+ * normal_average, normal_load_<d>, rhs_<d>, centroid_values).  *count = -1 if absent. */
+int psr_result_stage(const psr_result* result, const char* name, const void** data, int64_t* count, int32_t* elem);
+
+/* Weighted mean sum(v*w)/sum(w) with float64 accumulation, written to out[0] (dtype). */
+int psr_isovalue(int32_t dtype, const void* values, const void* weights, int64_t n, void* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,449 @@
+// C ABI of libpsr_b200 (declared in include/psr_b200.h): argument validation, stage
+// orchestration on the caller's stream, result ownership and the stage-level entry points.
+#include "../../include/psr_b200.h"
+#include "psr_internal.cuh"
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+
+using namespace psr;
+
+static thread_local std::string g_error;
+
+namespace psr {
+__global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, int64_t* keys, int32_t* vals,
+                                   uint64_t mask, int32_t value_offset) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int64_t key = src[i];
+  uint64_t h = HashView::mix(uint64_t(key)) & mask;
+  while (true) {
+    unsigned long long prev = atomicCAS(reinterpret_cast<unsigned long long*>(keys + h), ~0ULL,
+                                        static_cast<unsigned long long>(key));
+    if (prev == ~0ULL || prev == static_cast<unsigned long long>(key)) {
+      vals[h] = int32_t(i) + value_offset;
+      return;
+    }
+    h = (h + 1) & mask;
+  }
+}
+}  // namespace psr
+
+struct psr_result {
+  int dtype = 0;
+  int depth = 0;
+  Params params{};
+  int64_t groups = 0;
+  std::vector<int64_t> level_offsets;
+  std::vector<int64_t> support_count;
+  DBuf<int64_t> keys;
+  DBuf<char> coefficients, cumulative, transforms;
+  std::vector<DBuf<int64_t>> support;
+  HashMap hash;
+  double iso = 0;
+  double host_transforms[32] = {0};
+  double stage_ms[8] = {0};
+  SolveStats stats;
+  StageSink sink;
+};
+
+namespace {
+
+int fail(const Error& e) {
+  g_error = e.what();
+  return e.code;
+}
+
+void validate(const psr_params* p) {
+  if (!p) throw Error(PSR_EINVAL, "params must not be NULL");
+  // reconstruction.py:160-203
+  if (!(0 <= p->base_depth && p->base_depth <= p->full_depth && p->full_depth <= p->solve_depth &&
+        p->solve_depth <= p->depth && p->depth <= 15) ||
+      p->depth < 1 || !(0 <= p->kernel_depth && p->kernel_depth <= p->depth))
+    throw Error(PSR_EINVAL,
+                "Require 0 <= base_depth <= full_depth <= solve_depth <= depth <= 15, depth >= 1, and 0 <= "
+                "kernel_depth <= depth");
+  if (p->iters < 1 || p->base_v_cycles < 1) throw Error(PSR_EINVAL, "iters and base_v_cycles must be positive integers");
+  if (!std::isfinite(p->point_weight) || p->point_weight < 0 || !std::isfinite(p->cg_accuracy) || p->cg_accuracy <= 0)
+    throw Error(PSR_EINVAL, "Require finite nonnegative point_weight and positive cg_accuracy");
+  if (!std::isfinite(p->samples_per_node) || p->samples_per_node <= 0 || !std::isfinite(p->scale) || p->scale <= 1)
+    throw Error(PSR_EINVAL, "Require finite positive samples_per_node and scale > 1");
+  if (p->precision != PSR_PRECISION_INPUT && p->precision != PSR_PRECISION_MIXED)
+    throw Error(PSR_EINVAL, "precision must be PSR_PRECISION_INPUT or PSR_PRECISION_MIXED");
+}
+
+void tune_pool() {
+  static bool done = false;
+  if (done) return;
+  int dev = 0;
+  PSR_CUDA(cudaGetDevice(&dev));
+  cudaMemPool_t pool;
+  PSR_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t threshold = ~uint64_t(0);
+  PSR_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+  done = true;
+}
+
+__global__ void upcast_kernel(const float* in, int64_t n, double* out) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i < n) out[i] = double(in[i]);
+}
+
+
+template <class T>
+void run(const T* pos, const T* nrm, int64_t n, const Params& prm, cudaStream_t s, psr_result* R) {
+  cudaEvent_t ev[8];
+  for (auto& e : ev) PSR_CUDA(cudaEventCreate(&e));
+  PSR_CUDA(cudaEventRecord(ev[0], s));
+  SampleGroups<T> G = prepare_samples<T>(pos, nrm, n, prm.depth, prm.scale, s);
+  PSR_CUDA(cudaEventRecord(ev[1], s));
+  DensityData<T> D = build_density<T>(G, prm.depth, prm.kernel_depth, prm.samples_per_node, s);
+  PSR_CUDA(cudaEventRecord(ev[2], s));
+  NormalData<T> N = build_normals<T>(G, D, prm.base_depth, prm.depth, s);
+  StageSink& sink = R->sink;
+  sink.put("group_keys", G.keys.p, G.count, s);
+  sink.put("group_sums", G.sums.p, 3 * G.count, s);
+  sink.put("group_normal_sums", G.normal_sums.p, 3 * G.count, s);
+  sink.put("group_weights", G.weights.p, G.count, s);
+  sink.put("group_first", G.first.p, G.count, s);
+  sink.put("transform", G.transform.p, 5, s);
+  sink.put("depths_and_weights", D.dw.p, 2 * G.count, s);
+  sink.put("normal_keys", N.keys.p, N.count, s);
+  sink.put("normal_values", N.values.p, 4 * N.count, s);
+  sink.put("normal_average", N.average.p, 3, s);
+  PSR_CUDA(cudaEventRecord(ev[3], s));
+  TreeData tree = build_tree<T>(N, prm.depth, prm.full_depth, prm.base_depth, s);
+  PSR_CUDA(cudaEventRecord(ev[4], s));
+  // Concatenated basis keys of every level (reconstruction.py:260-267).
+  R->level_offsets.assign(prm.depth + 2, 0);
+  for (int d = 0; d <= prm.depth; ++d) R->level_offsets[d + 1] = R->level_offsets[d] + tree.basis_count[d];
+  int64_t total = R->level_offsets[prm.depth + 1];
+  R->keys.alloc(total, s);
+  for (int d = 0; d <= prm.depth; ++d)
+    if (tree.basis_count[d])
+      PSR_CUDA(cudaMemcpyAsync(R->keys.p + R->level_offsets[d], tree.basis[d].p, tree.basis_count[d] * sizeof(int64_t),
+                               cudaMemcpyDeviceToDevice, s));
+  R->hash.build(R->keys.p, total, s);
+  R->coefficients.alloc(total * int64_t(sizeof(T)), s);
+  R->coefficients.zero();
+  T* coeff = reinterpret_cast<T*>(R->coefficients.p);
+  solve_levels<T>(tree, D, N, R->level_offsets, R->keys.p, R->hash, prm, coeff, s, &R->stats, &sink);
+  PSR_CUDA(cudaEventRecord(ev[5], s));
+  R->cumulative.alloc(total * int64_t(sizeof(T)), s);
+  T* cum = reinterpret_cast<T*>(R->cumulative.p);
+  HashView hv = R->hash.view();
+  cumulative_coefficients<T>(R->keys.p, R->level_offsets, hv, coeff, cum, prm.depth, s);
+  DBuf<T> values(G.count, s);
+  evaluate_queries<T>(R->keys.p, hv, coeff, cum, nullptr, G.count, nullptr, nullptr, prm.depth, values.p, nullptr,
+                      nullptr, true, G.sums.p, G.weights.p, s);
+  PSR_CUDA(cudaEventRecord(ev[6], s));
+  sink.put("centroid_values", values.p, G.count, s);
+  DBuf<T> iso(1, s);
+  isovalue<T>(values.p, G.weights.p, G.count, iso.p, s);
+  R->transforms.alloc(32 * int64_t(sizeof(T)), s);
+  evaluation_transforms<T>(G.transform.p, reinterpret_cast<T*>(R->transforms.p), s);
+  PSR_CUDA(cudaEventRecord(ev[7], s));
+  T host_iso;
+  T host_tr[32];
+  PSR_CUDA(cudaMemcpyAsync(&host_iso, iso.p, sizeof(T), cudaMemcpyDeviceToHost, s));
+  PSR_CUDA(cudaMemcpyAsync(host_tr, R->transforms.p, 32 * sizeof(T), cudaMemcpyDeviceToHost, s));
+  PSR_CUDA(cudaStreamSynchronize(s));
+  R->iso = double(host_iso);
+  for (int i = 0; i < 32; ++i) R->host_transforms[i] = double(host_tr[i]);
+  for (int i = 0; i < 7; ++i) {
+    float ms = 0;
+    PSR_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+    R->stage_ms[i] = ms;
+  }
+  float all = 0;
+  PSR_CUDA(cudaEventElapsedTime(&all, ev[0], ev[7]));
+  R->stage_ms[7] = all;
+  for (auto& e : ev) cudaEventDestroy(e);
+  R->groups = G.count;
+  R->support_count = tree.support_count;
+  R->support = std::move(tree.support);
+}
+
+}  // namespace
+
+extern "C" {
+
+int psr_reconstruct(const void* positions, const void* normals, int64_t n, int32_t dtype, const psr_params* params,
+                    void* stream, psr_result** out) {
+  try {
+    if (!out) throw Error(PSR_EINVAL, "out must not be NULL");
+    *out = nullptr;
+    validate(params);
+    if (dtype != PSR_FLOAT32 && dtype != PSR_FLOAT64)
+      throw Error(PSR_EINVAL, "Reconstruction requires matching float32/float64 3D vectors on the same CUDA device");
+    if (!positions || !normals || n <= 0) throw Error(PSR_EINVAL, "points and normals must have equal nonempty 1D shapes");
+    if (n > int64_t(INT32_MAX) / 54) throw Error(PSR_EINVAL, "too many points for 32-bit record indices");
+    cudaStream_t s = (cudaStream_t)stream;
+    tune_pool();
+    Params prm{params->depth, params->full_depth, params->base_depth, params->solve_depth, params->kernel_depth,
+               params->samples_per_node, params->scale, params->point_weight, params->cg_accuracy,
+               params->exact_interpolation, params->iters, params->base_v_cycles, params->precision};
+    std::unique_ptr<psr_result> R(new psr_result());
+    R->sink.on = params->keep_stages != 0;
+    R->depth = prm.depth;
+    R->params = prm;
+    if (prm.precision == PSR_PRECISION_MIXED || dtype == PSR_FLOAT64) {
+      R->dtype = PSR_FLOAT64;
+      if (dtype == PSR_FLOAT32) {
+        DBuf<double> p64(3 * n, s), n64(3 * n, s);
+        upcast_kernel<<<blocks_for(3 * n), kThreads, 0, s>>>((const float*)positions, 3 * n, p64.p);
+        upcast_kernel<<<blocks_for(3 * n), kThreads, 0, s>>>((const float*)normals, 3 * n, n64.p);
+        PSR_LAUNCH_CHECK();
+        run<double>(p64.p, n64.p, n, prm, s, R.get());
+      } else {
+        run<double>((const double*)positions, (const double*)normals, n, prm, s, R.get());
+      }
+    } else {
+      R->dtype = PSR_FLOAT32;
+      run<float>((const float*)positions, (const float*)normals, n, prm, s, R.get());
+    }
+    *out = R.release();
+    return PSR_OK;
+  } catch (const Error& e) {
+    return fail(e);
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return PSR_ECUDA;
+  }
+}
+
+int psr_result_info(const psr_result* R, psr_info* info) {
+  if (!R || !info) {
+    g_error = "NULL argument";
+    return PSR_EINVAL;
+  }
+  std::memset(info, 0, sizeof(*info));
+  info->dtype = R->dtype;
+  info->depth = R->depth;
+  info->total = R->level_offsets.back();
+  info->groups = R->groups;
+  for (int d = 0; d <= R->depth && d < 16; ++d) {
+    info->basis_counts[d] = R->level_offsets[d + 1] - R->level_offsets[d];
+    info->support_counts[d] = R->support_count[d];
+  }
+  info->iso_value = R->iso;
+  for (int i = 0; i < 16; ++i) {
+    info->cube_to_model[i] = R->host_transforms[i];
+    info->model_to_cube[i] = R->host_transforms[16 + i];
+  }
+  for (int i = 0; i < 8; ++i) info->stage_ms[i] = R->stage_ms[i];
+  return PSR_OK;
+}
+
+int psr_result_arrays(const psr_result* R, psr_arrays* a) {
+  if (!R || !a) {
+    g_error = "NULL argument";
+    return PSR_EINVAL;
+  }
+  std::memset(a, 0, sizeof(*a));
+  a->keys = R->keys.p;
+  a->coefficients = R->coefficients.p;
+  a->cumulative = R->cumulative.p;
+  a->level_offsets = R->level_offsets.data();
+  for (int d = 0; d <= R->depth && d < 16; ++d) a->support_keys[d] = R->support[d].p;
+  return PSR_OK;
+}
+
+int psr_evaluate(const psr_result* R, const void* queries, int64_t nq, void* values, void* gradients, int32_t* valid,
+                 void* stream) {
+  try {
+    if (!R) throw Error(PSR_EINVAL, "result must not be NULL");
+    if (nq < 0 || (nq > 0 && (!queries || !values))) throw Error(PSR_EINVAL, "queries and values are required");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (nq == 0) return PSR_OK;
+    if (R->dtype == PSR_FLOAT64) {
+      DBuf<double> lt(12, s);
+      double h[12];
+      for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 3; ++c) h[3 * r + c] = R->host_transforms[16 + 4 * r + c];
+        h[9 + r] = R->host_transforms[16 + 4 * r + 3];
+      }
+      PSR_CUDA(cudaMemcpyAsync(lt.p, h, sizeof(h), cudaMemcpyHostToDevice, s));
+      evaluate_queries<double>(R->keys.p, R->hash.view(), (const double*)R->coefficients.p,
+                               (const double*)R->cumulative.p, (const double*)queries, nq, lt.p, lt.p + 9, R->depth,
+                               (double*)values, (double*)gradients, valid, false, nullptr, nullptr, s);
+    } else {
+      DBuf<float> lt(12, s);
+      float h[12];
+      for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 3; ++c) h[3 * r + c] = float(R->host_transforms[16 + 4 * r + c]);
+        h[9 + r] = float(R->host_transforms[16 + 4 * r + 3]);
+      }
+      PSR_CUDA(cudaMemcpyAsync(lt.p, h, sizeof(h), cudaMemcpyHostToDevice, s));
+      evaluate_queries<float>(R->keys.p, R->hash.view(), (const float*)R->coefficients.p, (const float*)R->cumulative.p,
+                              (const float*)queries, nq, lt.p, lt.p + 9, R->depth, (float*)values, (float*)gradients,
+                              valid, false, nullptr, nullptr, s);
+    }
+    PSR_CUDA(cudaStreamSynchronize(s));
+    return PSR_OK;
+  } catch (const Error& e) {
+    return fail(e);
+  }
+}
+
+int psr_device_field(const psr_result* R, psr_field_handle* h) {
+  if (!R || !h) {
+    g_error = "NULL argument";
+    return PSR_EINVAL;
+  }
+  std::memset(h, 0, sizeof(*h));
+  h->keys = R->keys.p;
+  h->coefficients = R->coefficients.p;
+  h->cumulative = R->cumulative.p;
+  h->count = R->level_offsets.back();
+  for (int r = 0; r < 3; ++r) {
+    for (int c = 0; c < 3; ++c) h->linear[3 * r + c] = R->host_transforms[16 + 4 * r + c];
+    h->translation[r] = R->host_transforms[16 + 4 * r + 3];
+  }
+  h->depth = R->depth;
+  h->dtype = R->dtype;
+  h->iso_value = R->iso;
+  return PSR_OK;
+}
+
+int psr_free(psr_result* R) {
+  if (!R) return PSR_OK;
+  cudaDeviceSynchronize();
+  delete R;
+  return PSR_OK;
+}
+
+namespace {
+__global__ void csr_to_ell_kernel(const int32_t* offsets, const int32_t* columns, const char* values, int elem,
+                                  int64_t n, int32_t* cols, char* vals, int* error) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int b = offsets[i], e = offsets[i + 1];
+  if (e - b > 27 || e < b) {
+    atomicExch(error, 1);
+    e = b;
+  }
+  for (int k = 0; k < e - b; ++k)
+    if (columns[b + k] < 0 || columns[b + k] >= n) {
+      atomicExch(error, 3);
+      e = b;
+    }
+  for (int k = 0; k < 28; ++k) {
+    bool in = k < e - b;
+    cols[i * 28 + k] = in ? columns[b + k] : -1;
+    for (int q = 0; q < elem; ++q) vals[(i * 28 + k) * elem + q] = in ? values[(int64_t(b) + k) * elem + q] : 0;
+  }
+}
+
+__global__ void sliced_group_kernel(const int64_t* keys, int64_t n, int depth, uint32_t* groups, int32_t* ids,
+                                    int* error) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int c[3];
+  key_coords(keys[i], c);
+  if (c[2] > (1 << depth) || int(keys[i] >> 48) != depth) atomicExch(error, 2);
+  groups[i] = uint32_t((c[0] & 1) + 2 * (c[1] & 1) + 4 * min(c[2], 1 << depth));
+  ids[i] = int32_t(i);
+}
+
+__global__ void offsets_kernel(const uint32_t* sorted, int64_t n, int count, int32_t* off) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g > count) return;
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) / 2;
+    if (sorted[mid] < uint32_t(g))
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  off[g] = int32_t(lo);
+}
+}  // namespace
+
+int psr_relax_sliced(int32_t dtype, const int64_t* keys, int64_t n, int32_t depth, const int32_t* offsets,
+                     const int32_t* columns, const void* values, const void* b, void* x, int32_t iters, void* stream) {
+  try {
+    if (dtype != PSR_FLOAT32 && dtype != PSR_FLOAT64) throw Error(PSR_EINVAL, "dtype must be float32 or float64");
+    if (depth < 0 || depth > 15 || iters < 0 || n < 0) throw Error(PSR_EINVAL, "invalid depth, iters or size");
+    if (n == 0 || iters == 0) return PSR_OK;
+    if (!keys || !offsets || !columns || !values || !b || !x) throw Error(PSR_EINVAL, "NULL array");
+    cudaStream_t s = (cudaStream_t)stream;
+    int elem = dtype == PSR_FLOAT64 ? 8 : 4;
+    DBuf<int32_t> cols(28 * n, s);
+    DBuf<char> vals(28 * n * elem, s);
+    DBuf<int> error(1, s);
+    error.zero();
+    csr_to_ell_kernel<<<blocks_for(n), kThreads, 0, s>>>(offsets, columns, (const char*)values, elem, n, cols.p, vals.p,
+                                                         error.p);
+    PSR_LAUNCH_CHECK();
+    int groups = 4 * ((1 << depth) + 1);
+    DBuf<uint32_t> g(n, s), sg(n, s);
+    DBuf<int32_t> ids(n, s), rows(n, s), off(groups + 1, s);
+    sliced_group_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, depth, g.p, ids.p, error.p);
+    PSR_LAUNCH_CHECK();
+    sort_pairs(g.p, sg.p, ids.p, rows.p, n, bits_for(uint64_t(groups)), s);
+    offsets_kernel<<<blocks_for(groups + 1), kThreads, 0, s>>>(sg.p, n, groups, off.p);
+    PSR_LAUNCH_CHECK();
+    int err = read_scalar(error.p, s);
+    if (err == 1) throw Error(PSR_EINVAL, "a row has more than 27 entries");
+    if (err == 2) throw Error(PSR_EINVAL, "keys must be basis keys of `depth`");
+    if (err == 3) throw Error(PSR_EINVAL, "column index out of range");
+    if (dtype == PSR_FLOAT64)
+      relax_sliced_ell<double, double>(cols.p, (const double*)vals.p, (const double*)b, (double*)x, rows.p, off.p,
+                                       depth, iters, s, nullptr);
+    else
+      relax_sliced_ell<float, float>(cols.p, (const float*)vals.p, (const float*)b, (float*)x, rows.p, off.p, depth,
+                                     iters, s, nullptr);
+    PSR_CUDA(cudaStreamSynchronize(s));
+    return PSR_OK;
+  } catch (const Error& e) {
+    return fail(e);
+  }
+}
+
+int psr_isovalue(int32_t dtype, const void* values, const void* weights, int64_t n, void* out, void* stream) {
+  try {
+    if (dtype != PSR_FLOAT32 && dtype != PSR_FLOAT64) throw Error(PSR_EINVAL, "dtype must be float32 or float64");
+    if (n <= 0 || !values || !weights || !out) throw Error(PSR_EINVAL, "nonempty values and weights are required");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == PSR_FLOAT64)
+      isovalue<double>((const double*)values, (const double*)weights, n, (double*)out, s);
+    else
+      isovalue<float>((const float*)values, (const float*)weights, n, (float*)out, s);
+    PSR_CUDA(cudaStreamSynchronize(s));
+    return PSR_OK;
+  } catch (const Error& e) {
+    return fail(e);
+  }
+}
+
+int psr_result_stage(const psr_result* R, const char* name, const void** data, int64_t* count, int32_t* elem) {
+  if (!R || !name || !data || !count || !elem) {
+    g_error = "NULL argument";
+    return PSR_EINVAL;
+  }
+  auto it = R->sink.entries.find(name);
+  if (it == R->sink.entries.end()) {
+    *data = nullptr;
+    *count = -1;
+    *elem = 0;
+    return PSR_OK;
+  }
+  *data = it->second.data.p;
+  *count = it->second.count;
+  *elem = it->second.elem;
+  return PSR_OK;
+}
+
+int psr_last_error(char* buffer, size_t length) {
+  if (!buffer || !length) return PSR_EINVAL;
+  std::strncpy(buffer, g_error.c_str(), length - 1);
+  buffer[length - 1] = 0;
+  return PSR_OK;
+}
+
+}  // extern "C"

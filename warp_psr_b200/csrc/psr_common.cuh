@@ -1,0 +1,237 @@
+// Shared device/host helpers of the B200 screened-Poisson library: error handling,
+// stream-ordered buffers, key packing, GPU hash maps (the replacement of warp-psr's
+// binary-search `find_key`, field.py:19-32) and thin CUB wrappers for radix sort / scan.
+#pragma once
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace psr {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define PSR_CUDA(call)                                                                              \
+  do {                                                                                              \
+    cudaError_t e_ = (call);                                                                        \
+    if (e_ != cudaSuccess)                                                                          \
+      throw ::psr::Error(2, std::string(#call) + ": " + cudaGetErrorString(e_) + " (" + __FILE__ + \
+                                ":" + std::to_string(__LINE__) + ")");                              \
+  } while (0)
+
+#define PSR_LAUNCH_CHECK() PSR_CUDA(cudaGetLastError())
+
+constexpr int64_t kInvalidKey = 0x7fffffffffffffffLL;
+constexpr int kThreads = 256;
+
+inline unsigned blocks_for(int64_t n, int threads = kThreads) {
+  int64_t b = (n + threads - 1) / threads;
+  return unsigned(b < 1 ? 1 : b);
+}
+
+// ------------------------------------------------------------------ stream-ordered buffers
+struct Stream {
+  cudaStream_t s;
+};
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  int64_t n = 0;
+  cudaStream_t s = nullptr;
+  DBuf() = default;
+  DBuf(int64_t count, cudaStream_t stream) { alloc(count, stream); }
+  void alloc(int64_t count, cudaStream_t stream) {
+    release();
+    s = stream;
+    n = count;
+    if (count > 0) PSR_CUDA(cudaMallocAsync((void**)&p, size_t(count) * sizeof(T), stream));
+  }
+  void zero() {
+    if (n > 0) PSR_CUDA(cudaMemsetAsync(p, 0, size_t(n) * sizeof(T), s));
+  }
+  void release() {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+    n = 0;
+  }
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
+  DBuf& operator=(DBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      n = o.n;
+      s = o.s;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DBuf() { release(); }
+  T* get() const { return p; }
+  int64_t size() const { return n; }
+};
+
+// Reads one device scalar (a count) synchronously — the analogue of the reference's
+// small status/count reads (samples.py:254,276; keyed.py:132,174; tree.py:139).
+template <class T>
+T read_scalar(const T* dptr, cudaStream_t s) {
+  T v;
+  PSR_CUDA(cudaMemcpyAsync(&v, dptr, sizeof(T), cudaMemcpyDeviceToHost, s));
+  PSR_CUDA(cudaStreamSynchronize(s));
+  return v;
+}
+
+template <class T>
+std::vector<T> read_vector(const T* dptr, int64_t n, cudaStream_t s) {
+  std::vector<T> v(size_t(n > 0 ? n : 0));
+  if (n > 0) {
+    PSR_CUDA(cudaMemcpyAsync(v.data(), dptr, size_t(n) * sizeof(T), cudaMemcpyDeviceToHost, s));
+    PSR_CUDA(cudaStreamSynchronize(s));
+  }
+  return v;
+}
+
+// ------------------------------------------------------------------ arithmetic helpers
+// Same NaN behaviour as std::min / std::max in the oracle.
+template <class T>
+__host__ __device__ __forceinline__ T dmin(T a, T b) { return (b < a) ? b : a; }
+template <class T>
+__host__ __device__ __forceinline__ T dmax(T a, T b) { return (a < b) ? b : a; }
+
+// density.py:14-22 degree-2 B-spline values (float64).
+__device__ __forceinline__ void quadratic(double x, double b[3]) {
+  b[0] = (1.0 - x) * (1.0 - x) * 0.5;
+  b[1] = ((1.0 - x) * (x + 1.0) + x * (2.0 - x)) * 0.5;
+  b[2] = x * x * 0.5;
+}
+
+template <class T>
+__device__ __forceinline__ int ceil_cell(T p, int n) {  // max(0, int(ceil(p*n)) - 1)
+  int c = int(ceil(p * T(n))) - 1;
+  return c < 0 ? 0 : c;
+}
+
+// ------------------------------------------------------------------ keys (field.py:13-16, tree.py:16-24)
+__host__ __device__ __forceinline__ int64_t basis_key(int d, int x, int y, int z) {
+  return (int64_t(d) << 48) | (int64_t(x) << 32) | (int64_t(y) << 16) | int64_t(z);
+}
+__host__ __device__ __forceinline__ void key_coords(int64_t k, int c[3]) {
+  c[0] = int((k >> 32) & 65535);
+  c[1] = int((k >> 16) & 65535);
+  c[2] = int(k & 65535);
+}
+__host__ __device__ __forceinline__ int64_t tree_key(int x, int y, int z) {
+  return (int64_t(x + 524288) << 40) | (int64_t(y + 524288) << 20) | int64_t(z + 524288);
+}
+__host__ __device__ __forceinline__ void tree_coords(int64_t k, int c[3]) {
+  c[0] = int((k >> 40) & 1048575) - 524288;
+  c[1] = int((k >> 20) & 1048575) - 524288;
+  c[2] = int(k & 1048575) - 524288;
+}
+
+// ------------------------------------------------------------------ GPU hash map: int64 key -> int32 index
+// Open addressing with linear probing over a power-of-two table at most half full.  A
+// lookup returns exactly the index the reference's binary search over the sorted key
+// array returns (or -1), so it can replace find_key anywhere.
+struct HashView {
+  const int64_t* keys = nullptr;
+  const int32_t* vals = nullptr;
+  uint64_t mask = 0;
+  __device__ __forceinline__ int32_t find(int64_t key) const {
+    if (!keys) return -1;
+    uint64_t h = mix(uint64_t(key)) & mask;
+    while (true) {
+      int64_t k = __ldg(keys + h);
+      if (k == key) return __ldg(vals + h);
+      if (k == -1) return -1;
+      h = (h + 1) & mask;
+    }
+  }
+  __host__ __device__ static __forceinline__ uint64_t mix(uint64_t x) {
+    x ^= x >> 31;
+    x *= 0x7fb5d329728ea185ULL;
+    x ^= x >> 27;
+    x *= 0x81dadef4bc2dd44dULL;
+    x ^= x >> 33;
+    return x;
+  }
+};
+
+__global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, int64_t* keys, int32_t* vals,
+                                   uint64_t mask, int32_t value_offset);
+
+struct HashMap {
+  DBuf<int64_t> keys;
+  DBuf<int32_t> vals;
+  uint64_t mask = 0;
+  int64_t count = 0;
+  // Build from n unique keys; key i maps to value_offset + i.
+  void build(const int64_t* src, int64_t n, cudaStream_t s, int32_t value_offset = 0) {
+    count = n;
+    uint64_t cap = 16;
+    while (cap < uint64_t(2 * n + 1)) cap <<= 1;
+    mask = cap - 1;
+    keys.alloc(int64_t(cap), s);
+    vals.alloc(int64_t(cap), s);
+    PSR_CUDA(cudaMemsetAsync(keys.p, 0xff, cap * sizeof(int64_t), s));
+    if (n > 0) {
+      hash_insert_kernel<<<blocks_for(n), kThreads, 0, s>>>(src, n, keys.p, vals.p, mask, value_offset);
+      PSR_LAUNCH_CHECK();
+    }
+  }
+  HashView view() const {
+    HashView v;
+    if (count > 0) {
+      v.keys = keys.p;
+      v.vals = vals.p;
+      v.mask = mask;
+    }
+    return v;
+  }
+};
+
+// ------------------------------------------------------------------ CUB wrappers
+// Stable LSD radix sort of (key, value) pairs on key bits [0, end_bit).
+template <class K, class V>
+void sort_pairs(const K* kin, K* kout, const V* vin, V* vout, int64_t n, int end_bit, cudaStream_t s) {
+  if (n <= 0) return;
+  size_t temp = 0;
+  PSR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, kin, kout, vin, vout, n, 0, end_bit, s));
+  DBuf<char> t(int64_t(temp), s);
+  PSR_CUDA(cub::DeviceRadixSort::SortPairs(t.p, temp, kin, kout, vin, vout, n, 0, end_bit, s));
+}
+
+template <class T>
+void exclusive_sum(const T* in, T* out, int64_t n, cudaStream_t s) {
+  if (n <= 0) return;
+  size_t temp = 0;
+  PSR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, in, out, n, s));
+  DBuf<char> t(int64_t(temp), s);
+  PSR_CUDA(cub::DeviceScan::ExclusiveSum(t.p, temp, in, out, n, s));
+}
+
+template <class T>
+void inclusive_sum(const T* in, T* out, int64_t n, cudaStream_t s) {
+  if (n <= 0) return;
+  size_t temp = 0;
+  PSR_CUDA(cub::DeviceScan::InclusiveSum(nullptr, temp, in, out, n, s));
+  DBuf<char> t(int64_t(temp), s);
+  PSR_CUDA(cub::DeviceScan::InclusiveSum(t.p, temp, in, out, n, s));
+}
+
+inline int bits_for(uint64_t maxval) {
+  int b = 1;
+  while (b < 64 && (maxval >> b)) ++b;
+  return b;
+}
+
+}  // namespace psr

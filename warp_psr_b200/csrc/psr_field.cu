@@ -1,0 +1,271 @@
+// A11/A12: cumulative coefficients, field evaluation, isovalue and evaluation transforms
+// (warp-psr field.py:187-421, reconstruction.py:18-116, transforms.py:211-280).
+#include "psr_internal.cuh"
+
+namespace psr {
+
+// field.py:187-203 — cumulative[i] = sum_h cumulative[parent]*h + coefficients[i], one depth per launch.
+template <class T>
+__global__ void cumulative_kernel(const int64_t* keys, int64_t begin, int64_t end, int d, HashView h, const T* coeff,
+                                  T* cum) {
+  int64_t i = begin + blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= end) return;
+  int c[3];
+  key_coords(keys[i], c);
+  T value = T(0);
+  for (int corner = 0; corner < 8; ++corner) {
+    int p[3] = {c[0] / 2 + corner / 4, c[1] / 2 + (corner / 2) % 2, c[2] / 2 + corner % 2};
+    T hw = (T(1) - fabs(T(c[0]) * T(.5) - T(p[0]))) * (T(1) - fabs(T(c[1]) * T(.5) - T(p[1]))) *
+           (T(1) - fabs(T(c[2]) * T(.5) - T(p[2])));
+    if (hw > T(0)) {
+      int32_t idx = h.find(basis_key(d - 1, p[0], p[1], p[2]));
+      if (idx >= 0) value = value + cum[idx] * hw;
+    }
+  }
+  cum[i] = value + coeff[i];
+}
+
+template <class T>
+void cumulative_coefficients(const int64_t* keys, const std::vector<int64_t>& offsets, const HashView& h,
+                             const T* coeff, T* cumulative, int depth, cudaStream_t s) {
+  int64_t total = offsets[depth + 1];
+  PSR_CUDA(cudaMemcpyAsync(cumulative, coeff, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
+  for (int d = 1; d <= depth; ++d) {
+    int64_t n = offsets[d + 1] - offsets[d];
+    if (!n) continue;
+    cumulative_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(keys, offsets[d], offsets[d + 1], d, h, coeff, cumulative);
+    PSR_LAUNCH_CHECK();
+  }
+}
+
+// field.py:370-393 — one level's contribution: left-owned neighbour cell, right-owned piece.
+template <class T>
+__device__ __forceinline__ void add_level(const HashView& h, const T* coeff, const T p[3], int d, T r[4]) {
+  int n = 1 << d;
+  T t[3], f[3];
+  int cell[3], base[3];
+  for (int a = 0; a < 3; ++a) {
+    t[a] = p[a] * T(n);
+    cell[a] = min(max(int(ceil(t[a])) - 1, 0), n - 1);
+    base[a] = int(floor(t[a]));
+    f[a] = t[a] - T(base[a]);
+  }
+  for (int corner = 0; corner < 8; ++corner) {
+    int node[3] = {cell[0] + corner / 4, cell[1] + (corner / 2) % 2, cell[2] + corner % 2};
+    if (min(node[0] - base[0], min(node[1] - base[1], node[2] - base[2])) < 0) continue;
+    int32_t idx = h.find(basis_key(d, node[0], node[1], node[2]));
+    if (idx < 0) continue;
+    T hh[3], sg[3];
+    for (int a = 0; a < 3; ++a) {
+      hh[a] = T(1) - f[a];
+      sg[a] = T(-1);
+      if (node[a] > base[a]) {
+        hh[a] = f[a];
+        sg[a] = T(1);
+      }
+    }
+    T c = coeff[idx];
+    r[0] = r[0] + c * hh[0] * hh[1] * hh[2];
+    r[1] = r[1] + c * T(n) * sg[0] * hh[1] * hh[2];
+    r[2] = r[2] + c * T(n) * hh[0] * sg[1] * hh[2];
+    r[3] = r[3] + c * T(n) * hh[0] * hh[1] * sg[2];
+  }
+}
+
+// field.py:395-421 reference evaluation kernel.  In the cube frame (centroids of the
+// reconstruction's isovalue, reconstruction.py:273-280) the query is sums/weights and the
+// transform is the identity.
+template <class T>
+__global__ void evaluate_kernel(const HashView h, const T* coeff, const T* cumulative, const T* queries, int64_t nq,
+                                const T* linear, const T* translation, int depth, T* values, T* gradients,
+                                int32_t* valid, int cube_frame, const T* gsums, const T* gweights) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nq) return;
+  T L[9], tr[3], q[3];
+  if (cube_frame) {
+    for (int a = 0; a < 9; ++a) L[a] = (a % 4 == 0) ? T(1) : T(0);
+    tr[0] = tr[1] = tr[2] = T(0);
+    T w = gweights[i];
+    for (int a = 0; a < 3; ++a) q[a] = gsums[3 * i + a] / w;
+  } else {
+    for (int a = 0; a < 9; ++a) L[a] = linear[a];
+    for (int a = 0; a < 3; ++a) tr[a] = translation[a];
+    for (int a = 0; a < 3; ++a) q[a] = queries[3 * i + a];
+  }
+  T p[3];
+  for (int r = 0; r < 3; ++r) p[r] = L[3 * r] * q[0] + L[3 * r + 1] * q[1] + L[3 * r + 2] * q[2] + tr[r];
+  bool ok = isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]) && dmin(p[0], dmin(p[1], p[2])) >= T(0) &&
+            dmax(p[0], dmax(p[1], p[2])) <= T(1);
+  if (valid) valid[i] = ok;
+  if (!ok) {
+    T nan = T(NAN);
+    values[i] = nan;
+    if (gradients)
+      for (int a = 0; a < 3; ++a) gradients[3 * i + a] = nan;
+    return;
+  }
+  int leaf = 0;
+  for (int d = depth; d >= 0; --d) {
+    int n = 1 << d;
+    int c[3];
+    for (int a = 0; a < 3; ++a) c[a] = min(max(int(ceil(p[a] * T(n))) - 1, 0), n - 1);
+    if (h.find(basis_key(d, c[0], c[1], c[2])) >= 0) {
+      leaf = d;
+      break;
+    }
+  }
+  for (int a = 0; a < 3; ++a) {
+    if (p[a] == T(0))
+      p[a] = T(1e-6);
+    else if (p[a] == T(1))
+      p[a] = T(1.0 - 1e-6);
+  }
+  T r[4] = {T(0), T(0), T(0), T(0)};
+  add_level(h, coeff, p, leaf, r);
+  if (leaf > 0) {
+    T s[4] = {T(0), T(0), T(0), T(0)};
+    add_level(h, cumulative, p, leaf - 1, s);
+    for (int a = 0; a < 4; ++a) r[a] = r[a] + s[a];
+  }
+  if (leaf < depth) {
+    T s[4] = {T(0), T(0), T(0), T(0)};
+    add_level(h, coeff, p, leaf + 1, s);
+    for (int a = 0; a < 4; ++a) r[a] = r[a] + s[a];
+  }
+  values[i] = r[0];
+  if (gradients)
+    for (int a = 0; a < 3; ++a) gradients[3 * i + a] = L[a] * r[1] + L[3 + a] * r[2] + L[6 + a] * r[3];
+}
+
+template <class T>
+void evaluate_queries(const int64_t* keys, const HashView& h, const T* coeff, const T* cumulative, const T* queries,
+                      int64_t nq, const T* linear, const T* translation, int depth, T* values, T* gradients,
+                      int32_t* valid, bool cube_frame, const T* group_sums, const T* group_weights, cudaStream_t s) {
+  (void)keys;
+  if (nq <= 0) return;
+  evaluate_kernel<T><<<blocks_for(nq, 128), 128, 0, s>>>(h, coeff, cumulative, queries, nq, linear, translation, depth,
+                                                         values, gradients, valid, cube_frame ? 1 : 0, group_sums,
+                                                         group_weights);
+  PSR_LAUNCH_CHECK();
+}
+
+// Weighted mean in a fixed order: 1024-value blocks, 256 lanes x 4 strided values summed
+// in float64, pairwise tree over lanes, block totals summed serially.  Products stay in
+// the input precision before the float64 accumulation (reconstruction.py:63-66).
+template <class T>
+__global__ void isovalue_blocks_kernel(const T* values, const T* weights, int64_t n, double* partial) {
+  __shared__ double tv[256], tw[256];
+  int l = threadIdx.x;
+  int64_t b = blockIdx.x * int64_t(1024);
+  double v = 0.0, w = 0.0;
+  for (int j = 0; j < 4; ++j) {
+    int64_t i = b + l + 256 * j;
+    if (i < n) {
+      v += double(values[i] * weights[i]);
+      w += double(weights[i]);
+    }
+  }
+  tv[l] = v;
+  tw[l] = w;
+  __syncthreads();
+  for (int stride = 128; stride >= 1; stride >>= 1) {
+    if (l < stride) {
+      tv[l] = tv[l] + tv[l + stride];
+      tw[l] = tw[l] + tw[l + stride];
+    }
+    __syncthreads();
+  }
+  if (l == 0) {
+    partial[2 * blockIdx.x] = tv[0];
+    partial[2 * blockIdx.x + 1] = tw[0];
+  }
+}
+
+template <class T>
+__global__ void isovalue_finish_kernel(const double* partial, int64_t blocks, T* out) {
+  if (threadIdx.x != 0) return;
+  double total = 0.0, mass = 0.0;
+  for (int64_t b = 0; b < blocks; ++b) {
+    total += partial[2 * b];
+    mass += partial[2 * b + 1];
+  }
+  out[0] = T(total / mass);
+}
+
+template <class T>
+void isovalue(const T* values, const T* weights, int64_t n, T* out, cudaStream_t s) {
+  int64_t blocks = (n + 1023) / 1024;
+  DBuf<double> partial(2 * (blocks > 0 ? blocks : 1), s);
+  if (blocks) {
+    isovalue_blocks_kernel<T><<<unsigned(blocks), 256, 0, s>>>(values, weights, n, partial.p);
+    PSR_LAUNCH_CHECK();
+  }
+  isovalue_finish_kernel<T><<<1, 32, 0, s>>>(partial.p, blocks, out);
+  PSR_LAUNCH_CHECK();
+}
+
+// transforms.py:216-280 — cofactor inverse of the cube->model matrix, applied twice.
+template <class T>
+__device__ T det3(const T m[9]) {
+  return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) + m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+template <class T>
+__device__ T minor4(const T m[16], int row, int col) {
+  T out[9];
+  int rr = 0;
+  for (int r = 0; r < 4; ++r) {
+    if (r == row) continue;
+    int cc = 0;
+    for (int c = 0; c < 4; ++c) {
+      if (c == col) continue;
+      out[rr * 3 + cc] = m[r * 4 + c];
+      ++cc;
+    }
+    ++rr;
+  }
+  return det3(out);
+}
+template <class T>
+__device__ void reference_inverse(const T m[16], T out[16]) {
+  T det = T(0);
+  for (int c = 0; c < 4; ++c) {
+    if (c % 2 == 0)
+      det = det + m[c] * minor4(m, 0, c);
+    else
+      det = det - m[c] * minor4(m, 0, c);
+  }
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) {
+      T v = minor4(m, r, c);
+      if ((r + c) % 2 != 0) v = -v;
+      out[c * 4 + r] = v / det;
+    }
+}
+
+template <class T>
+__global__ void transforms_kernel(const T* nz, T* out) {
+  if (threadIdx.x != 0) return;
+  T s = nz[0];
+  T m[16] = {T(0), s, T(0), nz[1], T(0), T(0), s, nz[2], s, T(0), T(0), nz[3], T(0), T(0), T(0), T(1)};
+  reference_inverse(m, out);
+  reference_inverse(out, out + 16);
+}
+
+template <class T>
+void evaluation_transforms(const T* normalization, T* transforms, cudaStream_t s) {
+  transforms_kernel<T><<<1, 32, 0, s>>>(normalization, transforms);
+  PSR_LAUNCH_CHECK();
+}
+
+#define INSTANTIATE(T)                                                                                               \
+  template void cumulative_coefficients<T>(const int64_t*, const std::vector<int64_t>&, const HashView&, const T*,  \
+                                           T*, int, cudaStream_t);                                                   \
+  template void evaluate_queries<T>(const int64_t*, const HashView&, const T*, const T*, const T*, int64_t,         \
+                                    const T*, const T*, int, T*, T*, int32_t*, bool, const T*, const T*,            \
+                                    cudaStream_t);                                                                   \
+  template void isovalue<T>(const T*, const T*, int64_t, T*, cudaStream_t);                                         \
+  template void evaluation_transforms<T>(const T*, T*, cudaStream_t);
+INSTANTIATE(float)
+INSTANTIATE(double)
+
+}  // namespace psr

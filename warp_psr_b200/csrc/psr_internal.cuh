@@ -1,0 +1,119 @@
+// Internal stage interfaces of the screened-Poisson pipeline.  Each stage runs on one
+// stream; data-dependent sizes are read back with read_scalar (a handful per stage).
+#pragma once
+#include "psr_common.cuh"
+
+#include <map>
+#include <string>
+
+namespace psr {
+
+struct Params {
+  int depth, full_depth, base_depth, solve_depth, kernel_depth;
+  double samples_per_node, scale, point_weight, cg_accuracy;
+  int exact, iters, base_v_cycles, precision;
+};
+
+// Optional copies of intermediate arrays, kept for stage-by-stage parity checks.
+struct StageSink {
+  struct Entry {
+    DBuf<char> data;
+    int64_t count = 0;
+    int elem = 0;
+  };
+  bool on = false;
+  std::map<std::string, Entry> entries;
+  template <class V>
+  void put(const std::string& name, const V* src, int64_t count, cudaStream_t s) {
+    if (!on) return;
+    Entry e;
+    e.count = count;
+    e.elem = int(sizeof(V));
+    e.data.alloc(count * int64_t(sizeof(V)), s);
+    if (count > 0) PSR_CUDA(cudaMemcpyAsync(e.data.p, src, count * sizeof(V), cudaMemcpyDeviceToDevice, s));
+    entries[name] = std::move(e);
+  }
+};
+
+// ---------------------------------------------------------------- A1 samples.py
+template <class T>
+struct SampleGroups {
+  int64_t count = 0;          // G accepted leaf groups
+  DBuf<int64_t> keys;         // basis keys at `depth`, sorted
+  DBuf<T> sums, normal_sums;  // 3 per group (positions / unit normals, unit-cube frame)
+  DBuf<T> weights;            // sample count per group
+  DBuf<int32_t> first;        // smallest input index of the group
+  DBuf<T> transform;          // [inv, t0, t1, t2, normal_scale]
+};
+template <class T>
+SampleGroups<T> prepare_samples(const T* pos, const T* nrm, int64_t n, int depth, double scale, cudaStream_t s);
+
+// ---------------------------------------------------------------- A2 density.py
+template <class T>
+struct DensityData {
+  std::vector<DBuf<int64_t>> agg_keys;  // per depth, sorted basis keys of occupied cells
+  std::vector<DBuf<T>> agg_values;      // 4 per record: position sum xyz, weight
+  std::vector<int64_t> agg_count;
+  DBuf<T> dw;                           // 2 per group: raw splat depth, splat weight
+  T scale;
+};
+template <class T>
+DensityData<T> build_density(const SampleGroups<T>& g, int depth, int kernel_depth, double spn, cudaStream_t s);
+template <class T>
+T density_scale();
+
+// ---------------------------------------------------------------- A3 normals.py
+template <class T>
+struct NormalData {
+  int64_t count = 0;
+  DBuf<int64_t> keys;               // sorted basis keys of every level
+  DBuf<T> values;                   // 4 per record (negated normal coefficients, 4th = -0)
+  std::vector<int64_t> offsets;     // per depth, depth+2 entries
+  DBuf<T> average;                  // [mean depth, mean weight, total weight]
+};
+template <class T>
+NormalData<T> build_normals(const SampleGroups<T>& g, const DensityData<T>& D, int minimum, int maximum,
+                            cudaStream_t s);
+
+// ---------------------------------------------------------------- A4 tree.py
+struct TreeData {
+  std::vector<DBuf<int64_t>> support;  // signed tree keys per depth (non-ghost support)
+  std::vector<DBuf<int64_t>> basis;    // basis keys per depth
+  std::vector<int64_t> support_count, basis_count;
+};
+template <class T>
+TreeData build_tree(const NormalData<T>& N, int depth, int full_depth, int base_depth, cudaStream_t s);
+
+// ---------------------------------------------------------------- A5-A10 solver.py
+struct SolveStats {
+  double relax_ms = 0;       // ordered relaxation kernels (sum over levels)
+  int64_t row_visits = 0;    // rows x sweeps relaxed by the sliced kernels
+  int64_t launches = 0;
+  std::vector<double> level_relax_ms;
+};
+template <class T>
+void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalData<T>& N,
+                  const std::vector<int64_t>& level_offsets, const int64_t* all_keys, const HashMap& all_hash,
+                  const Params& p, T* coefficients, cudaStream_t s, SolveStats* stats, StageSink* sink);
+
+// Ordered sliced relaxation on an ELL level (28 slots per row; slot k < 27 is the k-th
+// lexicographic neighbour, -1 absent).  Rows are referenced through `rows` grouped by
+// (x&1) + 2(y&1) + 4z with `group_off` (4*(2^depth+1)+1 entries).
+template <class T, class V>
+void relax_sliced_ell(const int32_t* cols, const T* vals, const V* b, V* x, const int32_t* rows,
+                      const int32_t* group_off, int depth, int iters, cudaStream_t s, float* ms);
+
+// ---------------------------------------------------------------- A11/A12 field.py, reconstruction.py
+template <class T>
+void cumulative_coefficients(const int64_t* keys, const std::vector<int64_t>& offsets, const HashView& h,
+                             const T* coeff, T* cumulative, int depth, cudaStream_t s);
+template <class T>
+void evaluate_queries(const int64_t* keys, const HashView& h, const T* coeff, const T* cumulative, const T* queries,
+                      int64_t nq, const T* linear, const T* translation, int depth, T* values, T* gradients,
+                      int32_t* valid, bool cube_frame, const T* group_sums, const T* group_weights, cudaStream_t s);
+template <class T>
+void isovalue(const T* values, const T* weights, int64_t n, T* out, cudaStream_t s);
+template <class T>
+void evaluation_transforms(const T* normalization, T* transforms /* 32 */, cudaStream_t s);
+
+}  // namespace psr

@@ -1,0 +1,611 @@
+// A1-A3: sample normalisation and grouping (warp-psr samples.py), degree-2 density and
+// splat depths (density.py), normal splat and weighted average (normals.py, keyed.py).
+//
+// Order-sensitive float sums follow the reference's record order exactly: records are
+// grouped with a stable radix sort and every segment is summed serially in record order
+// by one thread.  Keys are sorted in a compact form (coordinates packed at `depth` bits)
+// that has the same order as the reference's 64-bit keys but needs fewer radix passes.
+#include "psr_internal.cuh"
+
+#include <cmath>
+#include <limits>
+
+namespace psr {
+
+// ------------------------------------------------------------------ A1 samples.py:34-188
+template <class T>
+__global__ void bounds_partial_kernel(const T* __restrict__ pos, int64_t n, T* partial, int* status) {
+  __shared__ T lo[3][kThreads], hi[3][kThreads];
+  T l[3] = {T(INFINITY), T(INFINITY), T(INFINITY)}, h[3] = {T(-INFINITY), T(-INFINITY), T(-INFINITY)};
+  int bad = 0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    T p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    if (isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2])) {
+      for (int a = 0; a < 3; ++a) {
+        l[a] = dmin(l[a], p[a]);
+        h[a] = dmax(h[a], p[a]);
+      }
+    } else {
+      ++bad;
+    }
+  }
+  if (bad) atomicAdd(status, bad);
+  for (int a = 0; a < 3; ++a) {
+    lo[a][threadIdx.x] = l[a];
+    hi[a][threadIdx.x] = h[a];
+  }
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int a = 0; a < 3; ++a) {
+        lo[a][threadIdx.x] = dmin(lo[a][threadIdx.x], lo[a][threadIdx.x + st]);
+        hi[a][threadIdx.x] = dmax(hi[a][threadIdx.x], hi[a][threadIdx.x + st]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int a = 0; a < 3; ++a) {
+      partial[6 * blockIdx.x + a] = lo[a][0];
+      partial[6 * blockIdx.x + 3 + a] = hi[a][0];
+    }
+}
+
+// samples.py:54-88 — bounding cube, scale and the cofactor normal scale.
+template <class T>
+__global__ void transform_kernel(const T* partial, int blocks, T scale, T* transform, int* status) {
+  if (threadIdx.x != 0) return;
+  T lo[3] = {T(INFINITY), T(INFINITY), T(INFINITY)}, hi[3] = {T(-INFINITY), T(-INFINITY), T(-INFINITY)};
+  for (int b = 0; b < blocks; ++b)
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = dmin(lo[a], partial[6 * b + a]);
+      hi[a] = dmax(hi[a], partial[6 * b + 3 + a]);
+    }
+  T width = dmax(hi[0] - lo[0], dmax(hi[1] - lo[1], hi[2] - lo[2])) * scale;
+  if (!isfinite(width) || width <= T(0)) {
+    status[0] += 1;
+    return;
+  }
+  T inv = T(1.0 / double(width));
+  transform[0] = inv;
+  T determinant = inv * (inv * inv);
+  transform[4] = inv * inv / determinant * T(pow(double(determinant), 1.0 / 3.0));
+  for (int a = 0; a < 3; ++a) {
+    int axis = (a + 1) % 3;
+    T origin = (hi[axis] + lo[axis]) / T(2.0) - width / T(2.0);
+    transform[a + 1] = -origin * inv;
+  }
+}
+
+// samples.py:90-134 — cyclic axis permutation, unit normals, left-owned leaf cell.
+template <class T>
+__global__ void classify_kernel(const T* __restrict__ pos, const T* __restrict__ nrm, int64_t n,
+                                const T* __restrict__ transform, int depth, T* q, T* un, uint64_t* keys,
+                                int32_t* ids) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  T inv = transform[0], ns = transform[4];
+  const T* p = pos + 3 * i;
+  const T* m = nrm + 3 * i;
+  T qq[3] = {p[1] * inv + transform[1], p[2] * inv + transform[2], p[0] * inv + transform[3]};
+  T mm[3] = {m[1] * ns, m[2] * ns, m[0] * ns};
+  T length2 = mm[0] * mm[0] + mm[1] * mm[1] + mm[2] * mm[2];
+  for (int a = 0; a < 3; ++a) q[3 * i + a] = qq[a];
+  ids[i] = int32_t(i);
+  uint64_t key = uint64_t(1) << (3 * depth);
+  T u[3] = {T(0), T(0), T(0)};
+  if (length2 > T(0) && isfinite(length2) && dmin(qq[0], dmin(qq[1], qq[2])) >= T(0) &&
+      dmax(qq[0], dmax(qq[1], qq[2])) <= T(1)) {
+    T len = sqrt(length2);
+    for (int a = 0; a < 3; ++a) u[a] = mm[a] / len;
+    int res = 1 << depth;
+    key = (uint64_t(ceil_cell(qq[0], res)) << (2 * depth)) | (uint64_t(ceil_cell(qq[1], res)) << depth) |
+          uint64_t(ceil_cell(qq[2], res));
+  }
+  for (int a = 0; a < 3; ++a) un[3 * i + a] = u[a];
+  keys[i] = key;
+}
+
+// head[i] = 1 where a new valid segment of `keys >> shift` starts.
+__global__ void heads_kernel(const uint64_t* __restrict__ keys, int64_t n, uint64_t sentinel, int shift,
+                             int32_t* heads) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  uint64_t k = keys[i] >> shift;
+  heads[i] = (keys[i] < sentinel && (i == 0 || (keys[i - 1] >> shift) != k)) ? 1 : 0;
+}
+
+template <class T>
+__global__ void groups_kernel(const uint64_t* __restrict__ keys, const int32_t* __restrict__ order,
+                              const int32_t* __restrict__ heads, const int32_t* __restrict__ prefix, int64_t n,
+                              const T* __restrict__ q, const T* __restrict__ un, int depth, int64_t* gkeys,
+                              T* sums, T* nsums, T* weights, int32_t* first) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n || !heads[i]) return;
+  int64_t g = prefix[i] - 1;
+  uint64_t k = keys[i];
+  T p[3] = {T(0), T(0), T(0)}, m[3] = {T(0), T(0), T(0)}, w = T(0);
+  for (int64_t j = i; j < n && keys[j] == k; ++j) {
+    int64_t o = order[j];
+    for (int a = 0; a < 3; ++a) {
+      p[a] = p[a] + q[3 * o + a];
+      m[a] = m[a] + un[3 * o + a];
+    }
+    w = w + T(1.0);
+  }
+  uint64_t mask = (uint64_t(1) << depth) - 1;
+  gkeys[g] = basis_key(depth, int((k >> (2 * depth)) & mask), int((k >> depth) & mask), int(k & mask));
+  for (int a = 0; a < 3; ++a) {
+    sums[3 * g + a] = p[a];
+    nsums[3 * g + a] = m[a];
+  }
+  weights[g] = w;
+  first[g] = order[i];
+}
+
+// Marks segment heads of sorted keys and returns the number of segments.
+static int64_t segment_heads(const uint64_t* keys, int64_t n, uint64_t sentinel, int shift, DBuf<int32_t>& heads,
+                             DBuf<int32_t>& prefix, cudaStream_t s) {
+  heads.alloc(n, s);
+  prefix.alloc(n, s);
+  if (n == 0) return 0;
+  heads_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, sentinel, shift, heads.p);
+  PSR_LAUNCH_CHECK();
+  inclusive_sum(heads.p, prefix.p, n, s);
+  return read_scalar(prefix.p + n - 1, s);
+}
+
+template <class T>
+SampleGroups<T> prepare_samples(const T* pos, const T* nrm, int64_t n, int depth, double scale, cudaStream_t s) {
+  SampleGroups<T> G;
+  int blocks = int(blocks_for(n) < 592 ? blocks_for(n) : 592);
+  DBuf<T> partial(6 * blocks, s);
+  DBuf<int> status(1, s);
+  status.zero();
+  G.transform.alloc(5, s);
+  G.transform.zero();
+  bounds_partial_kernel<T><<<blocks, kThreads, 0, s>>>(pos, n, partial.p, status.p);
+  PSR_LAUNCH_CHECK();
+  transform_kernel<T><<<1, 32, 0, s>>>(partial.p, blocks, T(scale), G.transform.p, status.p);
+  PSR_LAUNCH_CHECK();
+  if (read_scalar(status.p, s)) throw Error(3, "Nonfinite positions or degenerate/overflowing bounding cube");
+  DBuf<T> q(3 * n, s), un(3 * n, s);
+  DBuf<uint64_t> keys(n, s), skeys(n, s);
+  DBuf<int32_t> ids(n, s), order(n, s);
+  classify_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(pos, nrm, n, G.transform.p, depth, q.p, un.p, keys.p, ids.p);
+  PSR_LAUNCH_CHECK();
+  sort_pairs(keys.p, skeys.p, ids.p, order.p, n, 3 * depth + 1, s);
+  DBuf<int32_t> heads, prefix;
+  uint64_t sentinel = uint64_t(1) << (3 * depth);
+  int64_t count = segment_heads(skeys.p, n, sentinel, 0, heads, prefix, s);
+  if (!count) throw Error(3, "No accepted samples with finite nonzero normals");
+  G.count = count;
+  G.keys.alloc(count, s);
+  G.sums.alloc(3 * count, s);
+  G.normal_sums.alloc(3 * count, s);
+  G.weights.alloc(count, s);
+  G.first.alloc(count, s);
+  groups_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(skeys.p, order.p, heads.p, prefix.p, n, q.p, un.p, depth,
+                                                      G.keys.p, G.sums.p, G.normal_sums.p, G.weights.p, G.first.p);
+  PSR_LAUNCH_CHECK();
+  return G;
+}
+
+// ------------------------------------------------------------------ A2 density.py:25-279
+template <class T>
+T density_scale() {  // density.py:37-50 (a constant of the precision)
+  T total = T(0);
+  T dx = T(0.1);
+  for (int x = 0; x < 10; ++x) {
+    T p = dx / T(2.0) + dx * T(x);
+    double xd = double(p);
+    double b0 = (1.0 - xd) * (1.0 - xd) * 0.5;
+    double b1 = ((1.0 - xd) * (xd + 1.0) + xd * (2.0 - xd)) * 0.5;
+    double b2 = xd * xd * 0.5;
+    T sc = T(1.0 / (b0 * b0 + b1 * b1 + b2 * b2));
+    for (int y = 0; y < 100; ++y) total = total + sc;
+  }
+  return total / T(1000.0);
+}
+
+template <class T>
+__global__ void leaf_values_kernel(const T* sums, const T* weights, int64_t n, T* out) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  for (int a = 0; a < 3; ++a) out[4 * i + a] = sums[3 * i + a];
+  out[4 * i + 3] = weights[i];
+}
+
+// Children of depth d sorted by (parent cell, morton child index): the order in which
+// density.py:228-240 (morton order, then a stable sort by parent key) sums them.
+__global__ void parent_composite_kernel(const int64_t* keys, int64_t n, int d, uint64_t* comp, int32_t* ids) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int c[3];
+  key_coords(keys[i], c);
+  int D = d - 1;
+  uint64_t parent = (uint64_t(c[0] >> 1) << (2 * D)) | (uint64_t(c[1] >> 1) << D) | uint64_t(c[2] >> 1);
+  comp[i] = (parent << 3) | uint64_t((c[0] & 1) | ((c[1] & 1) << 1) | ((c[2] & 1) << 2));
+  ids[i] = int32_t(i);
+}
+
+template <class T>
+__global__ void parent_reduce_kernel(const uint64_t* comp, const int32_t* order, const int32_t* heads,
+                                     const int32_t* prefix, int64_t n, const T* values, int d, int64_t* out_keys,
+                                     T* out_values) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n || !heads[i]) return;
+  int64_t g = prefix[i] - 1;
+  uint64_t parent = comp[i] >> 3;
+  T acc[4] = {T(0), T(0), T(0), T(0)};
+  for (int64_t j = i; j < n && (comp[j] >> 3) == parent; ++j)
+    for (int a = 0; a < 4; ++a) acc[a] = acc[a] + values[4 * int64_t(order[j]) + a];
+  int D = d - 1;
+  uint64_t mask = (uint64_t(1) << D) - 1;
+  out_keys[g] = basis_key(D, int((parent >> (2 * D)) & mask), int((parent >> D) & mask), int(parent & mask));
+  for (int a = 0; a < 4; ++a) out_values[4 * g + a] = acc[a];
+}
+
+__global__ void morton_kernel(const int64_t* keys, int64_t n, int d, uint64_t* codes, int32_t* ids) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int c[3];
+  key_coords(keys[i], c);
+  uint64_t m = 0;  // keyed.py:334-340
+  for (int bit = 0; bit < d; ++bit)
+    for (int a = 0; a < 3; ++a) m |= uint64_t((c[a] >> bit) & 1) << (3 * bit + a);
+  codes[i] = m;
+  ids[i] = int32_t(i);
+}
+
+// density.py:74-107 — 27 degree-2 splat records per occupied cell, in morton order.
+template <class T>
+__global__ void density_splat_kernel(const int64_t* keys, const T* values, const int32_t* order, int64_t m, int d,
+                                     T scale, uint64_t* rkeys, int32_t* rids, T* rvals) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= m) return;
+  int64_t j = order[i];
+  int c[3];
+  key_coords(keys[j], c);
+  const T* v = values + 4 * j;
+  int n = 1 << d;
+  T p[3] = {v[0] / v[3], v[1] / v[3], v[2] / v[3]};
+  T h = T(1.0) / T(n);
+  double b[3][3];
+  for (int a = 0; a < 3; ++a) quadratic(double((p[a] - T(c[a]) * h) / h), b[a]);
+  T weight = v[3] * scale;
+  int D = d > 0 ? d : 1;
+  uint64_t sentinel = uint64_t(1) << (3 * D);
+  for (int k = 0; k < 27; ++k) {
+    int x = k / 9, y = k / 3 % 3, z = k % 3;
+    int t[3] = {c[0] + x - 1, c[1] + y - 1, c[2] + z - 1};
+    int64_t r = 27 * i + k;
+    rids[r] = int32_t(r);
+    if (dmin(t[0], dmin(t[1], t[2])) >= 0 && dmax(t[0], dmax(t[1], t[2])) < n) {
+      rkeys[r] = (uint64_t(t[0]) << (2 * D)) | (uint64_t(t[1]) << D) | uint64_t(t[2]);
+      rvals[r] = T(double(weight) * b[0][x] * b[1][y] * b[2][z]);
+    } else {
+      rkeys[r] = sentinel;
+      rvals[r] = T(0);
+    }
+  }
+}
+
+template <class T>
+__global__ void scalar_reduce_kernel(const uint64_t* keys, const int32_t* order, const int32_t* heads,
+                                     const int32_t* prefix, int64_t n, const T* values, int d, int D,
+                                     int64_t* out_keys, T* out_values) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n || !heads[i]) return;
+  int64_t g = prefix[i] - 1;
+  uint64_t k = keys[i];
+  T acc = T(0);
+  for (int64_t j = i; j < n && keys[j] == k; ++j) acc = acc + values[order[j]];
+  uint64_t mask = (uint64_t(1) << D) - 1;
+  out_keys[g] = basis_key(d, int((k >> (2 * D)) & mask), int((k >> D) & mask), int(k & mask));
+  out_values[g] = acc;
+}
+
+// density.py:108-150 — density at every group centroid for level d.
+template <class T>
+__global__ void density_eval_kernel(HashView h, const T* lvals, const T* sums, const T* weights, int64_t G, int d,
+                                    int stride, T* dens) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= G) return;
+  T w = weights[i];
+  T p[3] = {sums[3 * i] / w, sums[3 * i + 1] / w, sums[3 * i + 2] / w};
+  int n = 1 << d;
+  int c[3] = {ceil_cell(p[0], n), ceil_cell(p[1], n), ceil_cell(p[2], n)};
+  T hh = T(1.0) / T(n);
+  double b[3][3];
+  for (int a = 0; a < 3; ++a) quadratic(double((p[a] - T(c[a]) * hh) / hh), b[a]);
+  T value = T(0);
+  for (int k = 0; k < 27; ++k) {
+    int x = k / 9, y = k / 3 % 3, z = k % 3;
+    int t[3] = {c[0] + x - 1, c[1] + y - 1, c[2] + z - 1};
+    if (dmin(t[0], dmin(t[1], t[2])) >= 0 && dmax(t[0], dmax(t[1], t[2])) < n) {
+      int32_t idx = h.find(basis_key(d, t[0], t[1], t[2]));
+      if (idx >= 0) value = value + T(b[0][x] * b[1][y] * b[2][z] * double(lvals[idx]));
+    }
+  }
+  dens[i * stride + d] = value;
+}
+
+// density.py:152-182 — raw splat depth and weight.
+template <class T>
+__global__ void depths_kernel(const T* dens, int64_t G, int kernel_depth, T target, T* dw) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= G) return;
+  int stride = kernel_depth + 1;
+  int d = kernel_depth;
+  T density = dens[i * stride + d];
+  T raw;
+  if (density >= target) {
+    raw = T(double(d) + double(T(log(double(density / target)))) / (log(2.0) * 2.0));
+  } else {
+    T fine = density;
+    while (density < target && d > 0) {
+      fine = density;
+      d -= 1;
+      density = dens[i * stride + d];
+    }
+    raw = T(T(d) + T(log(double(density / target))) / T(log(double(density / fine))));
+  }
+  T h = T(1.0) / T(1 << d);
+  dw[2 * i] = raw;
+  dw[2 * i + 1] = h * h / density;
+}
+
+template <class T>
+DensityData<T> build_density(const SampleGroups<T>& g, int depth, int kernel_depth, double spn, cudaStream_t s) {
+  DensityData<T> D;
+  int64_t G = g.count;
+  D.agg_keys.resize(depth + 1);
+  D.agg_values.resize(depth + 1);
+  D.agg_count.assign(depth + 1, 0);
+  D.agg_keys[depth].alloc(G, s);
+  PSR_CUDA(cudaMemcpyAsync(D.agg_keys[depth].p, g.keys.p, G * sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
+  D.agg_values[depth].alloc(4 * G, s);
+  D.agg_count[depth] = G;
+  leaf_values_kernel<T><<<blocks_for(G), kThreads, 0, s>>>(g.sums.p, g.weights.p, G, D.agg_values[depth].p);
+  PSR_LAUNCH_CHECK();
+  for (int d = depth; d > 0; --d) {
+    int64_t n = D.agg_count[d];
+    DBuf<uint64_t> comp(n, s), scomp(n, s);
+    DBuf<int32_t> ids(n, s), order(n, s);
+    parent_composite_kernel<<<blocks_for(n), kThreads, 0, s>>>(D.agg_keys[d].p, n, d, comp.p, ids.p);
+    PSR_LAUNCH_CHECK();
+    sort_pairs(comp.p, scomp.p, ids.p, order.p, n, 3 * d, s);
+    DBuf<int32_t> heads, prefix;
+    int64_t m = segment_heads(scomp.p, n, ~uint64_t(0), 3, heads, prefix, s);
+    D.agg_count[d - 1] = m;
+    D.agg_keys[d - 1].alloc(m, s);
+    D.agg_values[d - 1].alloc(4 * m, s);
+    parent_reduce_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(scomp.p, order.p, heads.p, prefix.p, n,
+                                                               D.agg_values[d].p, d, D.agg_keys[d - 1].p,
+                                                               D.agg_values[d - 1].p);
+    PSR_LAUNCH_CHECK();
+  }
+  D.scale = density_scale<T>();
+  DBuf<T> dens(G * (kernel_depth + 1), s);
+  for (int d = 0; d <= kernel_depth; ++d) {
+    int64_t m = D.agg_count[d];
+    DBuf<uint64_t> codes(m, s), scodes(m, s);
+    DBuf<int32_t> ids(m, s), order(m, s);
+    morton_kernel<<<blocks_for(m), kThreads, 0, s>>>(D.agg_keys[d].p, m, d, codes.p, ids.p);
+    PSR_LAUNCH_CHECK();
+    sort_pairs(codes.p, scodes.p, ids.p, order.p, m, d > 0 ? 3 * d : 1, s);
+    int64_t r = 27 * m;
+    DBuf<uint64_t> rkeys(r, s), skeys(r, s);
+    DBuf<int32_t> rids(r, s), rorder(r, s);
+    DBuf<T> rvals(r, s);
+    density_splat_kernel<T><<<blocks_for(m), kThreads, 0, s>>>(D.agg_keys[d].p, D.agg_values[d].p, order.p, m, d,
+                                                               D.scale, rkeys.p, rids.p, rvals.p);
+    PSR_LAUNCH_CHECK();
+    int Db = d > 0 ? d : 1;
+    sort_pairs(rkeys.p, skeys.p, rids.p, rorder.p, r, 3 * Db + 1, s);
+    DBuf<int32_t> heads, prefix;
+    int64_t u = segment_heads(skeys.p, r, uint64_t(1) << (3 * Db), 0, heads, prefix, s);
+    DBuf<int64_t> lkeys(u, s);
+    DBuf<T> lvals(u, s);
+    scalar_reduce_kernel<T><<<blocks_for(r), kThreads, 0, s>>>(skeys.p, rorder.p, heads.p, prefix.p, r, rvals.p, d,
+                                                               Db, lkeys.p, lvals.p);
+    PSR_LAUNCH_CHECK();
+    HashMap hm;
+    hm.build(lkeys.p, u, s);
+    density_eval_kernel<T><<<blocks_for(G), kThreads, 0, s>>>(hm.view(), lvals.p, g.sums.p, g.weights.p, G, d,
+                                                              kernel_depth + 1, dens.p);
+    PSR_LAUNCH_CHECK();
+  }
+  D.dw.alloc(2 * G, s);
+  depths_kernel<T><<<blocks_for(G), kThreads, 0, s>>>(dens.p, G, kernel_depth, T(spn), D.dw.p);
+  PSR_LAUNCH_CHECK();
+  return D;
+}
+
+// ------------------------------------------------------------------ A3 normals.py:311-524
+__global__ void first_keys_kernel(const int32_t* first, int64_t n, uint32_t* keys, int32_t* ids) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  keys[i] = uint32_t(first[i]);
+  ids[i] = int32_t(i);
+}
+
+// normals.py:325-383 — 54 records per group: two 27-node degree-2 splats on the same
+// node `top` (issue #12), weighted by dx and 1-dx.
+template <class T>
+__global__ void normal_splat_kernel(const int32_t* order, int64_t n, const T* sums, const T* nsums, const T* weights,
+                                    const T* dw, int minimum, int maximum, uint64_t* rkeys, int32_t* rids, T* rvals) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int D = maximum > 0 ? maximum : 1;
+  uint64_t sentinel = uint64_t(1) << (3 * D + 4);
+  for (int k = 0; k < 54; ++k) {
+    rkeys[54 * i + k] = sentinel;
+    rids[54 * i + k] = int32_t(54 * i + k);
+  }
+  int64_t src = order[i];
+  T w = weights[src];
+  T nm[3] = {nsums[3 * src] / w, nsums[3 * src + 1] / w, nsums[3 * src + 2] / w};
+  T length = sqrt(nm[0] * nm[0] + nm[1] * nm[1] + nm[2] * nm[2]);
+  if (!(length > T(0))) return;
+  for (int a = 0; a < 3; ++a) nm[a] = nm[a] / length * w;
+  T p[3] = {sums[3 * src] / w, sums[3 * src + 1] / w, sums[3 * src + 2] / w};
+  T depth = dmin(dmax(dw[2 * src], T(minimum)), T(maximum));
+  int top = int(ceil(depth));
+  T dx = T(1.0) - (T(top) - depth);
+  if (top <= minimum) {
+    top = minimum;
+    dx = T(1.0);
+  }
+  if (top > maximum) {
+    top = maximum;
+    dx = T(1.0);
+  }
+  int nn = 1 << top;
+  T h = T(1.0) / T(nn);
+  int c[3] = {ceil_cell(p[0], nn), ceil_cell(p[1], nn), ceil_cell(p[2], nn)};
+  double b[3][3];
+  for (int a = 0; a < 3; ++a) quadratic(double((p[a] - T(c[a]) * h) / h), b[a]);
+  bool second = fabs(1.0 - double(dx)) > 1e-06;
+  T sw = dw[2 * src + 1];
+  for (int k = 0; k < 54; ++k) {
+    if (k >= 27 && !second) break;
+    T fraction = k < 27 ? dx : T(1.0) - dx;
+    int q = k % 27;
+    int x = q / 9, y = q / 3 % 3, z = q % 3;
+    int t[3] = {c[0] + x - 1, c[1] + y - 1, c[2] + z - 1};
+    if (dmin(t[0], dmin(t[1], t[2])) >= 0 && dmax(t[0], dmax(t[1], t[2])) < nn) {
+      T bw = T(b[0][x] * b[1][y] * b[2][z]);
+      int64_t dst = 54 * i + k;
+      rkeys[dst] = (uint64_t(top) << (3 * D)) | (uint64_t(t[0]) << (2 * D)) | (uint64_t(t[1]) << D) | uint64_t(t[2]);
+      for (int a = 0; a < 3; ++a) rvals[3 * dst + a] = nm[a] * sw / (h * h * h) * fraction * bw;
+    }
+  }
+}
+
+template <class T>
+__global__ void normal_reduce_kernel(const uint64_t* keys, const int32_t* order, const int32_t* heads,
+                                     const int32_t* prefix, int64_t n, const T* values, int D, int64_t* out_keys,
+                                     T* out_values) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n || !heads[i]) return;
+  int64_t g = prefix[i] - 1;
+  uint64_t k = keys[i];
+  T acc[3] = {T(0), T(0), T(0)};
+  for (int64_t j = i; j < n && keys[j] == k; ++j) {
+    int64_t r = order[j];
+    for (int a = 0; a < 3; ++a) acc[a] = acc[a] + values[3 * r + a];
+  }
+  uint64_t mask = (uint64_t(1) << D) - 1;
+  out_keys[g] = basis_key(int(k >> (3 * D)), int((k >> (2 * D)) & mask), int((k >> D) & mask), int(k & mask));
+  for (int a = 0; a < 3; ++a) out_values[4 * g + a] = -acc[a];  // normals.py:385-388
+  out_values[4 * g + 3] = -T(0);
+}
+
+// normals.py:411-425 contributions, summed in fixed 1024-item chunks (serial inside a
+// chunk, then serially over chunk totals) — the order the oracle restates.
+template <class T>
+__global__ void average_chunks_kernel(const int32_t* order, int64_t n, const T* nsums, const T* weights, const T* dw,
+                                      T* partial) {
+  int64_t chunk = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  int64_t begin = chunk * 1024;
+  if (begin >= n) return;
+  int64_t end = begin + 1024 < n ? begin + 1024 : n;
+  T part[3] = {T(0), T(0), T(0)};
+  for (int64_t i = begin; i < end; ++i) {
+    int64_t src = order[i];
+    T w = weights[src];
+    T nm[3] = {nsums[3 * src] / w, nsums[3 * src + 1] / w, nsums[3 * src + 2] / w};
+    if (sqrt(nm[0] * nm[0] + nm[1] * nm[1] + nm[2] * nm[2]) > T(0) && w > T(0)) {
+      part[0] = part[0] + dw[2 * src] * w;
+      part[1] = part[1] + dw[2 * src + 1] * w;
+      part[2] = part[2] + w;
+    }
+  }
+  for (int a = 0; a < 3; ++a) partial[3 * chunk + a] = part[a];
+}
+
+template <class T>
+__global__ void average_finish_kernel(const T* partial, int64_t chunks, T* average) {
+  if (threadIdx.x != 0) return;
+  T total[3] = {T(0), T(0), T(0)};
+  for (int64_t c = 0; c < chunks; ++c)
+    for (int a = 0; a < 3; ++a) total[a] = total[a] + partial[3 * c + a];
+  average[0] = average[1] = average[2] = T(0);
+  if (total[2] > T(0)) {
+    average[0] = total[0] / total[2];
+    average[1] = total[1] / total[2];
+    average[2] = total[2];
+  }
+}
+
+__global__ void depth_offsets_kernel(const int64_t* keys, int64_t n, int levels, int64_t* offsets) {
+  int d = threadIdx.x;
+  if (d >= levels) return;
+  int64_t target = int64_t(d) << 48, lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) / 2;
+    if (keys[mid] < target)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  offsets[d] = lo;
+}
+
+template <class T>
+NormalData<T> build_normals(const SampleGroups<T>& g, const DensityData<T>& D, int minimum, int maximum,
+                            cudaStream_t s) {
+  NormalData<T> N;
+  int64_t n = g.count;
+  DBuf<uint32_t> fk(n, s), sfk(n, s);
+  DBuf<int32_t> ids(n, s), order(n, s);
+  first_keys_kernel<<<blocks_for(n), kThreads, 0, s>>>(g.first.p, n, fk.p, ids.p);
+  PSR_LAUNCH_CHECK();
+  sort_pairs(fk.p, sfk.p, ids.p, order.p, n, 32, s);
+  int64_t r = 54 * n;
+  int Db = maximum > 0 ? maximum : 1;
+  {
+    DBuf<uint64_t> rkeys(r, s), skeys(r, s);
+    DBuf<int32_t> rids(r, s), rorder(r, s);
+    DBuf<T> rvals(3 * r, s);
+    normal_splat_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(order.p, n, g.sums.p, g.normal_sums.p, g.weights.p,
+                                                              D.dw.p, minimum, maximum, rkeys.p, rids.p, rvals.p);
+    PSR_LAUNCH_CHECK();
+    sort_pairs(rkeys.p, skeys.p, rids.p, rorder.p, r, 3 * Db + 5, s);
+    DBuf<int32_t> heads, prefix;
+    int64_t u = segment_heads(skeys.p, r, uint64_t(1) << (3 * Db + 4), 0, heads, prefix, s);
+    N.count = u;
+    N.keys.alloc(u, s);
+    N.values.alloc(4 * u, s);
+    normal_reduce_kernel<T><<<blocks_for(r), kThreads, 0, s>>>(skeys.p, rorder.p, heads.p, prefix.p, r, rvals.p, Db,
+                                                               N.keys.p, N.values.p);
+    PSR_LAUNCH_CHECK();
+  }
+  int64_t chunks = (n + 1023) / 1024;
+  DBuf<T> partial(3 * chunks, s);
+  average_chunks_kernel<T><<<blocks_for(chunks, 128), 128, 0, s>>>(order.p, n, g.normal_sums.p, g.weights.p, D.dw.p,
+                                                                  partial.p);
+  PSR_LAUNCH_CHECK();
+  N.average.alloc(3, s);
+  average_finish_kernel<T><<<1, 32, 0, s>>>(partial.p, chunks, N.average.p);
+  PSR_LAUNCH_CHECK();
+  DBuf<int64_t> off(maximum + 2, s);
+  depth_offsets_kernel<<<1, 32, 0, s>>>(N.keys.p, N.count, maximum + 2, off.p);
+  PSR_LAUNCH_CHECK();
+  N.offsets = read_vector(off.p, maximum + 2, s);
+  return N;
+}
+
+template SampleGroups<float> prepare_samples<float>(const float*, const float*, int64_t, int, double, cudaStream_t);
+template SampleGroups<double> prepare_samples<double>(const double*, const double*, int64_t, int, double, cudaStream_t);
+template DensityData<float> build_density<float>(const SampleGroups<float>&, int, int, double, cudaStream_t);
+template DensityData<double> build_density<double>(const SampleGroups<double>&, int, int, double, cudaStream_t);
+template NormalData<float> build_normals<float>(const SampleGroups<float>&, const DensityData<float>&, int, int,
+                                                cudaStream_t);
+template NormalData<double> build_normals<double>(const SampleGroups<double>&, const DensityData<double>&, int, int,
+                                                  cudaStream_t);
+template float density_scale<float>();
+template double density_scale<double>();
+
+}  // namespace psr

@@ -1,0 +1,1124 @@
+// A5-A10: matrix-free level assembly, normal loads, ordered Gauss-Seidel, transfers and
+// the cascadic schedule (warp-psr solver.py:320-466 and the modules it calls).
+//
+// Operators are stored as 28-slot ELL rows (slot k < 27 = k-th lexicographic neighbour,
+// the reference's CSR column order; -1 = absent; slot 27 = padding for 16-byte vector
+// loads).  Stiffness values come from 1-D hat-integral tables (float64), the point
+// screening is accumulated in float64 per row exactly as screening_stencils.py:34-71, and
+// the result is rounded once to the solve precision.
+#include "psr_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace psr {
+
+constexpr int kSlots = 28;
+
+// ------------------------------------------------------------------ 1-D integral tables
+// stiffness.py:285-306 — mass (.x) and stiffness (.y) integrals of Neumann hats.
+__device__ void hat_integrals(int depth, int index, int trial_depth, int trial_index, double out[2]) {
+  int resolution = 1 << depth;
+  int ratio = 1 << (depth - trial_depth);
+  int first = max(0, max(index - 1, (trial_index - 1) * ratio));
+  int end = min(resolution, min(index + 1, (trial_index + 1) * ratio));
+  out[0] = out[1] = 0.0;
+  for (int cell = first; cell < end; ++cell) {
+    double t0 = double(cell - index);
+    double c0 = double(cell) / double(ratio) - double(trial_index);
+    double ts = cell >= index ? -1.0 : 1.0;
+    double cs = 1.0 / double(ratio);
+    if (cell >= trial_index * ratio) cs = -cs;
+    double tv = 1.0 - fabs(t0);
+    double cv = 1.0 - fabs(c0);
+    out[0] += (tv * cv + (tv * cs + ts * cv) * 0.5 + ts * cs / 3.0) / double(resolution);
+    out[1] += ts * cs * double(resolution);
+  }
+}
+
+__global__ void stiffness_table_kernel(int depth, int trial_depth, double* table) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > (1 << depth)) return;
+  for (int k = 0; k < 3; ++k) hat_integrals(depth, i, trial_depth, (i >> (depth - trial_depth)) + k - 1, table + (i * 3 + k) * 2);
+}
+
+// ordered_normal_loads.py:15-84 — Neumann hat (and derivative) against a Dirichlet B2.
+__device__ void quadratic_piece(double t0, double step, int offset, double b[3]) {
+  b[0] = b[1] = b[2] = 0.0;
+  if (offset == -1) {
+    b[0] = 0.5 * (1.0 - t0) * (1.0 - t0);
+    b[1] = -(1.0 - t0) * step;
+    b[2] = 0.5 * step * step;
+  } else if (offset == 0) {
+    b[0] = 0.5 + t0 - t0 * t0;
+    b[1] = (1.0 - 2.0 * t0) * step;
+    b[2] = -step * step;
+  } else if (offset == 1) {
+    b[0] = 0.5 * t0 * t0;
+    b[1] = t0 * step;
+    b[2] = 0.5 * step * step;
+  }
+}
+
+__device__ void normal_integral(int test_depth, int test_index, int normal_depth, int normal_index, double out[2]) {
+  int nt = 1 << test_depth, nn = 1 << normal_depth;
+  int resolution = max(nt, nn);
+  double test_step = double(nt) / double(resolution);
+  double normal_step = double(nn) / double(resolution);
+  int first = max(0, max((test_index - 1) * (resolution / nt), (normal_index - 1) * (resolution / nn)));
+  int end = min(resolution, min((test_index + 1) * (resolution / nt), (normal_index + 2) * (resolution / nn)));
+  out[0] = out[1] = 0.0;
+  for (int cell = first; cell < end; ++cell) {
+    double tx = double(cell) * test_step - double(test_index);
+    double sign = -1.0;
+    if (tx + 0.5 * test_step < 0.0) sign = 1.0;
+    double h0 = 1.0 + sign * tx;
+    double h1 = sign * test_step;
+    int normal_cell = int(floor((double(cell) + 0.5) * normal_step));
+    double t0 = double(cell) * normal_step - double(normal_cell);
+    double b[3], r[3];
+    quadratic_piece(t0, normal_step, normal_index - normal_cell, b);
+    quadratic_piece(t0, normal_step, -1 - normal_index - normal_cell, r);
+    for (int a = 0; a < 3; ++a) b[a] -= r[a];
+    quadratic_piece(t0, normal_step, 2 * nn - 1 - normal_index - normal_cell, r);
+    for (int a = 0; a < 3; ++a) b[a] -= r[a];
+    out[0] += (h0 * b[0] + (h0 * b[1] + h1 * b[0]) * 0.5 + (h0 * b[2] + h1 * b[1]) / 3.0 + h1 * b[2] * 0.25) /
+              double(resolution);
+    out[1] += (b[0] + b[1] * 0.5 + b[2] / 3.0) * sign * test_step;
+  }
+}
+
+__device__ __forceinline__ int normal_center(int index, int test_depth, int normal_depth) {
+  if (test_depth > normal_depth) return index >> 1;
+  if (test_depth < normal_depth) return index << 1;
+  return index;
+}
+
+__global__ void normal_table_kernel(int test_depth, int normal_depth, int first, int width, double* table) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > (1 << test_depth)) return;
+  for (int k = 0; k < width; ++k)
+    normal_integral(test_depth, i, normal_depth, normal_center(i, test_depth, normal_depth) + first + k,
+                    table + (i * width + k) * 2);
+}
+
+// ------------------------------------------------------------------ A6 normal loads (normal_stencils.py:210-260)
+// `nvals` are 4-wide normal coefficients indexed by (hash result - noff).
+template <class T>
+__global__ void normal_stencil_kernel(const int64_t* keys, int64_t n, int test_depth, int normal_depth, HashView nh,
+                                      int64_t noff, const T* nvals, const double* table, int width, int first,
+                                      double* out) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int c[3];
+  key_coords(keys[i], c);
+  int ctr[3] = {normal_center(c[0], test_depth, normal_depth), normal_center(c[1], test_depth, normal_depth),
+                normal_center(c[2], test_depth, normal_depth)};
+  int lim = 1 << normal_depth;
+  double value = 0.0;
+  for (int x = 0; x < width; ++x) {
+    int nx = ctr[0] + x + first;
+    if (nx < 0 || nx >= lim) continue;
+    const double* ix = table + (c[0] * width + x) * 2;
+    for (int y = 0; y < width; ++y) {
+      int ny = ctr[1] + y + first;
+      if (ny < 0 || ny >= lim) continue;
+      const double* iy = table + (c[1] * width + y) * 2;
+      for (int z = 0; z < width; ++z) {
+        int nz = ctr[2] + z + first;
+        if (nz < 0 || nz >= lim) continue;
+        int32_t j = nh.find(basis_key(normal_depth, nx, ny, nz));
+        if (j < 0) continue;
+        const double* iz = table + (c[2] * width + z) * 2;
+        const T* v = nvals + 4 * (int64_t(j) - noff);
+        value += double(v[0]) * ix[1] * iy[0] * iz[0];
+        value += double(v[1]) * ix[0] * iy[1] * iz[0];
+        value += double(v[2]) * ix[0] * iy[0] * iz[1];
+      }
+    }
+  }
+  out[i] = value;
+}
+
+// normal_loads.py:27-63 — degree-1 prolongation of normal coefficients (issue #35).
+template <class T>
+__global__ void prolong_normals_kernel(const int64_t* keys, int64_t n, int d, HashView nh, const T* nvals,
+                                       HashView bh, int64_t prev_off, const T* prev, T* out) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int c[3];
+  key_coords(keys[i], c);
+  T value[4] = {T(0), T(0), T(0), T(0)};
+  int32_t j = nh.find(keys[i]);
+  if (j >= 0)
+    for (int a = 0; a < 4; ++a) value[a] = nvals[4 * int64_t(j) + a];
+  if (d > 0) {
+    for (int corner = 0; corner < 8; ++corner) {
+      int p[3] = {c[0] / 2, c[1] / 2, c[2] / 2};
+      T weight = T(1.0);
+      for (int axis = 0; axis < 3; ++axis) {
+        if ((corner >> axis) & 1) p[axis] += 1;
+        weight = weight * (T(1.0) - fabs(T(c[axis]) * T(0.5) - T(p[axis])));
+      }
+      if (weight > T(0)) {
+        int32_t q = bh.find(basis_key(d - 1, p[0], p[1], p[2]));
+        if (q >= 0) {
+          const T* pv = prev + 4 * (int64_t(q) - prev_off);
+          for (int a = 0; a < 4; ++a) value[a] = value[a] + pv[a] * weight;
+        }
+      }
+    }
+  }
+  for (int a = 0; a < 4; ++a) out[4 * i + a] = value[a];
+}
+
+// next[i] = (P^T finer)[i] + next[i] over the 27 fine neighbours 2c+{-1,0,1}^3 (the
+// transposed trilinear prolongation, ascending fine index), with weights rounded in T.
+template <class T, class V>
+__global__ void restrict_add_kernel(const int64_t* coarse_keys, int64_t n, int d /*fine depth*/, HashView bh,
+                                    int64_t fine_off, const V* finer, V* next, bool accumulate) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int c[3];
+  key_coords(coarse_keys[i], c);
+  int lim = 1 << d;
+  V s = V(0);
+  for (int k = 0; k < 27; ++k) {
+    int f[3] = {2 * c[0] + k / 9 - 1, 2 * c[1] + (k / 3) % 3 - 1, 2 * c[2] + k % 3 - 1};
+    if (dmin(f[0], dmin(f[1], f[2])) < 0 || dmax(f[0], dmax(f[1], f[2])) > lim) continue;
+    int32_t g = bh.find(basis_key(d, f[0], f[1], f[2]));
+    if (g < 0) continue;
+    T h[3];
+    for (int a = 0; a < 3; ++a) h[a] = T(1.0) - fabs(T(f[a]) * T(0.5) - T(c[a]));
+    T w = h[0] * h[1] * h[2];
+    s = s + V(w) * finer[int64_t(g) - fine_off];
+  }
+  next[i] = accumulate ? s + next[i] : s;
+}
+
+__global__ void add3_kernel(const double* same, const double* finer, const double* parent, int64_t n, double* out) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  double v = finer[i] + same[i];
+  out[i] = parent ? parent[i] + v : v;
+}
+
+// ------------------------------------------------------------------ A5 point constraints (constraints.py:187-251)
+template <class T>
+__global__ void points_kernel(const int64_t* keys, const T* vals, int64_t m, int d, T pw, const T* average,
+                              HashView support, bool exact, T* pos, T* w, uint64_t* bin_keys, int32_t* ids) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= m) return;
+  const T* v = vals + 4 * i;
+  T p[3] = {v[0] / v[3], v[1] / v[3], v[2] / v[3]};
+  for (int a = 0; a < 3; ++a) pos[3 * i + a] = p[a];
+  int c[3];
+  key_coords(keys[i], c);
+  T wt = v[3] * T(1 << d);
+  wt = wt * (pw * average[1]);
+  if (d == 0 || support.find(tree_key(c[0], c[1], c[2])) < 0) wt = T(0);
+  w[i] = exact ? T(0) : wt;
+  int n = 1 << d, D = d > 0 ? d : 1;  // screening_stencils.py:17-26 floor bins
+  int b[3];
+  for (int a = 0; a < 3; ++a) b[a] = min(max(int(floor(p[a] * T(n))), 0), n - 1);
+  bin_keys[i] = (uint64_t(b[0]) << (2 * D)) | (uint64_t(b[1]) << D) | uint64_t(b[2]);
+  ids[i] = int32_t(i);
+}
+
+__global__ void bin_heads_kernel(const uint64_t* keys, int64_t n, int32_t* heads) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i < n) heads[i] = (i == 0 || keys[i] != keys[i - 1]);
+}
+
+__global__ void bin_fill_kernel(const uint64_t* keys, const int32_t* heads, const int32_t* prefix, int64_t n, int d,
+                                int64_t* bkeys, int32_t* bstart) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i > n) return;
+  if (i == n) {
+    if (n > 0) bstart[prefix[n - 1]] = int32_t(n);
+    return;
+  }
+  if (!heads[i]) return;
+  int D = d > 0 ? d : 1;
+  uint64_t mask = (uint64_t(1) << D) - 1, k = keys[i];
+  int64_t u = prefix[i] - 1;
+  bkeys[u] = basis_key(d, int((k >> (2 * D)) & mask), int((k >> D) & mask), int(k & mask));
+  bstart[u] = int32_t(i);
+}
+
+template <class T>
+struct PointsView {
+  const T* pos = nullptr;
+  const T* w = nullptr;
+  const int32_t* ids = nullptr;     // point ids sorted by bin (stable)
+  const int32_t* bstart = nullptr;  // per unique bin, start into ids; count+1 entries
+  HashView bins;                    // basis key of a bin cell -> unique bin index
+};
+
+template <class T>
+struct PointsData {
+  int64_t m = 0, nbins = 0;
+  DBuf<T> pos, w;
+  DBuf<int32_t> ids, bstart;
+  DBuf<int64_t> bkeys;
+  HashMap bins;
+  PointsView<T> view() const {
+    PointsView<T> v;
+    v.pos = pos.p;
+    v.w = w.p;
+    v.ids = ids.p;
+    v.bstart = bstart.p;
+    v.bins = bins.view();
+    return v;
+  }
+};
+
+template <class T>
+__device__ __forceinline__ T hat3(const T p[3], const int c[3], int depth) {  // screening_stencils.py:28-32
+  T h[3];
+  for (int a = 0; a < 3; ++a) {
+    T t = p[a] * T(1 << depth) - T(c[a]);
+    h[a] = dmax(T(1.0) - fabs(t), T(0.0));
+  }
+  return h[0] * h[1] * h[2];
+}
+
+// Float64 screening sums of one row (screening_stencils.py:34-71): acc[k] for the row's
+// present slots, and the point load.
+template <class T>
+__device__ __forceinline__ double screening_row(const PointsView<T>& P, const int c[3], int d, int trial_depth,
+                                                const int q0[3], uint32_t present, double acc[27]) {
+  double rhs = 0.0;
+  for (int k8 = 0; k8 < 8; ++k8) {
+    int cell[3] = {c[0] - k8 / 4, c[1] - (k8 / 2) % 2, c[2] - k8 % 2};
+    if (dmin(cell[0], dmin(cell[1], cell[2])) < 0 || dmax(cell[0], dmax(cell[1], cell[2])) >= (1 << d)) continue;
+    int32_t u = P.bins.find(basis_key(d, cell[0], cell[1], cell[2]));
+    if (u < 0) continue;
+    for (int32_t j = P.bstart[u]; j < P.bstart[u + 1]; ++j) {
+      int32_t index = P.ids[j];
+      T p[3] = {P.pos[3 * index], P.pos[3 * index + 1], P.pos[3 * index + 2]};
+      T weight = P.w[index];
+      if (weight == T(0)) continue;
+      T phi = hat3(p, c, d);
+      rhs += double(phi * weight);
+#pragma unroll
+      for (int k = 0; k < 27; ++k) {
+        if (!((present >> k) & 1)) continue;
+        int q[3] = {q0[0] + k / 9, q0[1] + (k / 3) % 3, q0[2] + k % 3};
+        T trial = hat3(p, q, trial_depth);
+        acc[k] += double(phi * trial * weight);
+      }
+    }
+  }
+  return rhs;
+}
+
+// ------------------------------------------------------------------ A5/A7 level assembly
+// Same-level operator rows (stiffness.py:309-380 + screening) and b = T(load) + 0.5*T(point load).
+template <class T, bool SCREEN>
+__global__ void assemble_level_kernel(const int64_t* keys, int64_t n, int d, HashView bh, int64_t off,
+                                      const double* table, PointsView<T> P, const double* load, int32_t* cols,
+                                      T* vals, T* b) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int c[3];
+  key_coords(keys[i], c);
+  int lim = 1 << d;
+  uint32_t present = 0;
+  int32_t col[27];
+  for (int k = 0; k < 27; ++k) {
+    int q[3] = {c[0] + k / 9 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k % 3 - 1};
+    int32_t idx = -1;
+    if (dmin(q[0], dmin(q[1], q[2])) >= 0 && dmax(q[0], dmax(q[1], q[2])) <= lim) {
+      int32_t g = bh.find(basis_key(d, q[0], q[1], q[2]));
+      idx = g >= 0 ? int32_t(g - off) : -1;
+    }
+    col[k] = idx;
+    if (idx >= 0) present |= 1u << k;
+  }
+  double acc[27];
+  for (int k = 0; k < 27; ++k) acc[k] = 0.0;
+  double pl = 0.0;
+  if (SCREEN) {
+    int q0[3] = {c[0] - 1, c[1] - 1, c[2] - 1};
+    pl = screening_row(P, c, d, d, q0, present, acc);
+  }
+  for (int k = 0; k < 27; ++k) {
+    T v = T(0);
+    if (col[k] >= 0) {
+      const double* x = table + (c[0] * 3 + k / 9) * 2;
+      const double* y = table + (c[1] * 3 + (k / 3) % 3) * 2;
+      const double* z = table + (c[2] * 3 + k % 3) * 2;
+      double stiff = x[1] * y[0] * z[0] + x[0] * y[1] * z[0] + x[0] * y[0] * z[1];
+      v = T(SCREEN ? stiff + acc[k] : stiff);
+    }
+    cols[i * kSlots + k] = col[k];
+    vals[i * kSlots + k] = v;
+  }
+  cols[i * kSlots + 27] = -1;
+  vals[i * kSlots + 27] = T(0);
+  b[i] = T(load[i]) + T(0.5) * T(pl);
+}
+
+// Cross operator (rows at d, trial functions at d-1; stiffness + screening, rounded to T)
+// applied to the coarser cumulative solution: b = b - C cumulative (solver.py:428-446).
+template <class T, bool SCREEN>
+__global__ void cross_apply_kernel(const int64_t* keys, int64_t n, int d, HashView bh, int64_t coff,
+                                   const double* table, PointsView<T> P, const T* cumulative, T* b) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int c[3];
+  key_coords(keys[i], c);
+  int ctr[3] = {c[0] >> 1, c[1] >> 1, c[2] >> 1};
+  int lim = 1 << (d - 1);
+  uint32_t present = 0;
+  int32_t col[27];
+  for (int k = 0; k < 27; ++k) {
+    int q[3] = {ctr[0] + k / 9 - 1, ctr[1] + (k / 3) % 3 - 1, ctr[2] + k % 3 - 1};
+    int32_t idx = -1;
+    if (dmin(q[0], dmin(q[1], q[2])) >= 0 && dmax(q[0], dmax(q[1], q[2])) <= lim) {
+      int32_t g = bh.find(basis_key(d - 1, q[0], q[1], q[2]));
+      idx = g >= 0 ? int32_t(g - coff) : -1;
+    }
+    col[k] = idx;
+    if (idx >= 0) present |= 1u << k;
+  }
+  double acc[27];
+  for (int k = 0; k < 27; ++k) acc[k] = 0.0;
+  if (SCREEN) {
+    int q0[3] = {ctr[0] - 1, ctr[1] - 1, ctr[2] - 1};
+    screening_row(P, c, d, d - 1, q0, present, acc);
+  }
+  T s = T(0);
+  for (int k = 0; k < 27; ++k) {
+    if (col[k] < 0) continue;
+    const double* x = table + (c[0] * 3 + k / 9) * 2;
+    const double* y = table + (c[1] * 3 + (k / 3) % 3) * 2;
+    const double* z = table + (c[2] * 3 + k % 3) * 2;
+    double stiff = x[1] * y[0] * z[0] + x[0] * y[1] * z[0] + x[0] * y[0] * z[1];
+    T v = T(SCREEN ? stiff + acc[k] : stiff);
+    s = s + v * cumulative[col[k]];
+  }
+  b[i] = -s + b[i];
+}
+
+// ------------------------------------------------------------------ A9 transfers (transfer_stencils.py:116-151)
+template <class T>
+__global__ void prolongation_kernel(const int64_t* fine, int64_t n, int d, HashView bh, int64_t coff, int32_t* pcol,
+                                    T* pval) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int f[3];
+  key_coords(fine[i], f);
+  int out = 0;
+  for (int k = 0; k < 8; ++k) {
+    int c[3] = {f[0] / 2 + k / 4, f[1] / 2 + (k / 2) % 2, f[2] / 2 + k % 2};
+    T h[3];
+    for (int a = 0; a < 3; ++a) h[a] = T(1.0) - fabs(T(f[a]) * T(0.5) - T(c[a]));
+    T weight = h[0] * h[1] * h[2];
+    int32_t column = -1;
+    if (weight > T(0)) {
+      int32_t g = bh.find(basis_key(d - 1, c[0], c[1], c[2]));
+      column = g >= 0 ? int32_t(g - coff) : -1;
+    }
+    if (column >= 0) {
+      pcol[i * 8 + out] = column;
+      pval[i * 8 + out] = weight;
+      ++out;
+    }
+  }
+  for (; out < 8; ++out) {
+    pcol[i * 8 + out] = -1;
+    pval[i * 8 + out] = T(0);
+  }
+}
+
+// y[i] = (P x)[i] + y[i]  (warp.sparse.bsr_mv with beta = 1)
+template <class T>
+__global__ void prolong_add_kernel(const int32_t* pcol, const T* pval, int64_t n, const T* x, T* y) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  T s = T(0);
+  for (int e = 0; e < 8; ++e) {
+    int32_t c = pcol[i * 8 + e];
+    if (c < 0) break;
+    s = s + pval[i * 8 + e] * x[c];
+  }
+  y[i] = s + y[i];
+}
+
+// ------------------------------------------------------------------ A8 ordered relaxation (relaxation.py)
+template <class V>
+__device__ __forceinline__ V ld_x(const V* x, int64_t i) { return __ldcg(x + i); }
+template <class V>
+__device__ __forceinline__ void st_x(V* x, int64_t i, V v) { __stcg(x + i, v); }
+
+// relaxation.py:51-62, one row: r = b_i - sum_k x[c_k] A_k (slot order); x_i += r / A_ii.
+template <class T, class V>
+__device__ __forceinline__ void gs_row(const int32_t* __restrict__ cols, const T* __restrict__ vals,
+                                       const V* __restrict__ b, V* x, int32_t row) {
+  const int4* cr = reinterpret_cast<const int4*>(cols + int64_t(row) * kSlots);
+  int cc[kSlots];
+#pragma unroll
+  for (int q = 0; q < kSlots / 4; ++q) {
+    int4 v = __ldg(cr + q);
+    cc[4 * q] = v.x;
+    cc[4 * q + 1] = v.y;
+    cc[4 * q + 2] = v.z;
+    cc[4 * q + 3] = v.w;
+  }
+  T aa[kSlots];
+  const T* vr = vals + int64_t(row) * kSlots;
+#pragma unroll
+  for (int q = 0; q < kSlots; ++q) aa[q] = __ldg(vr + q);
+  V xs[27];
+#pragma unroll
+  for (int k = 0; k < 27; ++k) xs[k] = cc[k] >= 0 ? ld_x(x, cc[k]) : V(0);
+  V r = b[row];
+  T diagonal = T(0);
+  V xi = V(0);
+#pragma unroll
+  for (int k = 0; k < 27; ++k) {
+    if (cc[k] < 0) continue;
+    r = r - xs[k] * V(aa[k]);
+    if (cc[k] == row) {
+      diagonal = aa[k];
+      xi = xs[k];
+    }
+  }
+  if (diagonal != T(0)) st_x(x, row, xi + r * (V(1.0) / V(diagonal)));
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Bounded wait: returns false if `*p >= v` did not happen within the iteration limit.
+__device__ __forceinline__ bool wait_geq(const int* p, int v, const int* error) {
+  for (long long it = 0; it < (1LL << 26); ++it) {
+    if (ld_acquire(p) >= v) return true;
+    if ((it & 63) == 63 && *(volatile const int*)error) return false;
+    __nanosleep(it < 256 ? 20 : 200);
+  }
+  return false;
+}
+
+// Persistent dependency-scheduled sliced Gauss-Seidel.  Tasks (slice z, visit t) are taken
+// from a counter in the reference's sequential order (relaxation.py:121-126).  Visit t of
+// slice z waits for visit t of z+1 and visit t-1 of z-1 (relaxation.py:128-135); the four
+// colours of a slice run in order inside one CTA.  Any schedule honouring these edges is
+// bitwise identical to the sequential order.  A task only waits on tasks taken earlier, so
+// the scheme cannot deadlock; every wait is bounded and reports PSR_ETIMEOUT.
+template <class T, class V>
+__global__ void __launch_bounds__(512) sliced_gs_kernel(const int32_t* __restrict__ cols, const T* __restrict__ vals,
+                                                         const V* __restrict__ b, V* x,
+                                                         const int32_t* __restrict__ rows,
+                                                         const int32_t* __restrict__ group_off,
+                                                         const int2* __restrict__ tasks, int ntasks, int nslices,
+                                                         int* progress, int* counter, int* error) {
+  __shared__ int s_task, s_fail;
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_task = atomicAdd(counter, 1);
+      s_fail = 0;
+    }
+    __syncthreads();
+    int task = s_task;
+    if (task >= ntasks) return;
+    int z = tasks[task].x, t = tasks[task].y;
+    if (threadIdx.x == 0) {
+      bool ok = true;
+      if (z + 1 < nslices) ok = ok && wait_geq(progress + z + 1, t + 1, error);
+      if (z > 0) ok = ok && wait_geq(progress + z - 1, t, error);
+      ok = ok && wait_geq(progress + z, t, error);
+      if (!ok) {
+        atomicExch(error, 1);
+        s_fail = 1;
+      }
+    }
+    __syncthreads();
+    if (s_fail) return;
+    for (int c = 0; c < 4; ++c) {
+      int g = 4 * z + c;
+      int end = group_off[g + 1];
+      for (int j = group_off[g] + threadIdx.x; j < end; j += blockDim.x) gs_row(cols, vals, b, x, rows[j]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      __threadfence();
+      st_release(progress + z, t + 1);
+    }
+  }
+}
+
+// Eight-colour relaxation of a small level by one CTA (relaxation.py:261-271).
+template <class T>
+__global__ void __launch_bounds__(512) relax_colors_kernel(const int32_t* cols, const T* vals, const T* b, T* x,
+                                                            const int32_t* rows, const int32_t* group_off, int iters,
+                                                            int forward) {
+  for (int it = 0; it < iters; ++it)
+    for (int cc = 0; cc < 8; ++cc) {
+      int g = forward ? cc : 7 - cc;
+      for (int j = group_off[g] + threadIdx.x; j < group_off[g + 1]; j += blockDim.x) gs_row(cols, vals, b, x, rows[j]);
+      __syncthreads();
+    }
+}
+
+// r = rhs - A x  (bsr_mv alpha=-1, beta=1)
+template <class T>
+__global__ void residual_kernel(const int32_t* cols, const T* vals, const T* rhs, const T* x, int64_t n, T* r) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  T s = T(0);
+  for (int k = 0; k < 27; ++k) {
+    int32_t c = cols[i * kSlots + k];
+    if (c < 0) continue;
+    s = s + vals[i * kSlots + k] * x[c];
+  }
+  r[i] = -s + rhs[i];
+}
+
+// ------------------------------------------------------------------ schedules
+__global__ void group_kernel(const int64_t* keys, int64_t n, int sliced, uint32_t* groups, int32_t* ids) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int c[3];
+  key_coords(keys[i], c);
+  groups[i] = uint32_t(sliced ? (c[0] & 1) + 2 * (c[1] & 1) + 4 * c[2] : (c[0] & 1) + 2 * (c[1] & 1) + 4 * (c[2] & 1));
+  ids[i] = int32_t(i);
+}
+
+__global__ void group_offsets_kernel(const uint32_t* sorted, int64_t n, int count, int32_t* off) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g > count) return;
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) / 2;
+    if (sorted[mid] < uint32_t(g))
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  off[g] = int32_t(lo);
+}
+
+struct Schedule {
+  DBuf<int32_t> rows, off;
+  int groups = 0;
+};
+
+static Schedule make_schedule(const int64_t* keys, int64_t n, int depth, bool sliced, cudaStream_t s) {
+  Schedule S;
+  S.groups = sliced ? 4 * ((1 << depth) + 1) : 8;
+  DBuf<uint32_t> g(n, s), sg(n, s);
+  DBuf<int32_t> ids(n, s);
+  S.rows.alloc(n, s);
+  S.off.alloc(S.groups + 1, s);
+  if (n > 0) {
+    group_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, sliced, g.p, ids.p);
+    PSR_LAUNCH_CHECK();
+    sort_pairs(g.p, sg.p, ids.p, S.rows.p, n, bits_for(uint64_t(S.groups)), s);
+  }
+  group_offsets_kernel<<<blocks_for(S.groups + 1), kThreads, 0, s>>>(sg.p, n, S.groups, S.off.p);
+  PSR_LAUNCH_CHECK();
+  return S;
+}
+
+static int sm_count() {
+  static int count = 0;
+  if (!count) {
+    int dev = 0;
+    PSR_CUDA(cudaGetDevice(&dev));
+    PSR_CUDA(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev));
+  }
+  return count;
+}
+
+template <class T, class V>
+void relax_sliced_ell(const int32_t* cols, const T* vals, const V* b, V* x, const int32_t* rows,
+                      const int32_t* group_off, int depth, int iters, cudaStream_t s, float* ms) {
+  if (iters <= 0) return;
+  int n = 1 << depth;
+  std::vector<int2> tasks;
+  for (int front = n; front > -iters; --front)
+    for (int z = std::max(front, 0); z < std::min(front + iters, n + 1); ++z) tasks.push_back(make_int2(z, z - front));
+  int ntasks = int(tasks.size());
+  DBuf<int2> dtasks(ntasks, s);
+  PSR_CUDA(cudaMemcpyAsync(dtasks.p, tasks.data(), ntasks * sizeof(int2), cudaMemcpyHostToDevice, s));
+  DBuf<int> flags(n + 1 + 2, s);
+  flags.zero();
+  int* progress = flags.p;
+  int* counter = flags.p + n + 1;
+  int* error = flags.p + n + 2;
+  int grid = std::min(ntasks, 2 * sm_count());
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ms) {
+    PSR_CUDA(cudaEventCreate(&e0));
+    PSR_CUDA(cudaEventCreate(&e1));
+    PSR_CUDA(cudaEventRecord(e0, s));
+  }
+  sliced_gs_kernel<T, V><<<grid, 512, 0, s>>>(cols, vals, b, x, rows, group_off, dtasks.p, ntasks, n + 1, progress,
+                                              counter, error);
+  PSR_LAUNCH_CHECK();
+  if (ms) {
+    PSR_CUDA(cudaEventRecord(e1, s));
+  }
+  int err = read_scalar(error, s);
+  if (ms) {
+    PSR_CUDA(cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  if (err) throw Error(4, "ordered relaxation: a dependency wait timed out");
+}
+
+// ------------------------------------------------------------------ A10 base solve (solver.py:241-317)
+// Galerkin R A P on a complete regular level (all nodes of [0, 2^d]^3 present): one thread
+// per coarse row, products summed in the fixed order of the oracle's sparse product.
+template <class T>
+__global__ void galerkin_kernel(const int64_t* coarse_keys, int64_t nc, int d /*fine*/, HashView bh, int64_t foff,
+                                int64_t coff, const int32_t* fcols, const T* fvals, int32_t* ccols, T* cvals) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nc) return;
+  int c[3];
+  key_coords(coarse_keys[i], c);
+  int lim = 1 << d;
+  T acc[125];
+  uint64_t touched[2] = {0, 0};
+  for (int o = 0; o < 125; ++o) acc[o] = T(0);
+  for (int k = 0; k < 27; ++k) {  // rows of R = columns of P: fine nodes 2c + {-1,0,1}^3
+    int f[3] = {2 * c[0] + k / 9 - 1, 2 * c[1] + (k / 3) % 3 - 1, 2 * c[2] + k % 3 - 1};
+    if (dmin(f[0], dmin(f[1], f[2])) < 0 || dmax(f[0], dmax(f[1], f[2])) > lim) continue;
+    int32_t g = bh.find(basis_key(d, f[0], f[1], f[2]));
+    if (g < 0) continue;
+    int64_t fr = int64_t(g) - foff;
+    T h[3];
+    for (int a = 0; a < 3; ++a) h[a] = T(1.0) - fabs(T(f[a]) * T(0.5) - T(c[a]));
+    T r = h[0] * h[1] * h[2];
+    for (int e = 0; e < 27; ++e) {
+      if (fcols[fr * kSlots + e] < 0) continue;
+      int j[3] = {f[0] + e / 9 - 1, f[1] + (e / 3) % 3 - 1, f[2] + e % 3 - 1};
+      int o = (j[0] - 2 * c[0] + 2) * 25 + (j[1] - 2 * c[1] + 2) * 5 + (j[2] - 2 * c[2] + 2);
+      acc[o] = acc[o] + r * fvals[fr * kSlots + e];
+      touched[o >> 6] |= uint64_t(1) << (o & 63);
+    }
+  }
+  T cacc[27];
+  uint32_t ctouched = 0;
+  for (int k = 0; k < 27; ++k) cacc[k] = T(0);
+  for (int o = 0; o < 125; ++o) {
+    if (!((touched[o >> 6] >> (o & 63)) & 1)) continue;
+    int j[3] = {2 * c[0] - 2 + o / 25, 2 * c[1] - 2 + (o / 5) % 5, 2 * c[2] - 2 + o % 5};
+    for (int k = 0; k < 8; ++k) {
+      int jj[3] = {j[0] / 2 + k / 4, j[1] / 2 + (k / 2) % 2, j[2] / 2 + k % 2};
+      T h[3];
+      for (int a = 0; a < 3; ++a) h[a] = T(1.0) - fabs(T(j[a]) * T(0.5) - T(jj[a]));
+      T w = h[0] * h[1] * h[2];
+      if (!(w > T(0))) continue;
+      if (dmax(jj[0], dmax(jj[1], jj[2])) > (lim >> 1)) continue;
+      int s = (jj[0] - c[0] + 1) * 9 + (jj[1] - c[1] + 1) * 3 + (jj[2] - c[2] + 1);
+      cacc[s] = cacc[s] + acc[o] * w;
+      ctouched |= 1u << s;
+    }
+  }
+  for (int k = 0; k < 27; ++k) {
+    int32_t col = -1;
+    if ((ctouched >> k) & 1) {
+      int q[3] = {c[0] + k / 9 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k % 3 - 1};
+      int32_t g = bh.find(basis_key(d - 1, q[0], q[1], q[2]));
+      col = g >= 0 ? int32_t(g - coff) : -1;
+    }
+    ccols[i * kSlots + k] = col;
+    cvals[i * kSlots + k] = col >= 0 ? cacc[k] : T(0);
+  }
+  ccols[i * kSlots + 27] = -1;
+  cvals[i * kSlots + 27] = T(0);
+}
+
+__device__ __forceinline__ int root_row(int64_t key) {  // solver.py:30-33
+  int c[3];
+  key_coords(key, c);
+  for (int a = 0; a < 3; ++a) c[a] += 2;
+  return c[2] * 16 + (c[0] & 1) + 2 * (c[1] & 1) + 2 * (c[0] & 2) + 4 * (c[1] & 2);
+}
+
+// Root conjugate gradients (warp.optim.linear.cg stopping rule) on the 8-row depth-0
+// system, or on the 64-row padded system with the constant-mode term (solver.py:167-202).
+// One thread; dot products sequential in T.
+template <class T>
+__global__ void root_solve_kernel(const int64_t* keys, int nk, const int32_t* cols, const T* vals, const T* rhs, T* x,
+                                  T* root_state, int dc, double cg_accuracy, int base, int cycle) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int N = dc ? 64 : nk;
+  T K[64][64];
+  unsigned char has[64][64];
+  T bb[64], xx[64], r[64], p[64], Ap[64];
+  for (int a = 0; a < N; ++a) {
+    bb[a] = T(0);
+    xx[a] = T(0);
+    for (int q = 0; q < N; ++q) {
+      K[a][q] = T(0);
+      has[a][q] = 0;
+    }
+  }
+  if (dc)
+    for (int a = 0; a < N; ++a) xx[a] = root_state[a];
+  for (int i = 0; i < nk; ++i) {
+    int ri = dc ? root_row(keys[i]) : i;
+    bb[ri] = rhs[i];
+    if (!dc) xx[ri] = x[i];
+    for (int k = 0; k < 27; ++k) {
+      int32_t c = cols[i * kSlots + k];
+      if (c < 0) continue;
+      int rc = dc ? root_row(keys[c]) : c;
+      K[ri][rc] = vals[i * kSlots + k];
+      has[ri][rc] = 1;
+    }
+  }
+  auto apply = [&](const T* in, const T* y, T* out, int alpha, int beta) {
+    T mean = T(0);
+    if (dc) {
+      for (int a = 0; a < N; ++a) mean = mean + in[a];
+      mean = mean / T(N);
+    }
+    for (int a = 0; a < N; ++a) {
+      T s = T(0);
+      for (int q = 0; q < N; ++q)
+        if (has[a][q]) s = s + K[a][q] * in[q];
+      T v = alpha == 1 ? s : -s;
+      v = beta == 0 ? v : v + y[a];
+      if (dc) v = v + T(alpha) * mean;
+      out[a] = v;
+    }
+  };
+  auto dot = [&](const T* u, const T* v) {
+    T s = T(0);
+    for (int a = 0; a < N; ++a) s = s + u[a] * v[a];
+    return s;
+  };
+  T residual[64];
+  for (int a = 0; a < N; ++a) residual[a] = bb[a];
+  if (base == 0 && cycle > 0) apply(xx, bb, residual, -1, 1);
+  T nsq = dot(residual, residual);
+  if (double(nsq) > cg_accuracy * cg_accuracy) {
+    double tol = base == 0 ? 0.0 : cg_accuracy;
+    double atol = base == 0 ? cg_accuracy * sqrt(double(nsq)) : 0.0;
+    double eps = sizeof(T) == 8 ? 2.220446049250313e-16 : 1.1920928955078125e-07;
+    double bnorm = sqrt(double(dot(bb, bb)));
+    double abs_tol = dmax(dmax(atol, tol * bnorm), pow(eps, 9.0 / 4.0));
+    double atol_sq = abs_tol * abs_tol;
+    T gate = T(atol_sq);
+    apply(xx, bb, r, -1, 1);
+    T rr = dot(r, r);
+    for (int a = 0; a < N; ++a) p[a] = r[a];
+    for (int it = 0; it < nk; ++it) {
+      if (double(rr) <= atol_sq) break;
+      apply(p, Ap, Ap, 1, 0);
+      T pAp = dot(p, Ap);
+      T alpha = rr > gate ? rr / pAp : T(0);
+      for (int a = 0; a < N; ++a) {
+        xx[a] = xx[a] + alpha * p[a];
+        r[a] = r[a] - alpha * Ap[a];
+      }
+      T rr_new = dot(r, r);
+      T beta = rr_new > gate ? rr_new / rr : T(0);
+      for (int a = 0; a < N; ++a) p[a] = r[a] + beta * p[a];
+      rr = rr_new;
+    }
+  }
+  if (dc)
+    for (int a = 0; a < N; ++a) root_state[a] = xx[a];
+  for (int i = 0; i < nk; ++i) x[i] = xx[dc ? root_row(keys[i]) : i];
+}
+
+template <class T>
+__global__ void narrow_kernel(const T* in, int64_t n, float* out) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i < n) out[i] = float(in[i]);
+}
+
+// ------------------------------------------------------------------ orchestration
+struct LevelOp {
+  DBuf<int32_t> cols;
+  DBuf<char> vals;  // T
+};
+
+template <class T>
+static PointsData<T> make_points(const DensityData<T>& D, const NormalData<T>& N, const TreeData& tree, int d,
+                                 double pw, bool exact, cudaStream_t s) {
+  PointsData<T> P;
+  int64_t m = D.agg_count[d];
+  P.m = m;
+  P.pos.alloc(3 * m, s);
+  P.w.alloc(m, s);
+  HashMap support;
+  support.build(tree.support[d].p, tree.support_count[d], s);
+  DBuf<uint64_t> bk(m, s), sbk(m, s);
+  DBuf<int32_t> ids(m, s);
+  P.ids.alloc(m, s);
+  if (m) {
+    points_kernel<T><<<blocks_for(m), kThreads, 0, s>>>(D.agg_keys[d].p, D.agg_values[d].p, m, d, T(pw), N.average.p,
+                                                        support.view(), exact, P.pos.p, P.w.p, bk.p, ids.p);
+    PSR_LAUNCH_CHECK();
+    int Db = d > 0 ? d : 1;
+    sort_pairs(bk.p, sbk.p, ids.p, P.ids.p, m, 3 * Db, s);
+  }
+  DBuf<int32_t> heads(m, s), prefix(m, s);
+  int64_t u = 0;
+  if (m) {
+    bin_heads_kernel<<<blocks_for(m), kThreads, 0, s>>>(sbk.p, m, heads.p);
+    PSR_LAUNCH_CHECK();
+    inclusive_sum(heads.p, prefix.p, m, s);
+    u = read_scalar(prefix.p + m - 1, s);
+  }
+  P.nbins = u;
+  P.bkeys.alloc(u, s);
+  P.bstart.alloc(u + 1, s);
+  if (m) {
+    bin_fill_kernel<<<blocks_for(m + 1), kThreads, 0, s>>>(sbk.p, heads.p, prefix.p, m, d, P.bkeys.p, P.bstart.p);
+    PSR_LAUNCH_CHECK();
+  }
+  P.bins.build(P.bkeys.p, u, s);
+  return P;
+}
+
+template <class T>
+void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalData<T>& N,
+                  const std::vector<int64_t>& level_offsets, const int64_t* all_keys, const HashMap& all_hash,
+                  const Params& p, T* coefficients, cudaStream_t s, SolveStats* stats, StageSink* sink) {
+  const int finest = p.depth, base = p.base_depth;
+  HashView bh = all_hash.view();
+  auto keys_at = [&](int d) { return all_keys + level_offsets[d]; };
+  auto count_at = [&](int d) { return level_offsets[d + 1] - level_offsets[d]; };
+  HashMap nhash;
+  nhash.build(N.keys.p, N.count, s);
+  HashView nh = nhash.view();
+
+  // ---- A6 normal loads through the finest depth (normal_loads.py:66-190)
+  std::vector<DBuf<double>> same(finest + 1), from_child(finest + 1), from_parent(finest + 1);
+  auto stencil = [&](int test_d, int normal_d, HashView h, int64_t noff, const T* nvals, int64_t nrec,
+                     DBuf<double>& out) {
+    int64_t n = count_at(test_d);
+    out.alloc(n, s);
+    out.zero();
+    if (!nrec || !n) return;
+    int width = test_d < normal_d ? 6 : 4, first = test_d < normal_d ? -3 : -2;
+    int res = 1 << test_d;
+    DBuf<double> table(int64_t(res + 1) * width * 2, s);
+    normal_table_kernel<<<blocks_for(res + 1), kThreads, 0, s>>>(test_d, normal_d, first, width, table.p);
+    PSR_LAUNCH_CHECK();
+    normal_stencil_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(keys_at(test_d), n, test_d, normal_d, h, noff, nvals,
+                                                                table.p, width, first, out.p);
+    PSR_LAUNCH_CHECK();
+  };
+  DBuf<T> prev;
+  bool has_cumulative = false;
+  for (int d = 0; d <= finest; ++d) {
+    int64_t nrec = N.offsets[d + 1] - N.offsets[d];
+    has_cumulative = has_cumulative || nrec > 0;
+    if (d >= base) {
+      stencil(d, d, nh, 0, N.values.p, nrec, same[d]);
+      if (d > base) stencil(d - 1, d, nh, 0, N.values.p, nrec, from_child[d - 1]);
+    }
+    if (d < finest) {
+      int64_t n = count_at(d);
+      DBuf<T> cum(4 * n, s);
+      if (n) {
+        prolong_normals_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(keys_at(d), n, d, nh, N.values.p, bh,
+                                                                     d > 0 ? level_offsets[d - 1] : 0, prev.p, cum.p);
+        PSR_LAUNCH_CHECK();
+      }
+      if (d >= base && has_cumulative) stencil(d + 1, d, bh, level_offsets[d], cum.p, n, from_parent[d + 1]);
+      prev = std::move(cum);
+    }
+  }
+  std::vector<DBuf<double>> loads(finest + 1);
+  {
+    DBuf<double> finer(count_at(finest), s);
+    finer.zero();
+    for (int d = finest; d >= base; --d) {
+      int64_t n = count_at(d);
+      loads[d].alloc(n, s);
+      if (n) {
+        add3_kernel<<<blocks_for(n), kThreads, 0, s>>>(same[d].p, finer.p, from_parent[d].p ? from_parent[d].p : nullptr,
+                                                       n, loads[d].p);
+        PSR_LAUNCH_CHECK();
+      }
+      if (d > base) {
+        int64_t nc = count_at(d - 1);
+        DBuf<double> next(nc, s);
+        if (nc) {
+          PSR_CUDA(cudaMemcpyAsync(next.p, from_child[d - 1].p, nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+          restrict_add_kernel<T, double><<<blocks_for(nc), kThreads, 0, s>>>(keys_at(d - 1), nc, d, bh, level_offsets[d],
+                                                                             finer.p, next.p, true);
+          PSR_LAUNCH_CHECK();
+        }
+        finer = std::move(next);
+      }
+    }
+  }
+  same.clear();
+  from_child.clear();
+  from_parent.clear();
+  prev.release();
+
+  // ---- transfers (solver.py:339-342)
+  std::vector<DBuf<int32_t>> pcol(finest + 1);
+  std::vector<DBuf<T>> pval(finest + 1);
+  for (int d = 1; d <= std::min(finest, p.solve_depth); ++d) {
+    int64_t n = count_at(d);
+    pcol[d].alloc(8 * n, s);
+    pval[d].alloc(8 * n, s);
+    if (n) {
+      prolongation_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(keys_at(d), n, d, bh, level_offsets[d - 1], pcol[d].p,
+                                                                pval[d].p);
+      PSR_LAUNCH_CHECK();
+    }
+  }
+
+  const bool screened = p.point_weight > 0 && !p.exact;
+  DBuf<T> cumulative;
+  for (int d = base; d <= p.solve_depth; ++d) {
+    int64_t n = count_at(d);
+    if (!n) break;
+    PointsData<T> P;
+    if (screened) P = make_points(D, N, tree, d, p.point_weight, bool(p.exact), s);
+    PointsView<T> pv = screened ? P.view() : PointsView<T>();
+    int res = 1 << d;
+    DBuf<double> table(int64_t(res + 1) * 6, s);
+    stiffness_table_kernel<<<blocks_for(res + 1), kThreads, 0, s>>>(d, d, table.p);
+    PSR_LAUNCH_CHECK();
+    DBuf<int32_t> cols(kSlots * n, s);
+    DBuf<T> vals(kSlots * n, s), b(n, s);
+    if (screened)
+      assemble_level_kernel<T, true><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bh, level_offsets[d],
+                                                                         table.p, pv, loads[d].p, cols.p, vals.p, b.p);
+    else
+      assemble_level_kernel<T, false><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bh, level_offsets[d],
+                                                                          table.p, pv, loads[d].p, cols.p, vals.p, b.p);
+    PSR_LAUNCH_CHECK();
+    T* x = coefficients + level_offsets[d];
+    PSR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), s));
+    if (sink) sink->put("normal_load_" + std::to_string(d), loads[d].p, n, s);
+    if (d == base) {
+      // ---- regular multigrid at the base depth (solver.py:241-317)
+      std::vector<DBuf<int32_t>> mc(base + 1);
+      std::vector<DBuf<T>> mv(base + 1), rhs(base + 1), xs(base + 1);
+      std::vector<Schedule> sched(base + 1);
+      for (int l = base - 1; l >= 0; --l) {
+        int64_t nl = count_at(l);
+        mc[l].alloc(kSlots * nl, s);
+        mv[l].alloc(kSlots * nl, s);
+        const int32_t* fc = l + 1 == base ? cols.p : mc[l + 1].p;
+        const T* fv = l + 1 == base ? vals.p : mv[l + 1].p;
+        galerkin_kernel<T><<<blocks_for(nl, 64), 64, 0, s>>>(keys_at(l), nl, l + 1, bh, level_offsets[l + 1],
+                                                            level_offsets[l], fc, fv, mc[l].p, mv[l].p);
+        PSR_LAUNCH_CHECK();
+      }
+      for (int l = 0; l <= base; ++l) {
+        int64_t nl = count_at(l);
+        sched[l] = make_schedule(keys_at(l), nl, l, false, s);
+        if (l < base) {
+          rhs[l].alloc(nl, s);
+          rhs[l].zero();
+          xs[l].alloc(nl, s);
+          xs[l].zero();
+        }
+      }
+      auto Cl = [&](int l) { return l == base ? cols.p : mc[l].p; };
+      auto Vl = [&](int l) { return l == base ? vals.p : mv[l].p; };
+      auto Rl = [&](int l) { return l == base ? b.p : rhs[l].p; };
+      auto Xl = [&](int l) { return l == base ? x : xs[l].p; };
+      bool dc = base == 0 && p.point_weight == 0;
+      DBuf<T> root_state(64, s);
+      root_state.zero();
+      for (int cycle = 0; cycle < p.base_v_cycles; ++cycle) {
+        for (int l = base; l > 0; --l) {
+          int64_t nl = count_at(l);
+          relax_colors_kernel<T><<<1, 512, 0, s>>>(Cl(l), Vl(l), Rl(l), Xl(l), sched[l].rows.p, sched[l].off.p,
+                                                    p.iters, 1);
+          PSR_LAUNCH_CHECK();
+          DBuf<T> r(nl, s);
+          residual_kernel<T><<<blocks_for(nl), kThreads, 0, s>>>(Cl(l), Vl(l), Rl(l), Xl(l), nl, r.p);
+          PSR_LAUNCH_CHECK();
+          int64_t nc = count_at(l - 1);
+          restrict_add_kernel<T, T><<<blocks_for(nc), kThreads, 0, s>>>(keys_at(l - 1), nc, l, bh, level_offsets[l], r.p,
+                                                                        rhs[l - 1].p, false);
+          PSR_LAUNCH_CHECK();
+          PSR_CUDA(cudaMemsetAsync(xs[l - 1].p, 0, nc * sizeof(T), s));
+        }
+        root_solve_kernel<T><<<1, 32, 0, s>>>(keys_at(0), int(count_at(0)), Cl(0), Vl(0), Rl(0), Xl(0), root_state.p,
+                                              dc, p.cg_accuracy, base, cycle);
+        PSR_LAUNCH_CHECK();
+        for (int l = 1; l <= base; ++l) {
+          int64_t nl = count_at(l);
+          prolong_add_kernel<T><<<blocks_for(nl), kThreads, 0, s>>>(pcol[l].p, pval[l].p, nl, Xl(l - 1), Xl(l));
+          PSR_LAUNCH_CHECK();
+          PSR_CUDA(cudaMemsetAsync(xs[l - 1].p, 0, count_at(l - 1) * sizeof(T), s));
+          relax_colors_kernel<T><<<1, 512, 0, s>>>(Cl(l), Vl(l), Rl(l), Xl(l), sched[l].rows.p, sched[l].off.p,
+                                                    p.iters, 0);
+          PSR_LAUNCH_CHECK();
+        }
+      }
+      cumulative.alloc(n, s);
+      PSR_CUDA(cudaMemcpyAsync(cumulative.p, x, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+      if (sink) sink->put("rhs_" + std::to_string(d), b.p, n, s);
+    } else {
+      DBuf<double> ctable(int64_t(res + 1) * 6, s);
+      stiffness_table_kernel<<<blocks_for(res + 1), kThreads, 0, s>>>(d, d - 1, ctable.p);
+      PSR_LAUNCH_CHECK();
+      if (screened)
+        cross_apply_kernel<T, true><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bh, level_offsets[d - 1],
+                                                                        ctable.p, pv, cumulative.p, b.p);
+      else
+        cross_apply_kernel<T, false><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bh, level_offsets[d - 1],
+                                                                         ctable.p, pv, cumulative.p, b.p);
+      PSR_LAUNCH_CHECK();
+      if (sink) sink->put("rhs_" + std::to_string(d), b.p, n, s);
+      Schedule sch = make_schedule(keys_at(d), n, d, true, s);
+      float ms = 0;
+      if (sizeof(T) == 8 && p.precision == 1) {
+        // Mixed precision: float32 operator storage, float64 vector arithmetic.
+        DBuf<float> v32(kSlots * n, s);
+        narrow_kernel<T><<<blocks_for(kSlots * n), kThreads, 0, s>>>(vals.p, kSlots * n, v32.p);
+        PSR_LAUNCH_CHECK();
+        vals.release();
+        relax_sliced_ell<float, T>(cols.p, v32.p, b.p, x, sch.rows.p, sch.off.p, d, p.iters, s, stats ? &ms : nullptr);
+      } else {
+        relax_sliced_ell<T, T>(cols.p, vals.p, b.p, x, sch.rows.p, sch.off.p, d, p.iters, s, stats ? &ms : nullptr);
+      }
+      if (stats) {
+        stats->relax_ms += ms;
+        stats->row_visits += n * p.iters;
+        stats->level_relax_ms.push_back(ms);
+        stats->launches += 1;
+      }
+      DBuf<T> next(n, s);
+      PSR_CUDA(cudaMemcpyAsync(next.p, x, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+      prolong_add_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(pcol[d].p, pval[d].p, n, cumulative.p, next.p);
+      PSR_LAUNCH_CHECK();
+      cumulative = std::move(next);
+    }
+  }
+}
+
+template void solve_levels<float>(const TreeData&, const DensityData<float>&, const NormalData<float>&,
+                                  const std::vector<int64_t>&, const int64_t*, const HashMap&, const Params&, float*,
+                                  cudaStream_t, SolveStats*, StageSink*);
+template void solve_levels<double>(const TreeData&, const DensityData<double>&, const NormalData<double>&,
+                                   const std::vector<int64_t>&, const int64_t*, const HashMap&, const Params&, double*,
+                                   cudaStream_t, SolveStats*, StageSink*);
+template void relax_sliced_ell<float, float>(const int32_t*, const float*, const float*, float*, const int32_t*,
+                                             const int32_t*, int, int, cudaStream_t, float*);
+template void relax_sliced_ell<double, double>(const int32_t*, const double*, const double*, double*, const int32_t*,
+                                               const int32_t*, int, int, cudaStream_t, float*);
+template void relax_sliced_ell<float, double>(const int32_t*, const float*, const double*, double*, const int32_t*,
+                                              const int32_t*, int, int, cudaStream_t, float*);
+
+}  // namespace psr
