@@ -1,0 +1,308 @@
+#!/usr/bin/env python
+"""Depth-9 screened-Poisson benchmark (synthetic stand-in for the eagle scan, 800k points).
+
+One step = one full reconstruction (sample grouping, density and normal splats, tree,
+operator assembly, cascadic ordered Gauss-Seidel solve, field and isovalue) of an 800k-point
+bumpy sphere at depth 9, full depth 4, point weight 2, in the mixed precision the metric names
+(float64 solve, float32 relaxation operators).  Multi-GPU runs are independent replicas
+(weak scaling): the ordered solve does not shard.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  ``--impl reference`` times the CPU restatement of the
+reference algorithm (the oracle) on the host cores instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "depth-9 SPSR solve+adjoint ms, FP32/FP64-refined vs FP64, at ≤1e-6 field error"
+CONFIG = dict(depth=9, full_depth=4, point_weight=2.0, samples_per_node=1.5, scale=1.1, iters=8)
+POINTS = 800_000
+BYTES_PER_ROW_VISIT = {"f32": 124, "f64": 244}  # 27 operator entries + b, x read, x write + row id
+
+
+def peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cloud():
+    from warp_psr_b200 import clouds
+    p, n = clouds.bumpy_sphere(POINTS)
+    return p.astype(np.float32), n.astype(np.float32)
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[3:7]):
+                if flag.lower() in ("active", "1", "yes"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def field_error(result, reference, queries):
+    """Max |f - f64| at the queries, raw and normalised by max |f64| (both evaluated in float64)."""
+    import torch
+    q = torch.from_numpy(queries.astype(np.float64)).cuda()
+    ref_v, _, ok = reference.evaluate(q)
+    if result.field.coefficients.dtype == torch.float64:
+        v, _, _ = result.evaluate(q)
+    else:
+        v, _, _ = result.evaluate(q.float())
+        v = v.double()
+    m = ok.bool()
+    err = (v[m] - ref_v[m]).abs().max().item()
+    scale = ref_v[m].abs().max().item()
+    iso_err = abs(result.iso_value - reference.iso_value)
+    return {"max_abs": err, "normalised": err / scale, "iso_abs": iso_err}
+
+
+def run_ours(args, rank, world):
+    import torch
+    import torch.distributed as dist
+    from warp_psr_b200 import reconstruct, _lib
+
+    device = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(device)
+    p_host, n_host = cloud()
+    p_pin = torch.from_numpy(p_host).pin_memory()
+    n_pin = torch.from_numpy(n_host).pin_memory()
+    p_dev = p_pin.to(device)
+    n_dev = n_pin.to(device)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)  # > 126 MB L2
+    stream = torch.cuda.current_stream(device)
+
+    def step(**kw):
+        return reconstruct(p_dev, n_dev, precision=args.precision, **CONFIG, **kw)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    def timed(fn, k):
+        total = 0.0
+        last = None
+        for _ in range(k):
+            flush.fill_(1)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            last = fn()
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        return total / k, last
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = _lib.kernel_launches()
+    with Clocks(device.index) as clocks:
+        ms, result = timed(step, args.steps)
+    launches = _lib.kernel_launches() - launches0
+    torch.cuda.synchronize()
+    if world > 1:
+        t = torch.tensor([ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = t.item()
+        dist.barrier()
+
+    # End to end through the public API with host buffers: pinned H2D copy of the cloud,
+    # reconstruction, and the device-to-host read of the isovalue and transforms.
+    def e2e_step():
+        p = p_pin.to(device, non_blocking=True)
+        n = n_pin.to(device, non_blocking=True)
+        return reconstruct(p, n, precision=args.precision, **CONFIG)
+
+    e2e_ms, _ = timed(e2e_step, args.steps)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = t.item()
+
+    out_dtype = "f64" if result.field.coefficients.dtype == torch.float64 else "f32"
+    info = result.diagnostics
+    relax_s = info["relax_seconds"]
+    visits = info["relax_row_visits"]
+    # Roofline of the ordered relaxation: float32 operator entries (the mixed path stores
+    # the operator in float32 and the vectors in float64: 27*4 + 3*8 + 4 bytes per row visit).
+    per_visit = 27 * 4 + 3 * (8 if out_dtype == "f64" else 4) + 4
+    achieved = visits * per_visit / relax_s / 1e9 if relax_s > 0 else None
+    peak, peak_kind = peaks()
+    traffic_file = ROOT / "profiles" / "sliced_gs_traffic.json"
+    traffic = json.loads(traffic_file.read_text()).get("bytes_per_launch") if traffic_file.exists() else None
+
+    line = {
+        "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": out_dtype, "data": "synthetic",
+        "config": {"workload": "bumpy sphere 800k points (SH l<=8, 10x density variation), depth 9, full depth 4, "
+                               "SPSR point weight 2, 8 GS iterations; forward reconstruction (adjoint not included)",
+                   "points": POINTS, "coefficients": int(result.field.keys.numel()),
+                   "basis_counts": result.metadata["basis_counts"], "precision": args.precision,
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": "sliced_gs_kernel (ordered relaxation, all levels)",
+                     "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4) if achieved else None, "peak_kind": peak_kind,
+                     "bytes_per_row_visit": per_visit, "row_visits": visits, "kernel_ms": round(relax_s * 1e3, 3),
+                     "traffic": traffic},
+        "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(p_pin.numel() * 4 * 2),
+                "d2h_bytes_per_step": (1 + 32) * (8 if out_dtype == "f64" else 4)},
+        "gpu_launches": int(launches),
+        "stage_ms": {k: round(v * 1e3, 3) for k, v in result.metadata["timings_seconds"].items()},
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and not args.no_accuracy:
+        fp64 = reconstruct(p_dev.double(), n_dev.double(), **CONFIG)
+        rng = np.random.default_rng(2027)
+        lo, hi = p_host.min(0), p_host.max(0)
+        q = np.concatenate([p_host[rng.choice(len(p_host), 20000, replace=False)],
+                            lo + (hi - lo) * rng.uniform(size=(20000, 3))])
+        line["error_vs_fp64"] = field_error(result, fp64, q)
+        if args.precision != "input":
+            f32 = reconstruct(p_dev, n_dev, **CONFIG)
+            line["fp32_error_vs_fp64"] = field_error(f32, fp64, q)
+            ms32, _ = timed(lambda: reconstruct(p_dev, n_dev, **CONFIG), max(1, args.steps // 2))
+            ms64, _ = timed(lambda: reconstruct(p_dev.double(), n_dev.double(), **CONFIG), max(1, args.steps // 2))
+            line["variants_ms"] = {"fp32": round(ms32, 3), "fp64": round(ms64, 3)}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(p_host, n_host, steps=1)
+    return line
+
+
+def cpu_baseline(p, n, steps):
+    import oracle
+    times = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        oracle.OracleResult(p, n, **CONFIG)
+        times.append((time.perf_counter() - t) * 1e3)
+    return {"value": round(statistics.mean(times), 1), "unit": "ms", "cores": oracle.threads(), "kind": "port",
+            "sample": f"{len(times)} full forward reconstruction(s) of the benchmark workload by the C++ oracle "
+                      f"(OpenMP, {oracle.threads()} threads)"}
+
+
+def run_reference(args):
+    """The reference's algorithm on the host cores: the oracle (PoissonRecon and Warp are not available)."""
+    import oracle
+    p, n = cloud()
+    # Warm-up steps run a small sample of the workload (thread pool, page cache).
+    small = 50_000
+    for _ in range(args.warmup):
+        oracle.OracleResult(p[:small], n[:small], **CONFIG)
+    budget_s = 240.0
+    times = []
+    start = time.perf_counter()
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        oracle.OracleResult(p, n, **CONFIG)
+        times.append((time.perf_counter() - t) * 1e3)
+        if time.perf_counter() - start + times[-1] / 1e3 > budget_s:
+            break
+    ms = statistics.mean(times)
+    return {"metric": METRIC, "value": round(ms, 1), "unit": "ms", "n_gpus": 1, "steps": len(times),
+            "warmup": args.warmup, "ms_per_step": round(ms, 1), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": "bumpy sphere 800k points, depth 9, full depth 4, SPSR point weight 2; forward "
+                                   "reconstruction by the C++ CPU restatement of warp-psr (PoissonRecon 262b0f5 "
+                                   "and Warp are not installable offline)", "points": POINTS},
+            "cpu_baseline": {"value": round(ms, 1), "unit": "ms", "cores": oracle.threads(), "kind": "port",
+                             "sample": f"{len(times)} full reconstruction(s), warm-up on {small}-point prefixes"},
+            "e2e": {"value": round(ms, 1), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--precision", choices=("mixed", "input"), default="mixed")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        line = run_ours(args, rank, world)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

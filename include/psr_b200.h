@@ -68,6 +68,9 @@ typedef struct psr_info {
   double cube_to_model[16]; /* row-major 4x4 (transforms.py:255-280, first matrix) */
   double model_to_cube[16]; /* row-major 4x4 (second matrix) */
   double stage_ms[8];       /* samples, density, normal_field, tree, assembly_and_solve, field, isovalue, total */
+  double relax_ms;          /* device time of the ordered sliced relaxation kernels (CUDA events) */
+  int64_t relax_row_visits; /* rows x sweeps relaxed by those kernels */
+  int64_t relax_launches;
 } psr_info;
 
 /* Device arrays owned by the result (valid until psr_free). */
@@ -101,6 +104,10 @@ int psr_evaluate(const psr_result* result, const void* queries, int64_t nq, void
 int psr_device_field(const psr_result* result, psr_field_handle* handle);
 int psr_free(psr_result* result);
 int psr_last_error(char* buffer, size_t length);
+
+/* Number of this library's own kernel launches since it was loaded (library sorts and
+ * scans from CUB are not counted). */
+int psr_kernel_launches(int64_t* count);
 
 /* Ordered sliced Gauss-Seidel of one level on a caller-supplied CSR operator (device
  * pointers; rows = basis keys of `depth`).  Result bitwise identical to the reference's

@@ -70,6 +70,11 @@ def test_reconstruction_matches_oracle_and_fixture(kat):
     # A6/A7 loads and right-hand sides per solved level
     prm = ref.options
     for d in range(prm["base_depth"], prm["solve_depth"] + 1):
+        try:
+            ref.stage(f"rhs_{d}", npdt)
+        except KeyError:  # the cascadic loop stops at the first empty level (solver.py:361-362)
+            assert stage(f"rhs_{d}", fdt) is None
+            break
         _close(stage(f"normal_load_{d}", torch.float64).cpu().numpy(), ref.stage(f"normal_load_{d}", np.float64),
                1e-12, f"load {d}")
         _close(stage(f"rhs_{d}", fdt).cpu().numpy(), ref.stage(f"rhs_{d}", npdt), 4 * rtol, f"rhs {d}")

@@ -31,6 +31,7 @@ class Info(ctypes.Structure):
         ("basis_counts", ctypes.c_int64 * 16), ("support_counts", ctypes.c_int64 * 16),
         ("iso_value", ctypes.c_double), ("cube_to_model", ctypes.c_double * 16),
         ("model_to_cube", ctypes.c_double * 16), ("stage_ms", ctypes.c_double * 8),
+        ("relax_ms", ctypes.c_double), ("relax_row_visits", ctypes.c_int64), ("relax_launches", ctypes.c_int64),
     ]
 
 
@@ -51,7 +52,8 @@ class FieldHandle(ctypes.Structure):
 
 
 EXPORTS = ("psr_reconstruct", "psr_result_info", "psr_result_arrays", "psr_evaluate", "psr_device_field",
-           "psr_free", "psr_last_error", "psr_relax_sliced", "psr_isovalue", "psr_result_stage")
+           "psr_free", "psr_last_error", "psr_relax_sliced", "psr_isovalue", "psr_result_stage",
+           "psr_kernel_launches")
 
 _lib = None
 
@@ -81,6 +83,7 @@ def load():
     L.psr_relax_sliced.argtypes = [i32, vp, i64, i32, vp, vp, vp, vp, vp, i32, vp]
     L.psr_isovalue.argtypes = [i32, vp, vp, i64, vp, vp]
     L.psr_result_stage.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(vp), ctypes.POINTER(i64), ctypes.POINTER(i32)]
+    L.psr_kernel_launches.argtypes = [ctypes.POINTER(i64)]
     for name in EXPORTS:
         getattr(L, name).restype = i32
     _lib = L
@@ -91,6 +94,12 @@ def last_error():
     buf = ctypes.create_string_buffer(1024)
     load().psr_last_error(buf, len(buf))
     return buf.value.decode(errors="replace")
+
+
+def kernel_launches():
+    count = ctypes.c_int64()
+    check(load().psr_kernel_launches(ctypes.byref(count)))
+    return count.value
 
 
 def check(code):

@@ -14,6 +14,8 @@ using namespace psr;
 static thread_local std::string g_error;
 
 namespace psr {
+std::atomic<long long> g_kernel_launches{0};
+
 __global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, int64_t* keys, int32_t* vals,
                                    uint64_t mask, int32_t value_offset) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
@@ -195,6 +197,7 @@ int psr_reconstruct(const void* positions, const void* normals, int64_t n, int32
       if (dtype == PSR_FLOAT32) {
         DBuf<double> p64(3 * n, s), n64(3 * n, s);
         upcast_kernel<<<blocks_for(3 * n), kThreads, 0, s>>>((const float*)positions, 3 * n, p64.p);
+        PSR_LAUNCH_CHECK();
         upcast_kernel<<<blocks_for(3 * n), kThreads, 0, s>>>((const float*)normals, 3 * n, n64.p);
         PSR_LAUNCH_CHECK();
         run<double>(p64.p, n64.p, n, prm, s, R.get());
@@ -235,6 +238,9 @@ int psr_result_info(const psr_result* R, psr_info* info) {
     info->model_to_cube[i] = R->host_transforms[16 + i];
   }
   for (int i = 0; i < 8; ++i) info->stage_ms[i] = R->stage_ms[i];
+  info->relax_ms = R->stats.relax_ms;
+  info->relax_row_visits = R->stats.row_visits;
+  info->relax_launches = R->stats.launches;
   return PSR_OK;
 }
 
@@ -436,6 +442,12 @@ int psr_result_stage(const psr_result* R, const char* name, const void** data, i
   *data = it->second.data.p;
   *count = it->second.count;
   *elem = it->second.elem;
+  return PSR_OK;
+}
+
+int psr_kernel_launches(int64_t* count) {
+  if (!count) return PSR_EINVAL;
+  *count = int64_t(g_kernel_launches.load());
   return PSR_OK;
 }
 

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
+#include <atomic>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -25,7 +26,14 @@ struct Error : std::runtime_error {
                                 ":" + std::to_string(__LINE__) + ")");                              \
   } while (0)
 
-#define PSR_LAUNCH_CHECK() PSR_CUDA(cudaGetLastError())
+// Every launch of this library's kernels is followed by PSR_LAUNCH_CHECK(), which also
+// counts it (psr_kernel_launches).
+extern std::atomic<long long> g_kernel_launches;
+#define PSR_LAUNCH_CHECK()                                           \
+  do {                                                               \
+    ::psr::g_kernel_launches.fetch_add(1, std::memory_order_relaxed); \
+    PSR_CUDA(cudaGetLastError());                                    \
+  } while (0)
 
 constexpr int64_t kInvalidKey = 0x7fffffffffffffffLL;
 constexpr int kThreads = 256;

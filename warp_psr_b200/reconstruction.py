@@ -37,7 +37,7 @@ class _DeviceArray:
     """Zero-copy view of a result-owned device buffer (keeps the result alive)."""
 
     def __init__(self, ptr, shape, typestr, owner):
-        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr or 0), True),
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr or 0), False),
                                          "version": 3, "strides": None}
         self._owner = owner
 
@@ -241,5 +241,7 @@ def reconstruct(positions, normals, *, depth=6, full_depth=3, base_depth=None, s
 
     diagnostics = {"groups": int(info.groups), "support_keys": support, "stage": stage,
                    "level_offsets": [int(arrays.level_offsets[d]) for d in range(depth + 2)],
-                   "total_seconds": info.stage_ms[7] / 1000.0}
+                   "total_seconds": info.stage_ms[7] / 1000.0,
+                   "relax_seconds": info.relax_ms / 1000.0, "relax_row_visits": int(info.relax_row_visits),
+                   "relax_launches": int(info.relax_launches)}
     return Reconstruction(field, metadata, diagnostics)
