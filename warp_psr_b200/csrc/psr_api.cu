@@ -323,24 +323,45 @@ int psr_free(psr_result* R) {
 }
 
 namespace {
-__global__ void csr_to_ell_kernel(const int32_t* offsets, const int32_t* columns, const char* values, int elem,
-                                  int64_t n, int32_t* cols, char* vals, int* error) {
+// CSR rows (columns ascending) -> 28-slot rows where slot k holds the k-th lexicographic
+// neighbour; error 1: an entry is not within the 27-neighbourhood or columns not ascending.
+__global__ void csr_to_slots_kernel(const int64_t* keys, const int32_t* offsets, const int32_t* columns,
+                                    const char* values, int elem, int64_t n, int32_t* cols, char* vals, int* error) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
-  int b = offsets[i], e = offsets[i + 1];
-  if (e - b > 27 || e < b) {
-    atomicExch(error, 1);
-    e = b;
-  }
-  for (int k = 0; k < e - b; ++k)
-    if (columns[b + k] < 0 || columns[b + k] >= n) {
-      atomicExch(error, 3);
-      e = b;
-    }
   for (int k = 0; k < 28; ++k) {
-    bool in = k < e - b;
-    cols[i * 28 + k] = in ? columns[b + k] : -1;
-    for (int q = 0; q < elem; ++q) vals[(i * 28 + k) * elem + q] = in ? values[(int64_t(b) + k) * elem + q] : 0;
+    cols[i * 28 + k] = -1;
+    for (int q = 0; q < elem; ++q) vals[(i * 28 + k) * elem + q] = 0;
+  }
+  int b = offsets[i], e = offsets[i + 1];
+  if (e < b || e - b > 27) {
+    atomicExch(error, 1);
+    return;
+  }
+  int c[3];
+  key_coords(keys[i], c);
+  int last = -1;
+  for (int j = b; j < e; ++j) {
+    int col = columns[j];
+    if (col < 0 || col >= n) {
+      atomicExch(error, 3);
+      return;
+    }
+    int q[3];
+    key_coords(keys[col], q);
+    int dx = q[0] - c[0], dy = q[1] - c[1], dz = q[2] - c[2];
+    if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1 || (keys[col] >> 48) != (keys[i] >> 48)) {
+      atomicExch(error, 1);
+      return;
+    }
+    int k = (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
+    if (k <= last) {
+      atomicExch(error, 1);
+      return;
+    }
+    last = k;
+    cols[i * 28 + k] = col;
+    for (int q2 = 0; q2 < elem; ++q2) vals[(i * 28 + k) * elem + q2] = values[int64_t(j) * elem + q2];
   }
 }
 
@@ -350,9 +371,10 @@ __global__ void sliced_group_kernel(const int64_t* keys, int64_t n, int depth, u
   if (i >= n) return;
   int c[3];
   key_coords(keys[i], c);
-  if (c[2] > (1 << depth) || int(keys[i] >> 48) != depth) atomicExch(error, 2);
-  groups[i] = uint32_t((c[0] & 1) + 2 * (c[1] & 1) + 4 * min(c[2], 1 << depth));
-  ids[i] = int32_t(i);
+  if (c[0] > (1 << depth) || c[1] > (1 << depth) || c[2] > (1 << depth) || int(keys[i] >> 48) != depth)
+    atomicExch(error, 2);
+  if (groups) groups[i] = uint32_t((c[0] & 1) + 2 * (c[1] & 1) + 4 * min(c[2], 1 << depth));
+  if (ids) ids[i] = int32_t(i);
 }
 
 __global__ void offsets_kernel(const uint32_t* sorted, int64_t n, int count, int32_t* off) {
@@ -383,27 +405,21 @@ int psr_relax_sliced(int32_t dtype, const int64_t* keys, int64_t n, int32_t dept
     DBuf<char> vals(28 * n * elem, s);
     DBuf<int> error(1, s);
     error.zero();
-    csr_to_ell_kernel<<<blocks_for(n), kThreads, 0, s>>>(offsets, columns, (const char*)values, elem, n, cols.p, vals.p,
-                                                         error.p);
+    sliced_group_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, depth, nullptr, nullptr, error.p);
     PSR_LAUNCH_CHECK();
-    int groups = 4 * ((1 << depth) + 1);
-    DBuf<uint32_t> g(n, s), sg(n, s);
-    DBuf<int32_t> ids(n, s), rows(n, s), off(groups + 1, s);
-    sliced_group_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, depth, g.p, ids.p, error.p);
-    PSR_LAUNCH_CHECK();
-    sort_pairs(g.p, sg.p, ids.p, rows.p, n, bits_for(uint64_t(groups)), s);
-    offsets_kernel<<<blocks_for(groups + 1), kThreads, 0, s>>>(sg.p, n, groups, off.p);
+    csr_to_slots_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, offsets, columns, (const char*)values, elem, n,
+                                                          cols.p, vals.p, error.p);
     PSR_LAUNCH_CHECK();
     int err = read_scalar(error.p, s);
-    if (err == 1) throw Error(PSR_EINVAL, "a row has more than 27 entries");
+    if (err == 1) throw Error(PSR_EINVAL, "every row needs at most 27 entries, ascending, within its 27-neighbourhood");
     if (err == 2) throw Error(PSR_EINVAL, "keys must be basis keys of `depth`");
     if (err == 3) throw Error(PSR_EINVAL, "column index out of range");
     if (dtype == PSR_FLOAT64)
-      relax_sliced_ell<double, double>(cols.p, (const double*)vals.p, (const double*)b, (double*)x, rows.p, off.p,
-                                       depth, iters, s, nullptr);
+      relax_sliced_strips<double, double>(keys, n, depth, cols.p, (const double*)vals.p, (const double*)b, (double*)x,
+                                          iters, s, nullptr);
     else
-      relax_sliced_ell<float, float>(cols.p, (const float*)vals.p, (const float*)b, (float*)x, rows.p, off.p, depth,
-                                     iters, s, nullptr);
+      relax_sliced_strips<float, float>(keys, n, depth, cols.p, (const float*)vals.p, (const float*)b, (float*)x,
+                                        iters, s, nullptr);
     PSR_CUDA(cudaStreamSynchronize(s));
     return PSR_OK;
   } catch (const Error& e) {

@@ -103,6 +103,12 @@ template <class T, class V>
 void relax_sliced_ell(const int32_t* cols, const T* vals, const V* b, V* x, const int32_t* rows,
                       const int32_t* group_off, int depth, int iters, cudaStream_t s, float* ms);
 
+// Strip-scheduled ordered relaxation (psr_relax.cu): slot-ELL rows in key order, x in key
+// order holds the initial guess and receives the result.
+template <class T, class V>
+void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int32_t* cols, const T* vals,
+                         const V* b, V* x, int iters, cudaStream_t s, float* ms);
+
 // ---------------------------------------------------------------- A11/A12 field.py, reconstruction.py
 template <class T>
 void cumulative_coefficients(const int64_t* keys, const std::vector<int64_t>& offsets, const HashView& h,

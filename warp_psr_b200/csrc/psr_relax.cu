@@ -1,0 +1,399 @@
+// A8: ordered sliced Gauss-Seidel (warp-psr relaxation.py:121-210) as a persistent,
+// dependency-scheduled kernel over x-strips of each slice.
+//
+// Sequential definition: for front = 2^d .. -iters+1, for z in [max(front,0),
+// min(front+iters, 2^d+1)), for colour 0..3 (colour = (x&1) + 2(y&1)): update every row of
+// slice z with that colour (rows of one colour in one slice never couple).  Visit t of slice
+// z needs visit t of z+1 and visit t-1 of z-1 (relaxation.py:128-135).
+//
+// B200 mapping:
+//  * each slice-visit (z, t) is split into NS x-strips; strip tasks run on independent CTAs;
+//  * a strip recomputes a halo of width 3-c around itself in colour phase c, so the four
+//    colour phases need no synchronisation with neighbouring strips (the halo values are
+//    the same arithmetic on the same inputs, hence bit-identical to the neighbour's);
+//  * the strip's x footprint (three slices, x within 4 of the strip) is staged in shared
+//    memory once the dependencies are met; the phases then run on shared memory only;
+//  * x is double-buffered by visit parity: visit t of a slice is written to buffer t&1, so a
+//    strip never overwrites values another strip of the same visit still reads.  The slice
+//    dependency edges order every reader of buffer t&1's previous contents before the write;
+//  * rows are permuted into schedule order (slice, colour, x, y), so every footprint is 12
+//    contiguous position ranges, found through a per-(slice, colour) x-start table.
+// Waits are bounded; a timeout sets an error word and every CTA exits.
+#include "psr_internal.cuh"
+
+#include <algorithm>
+
+namespace psr {
+
+constexpr int kSlotsR = 28;
+
+struct StripLevel {
+  int n;          // 2^depth (slices 0..n)
+  int strips;     // NS
+  int width;      // S
+  int iters;
+  int cap;        // footprint capacity (elements) per CTA
+  int use_scratch;
+  const int32_t* cols;       // schedule positions, slot k = lexicographic neighbour k, -1 absent
+  const void* vals;          // T[rows*28]
+  const void* b;             // V[rows]
+  void* xb0;                 // V[rows]  even visits
+  void* xb1;                 // V[rows]  odd visits (holds the initial x)
+  const int64_t* keys;       // schedule order
+  const int32_t* xstart;     // [(n+1)*4][n+2]: first position of group (z,c) with x >= X
+  const int2* visits;        // slice-visits (z, t) in the sequential order
+  int nvisits;
+  int* done;                 // [n+1] completed strip tasks per slice
+  int* counter;
+  int* error;
+  void* scratch;             // V[grid*cap] when use_scratch
+};
+
+__device__ __forceinline__ int ld_acquire_r(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ bool wait_at_least(const int* p, int v, const int* error) {
+  for (long long it = 0; it < (1LL << 26); ++it) {
+    if (ld_acquire_r(p) >= v) return true;
+    if ((it & 63) == 63 && *(volatile const int*)error) return false;
+    __nanosleep(it < 512 ? 32 : 256);
+  }
+  return false;
+}
+
+template <class T, class V>
+__global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_task, s_fail, s_lo[3][4], s_hi[3][4], s_base[3][4], s_total;
+  const T* __restrict__ vals = reinterpret_cast<const T*>(L.vals);
+  const V* __restrict__ b = reinterpret_cast<const V*>(L.b);
+  V* xb0 = reinterpret_cast<V*>(L.xb0);
+  V* xb1 = reinterpret_cast<V*>(L.xb1);
+  V* foot = L.use_scratch ? reinterpret_cast<V*>(L.scratch) + int64_t(blockIdx.x) * L.cap
+                          : reinterpret_cast<V*>(smem_raw);
+  const int nx = L.n + 2;
+  const int total_tasks = L.nvisits * L.strips;
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_task = atomicAdd(L.counter, 1);
+      s_fail = 0;
+    }
+    __syncthreads();
+    const int task = s_task;
+    if (task >= total_tasks) return;
+    const int2 zt = L.visits[task / L.strips];
+    const int z = zt.x, t = zt.y, s = task % L.strips;
+    const int x0 = s * L.width;
+    // Footprint ranges: slices z-1, z, z+1 (j = 0, 1, 2), colours 0..3, x in [x0-4, x0+S+4).
+    if (threadIdx.x < 12) {
+      int j = threadIdx.x >> 2, c = threadIdx.x & 3, zz = z + j - 1;
+      int lo = 0, hi = 0;
+      if (zz >= 0 && zz <= L.n) {
+        const int32_t* xs = L.xstart + int64_t(zz * 4 + c) * nx;
+        lo = xs[max(x0 - 4, 0)];
+        hi = xs[min(x0 + L.width + 4, L.n + 1)];
+      }
+      s_lo[j][c] = lo;
+      s_hi[j][c] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int total = 0;
+      for (int j = 0; j < 3; ++j)
+        for (int c = 0; c < 4; ++c) {
+          s_base[j][c] = total;
+          total += s_hi[j][c] - s_lo[j][c];
+        }
+      s_total = total;
+      bool ok = total <= L.cap;
+      if (!ok) atomicExch(L.error, 2);
+      if (ok && z + 1 <= L.n) ok = wait_at_least(L.done + z + 1, (t + 1) * L.strips, L.error);
+      if (ok && z > 0) ok = wait_at_least(L.done + z - 1, t * L.strips, L.error);
+      if (ok) ok = wait_at_least(L.done + z, t * L.strips, L.error);
+      if (!ok) {
+        atomicExch(L.error, max(1, *(volatile int*)L.error));
+        s_fail = 1;
+      }
+    }
+    __syncthreads();
+    if (s_fail) return;
+    // Stage the footprint: slice z+1 after visit t, slices z and z-1 after visit t-1.
+    const V* cur = (t & 1) ? xb1 : xb0;
+    const V* prev = (t & 1) ? xb0 : xb1;
+    for (int r = 0; r < 12; ++r) {
+      int j = r >> 2, c = r & 3;
+      int lo = s_lo[j][c], cnt = s_hi[j][c] - lo, base = s_base[j][c];
+      const V* src = j == 2 ? cur : prev;
+      for (int i = threadIdx.x; i < cnt; i += blockDim.x) foot[base + i] = __ldcg(src + lo + i);
+    }
+    __syncthreads();
+    // Colour phases on the staged footprint (halo 3-c).
+    for (int c = 0; c < 4; ++c) {
+      int h = 3 - c;
+      const int32_t* xs = L.xstart + int64_t(z * 4 + c) * nx;
+      int p0 = xs[max(x0 - h, 0)], p1 = xs[min(x0 + L.width + h, L.n + 1)];
+      for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+        int64_t key = __ldg(L.keys + p);
+        int px = int((key >> 32) & 65535), py = int((key >> 16) & 65535);
+        const int4* cr = reinterpret_cast<const int4*>(L.cols + int64_t(p) * kSlotsR);
+        int cc[kSlotsR];
+#pragma unroll
+        for (int q = 0; q < kSlotsR / 4; ++q) {
+          int4 v = __ldg(cr + q);
+          cc[4 * q] = v.x;
+          cc[4 * q + 1] = v.y;
+          cc[4 * q + 2] = v.z;
+          cc[4 * q + 3] = v.w;
+        }
+        V r = __ldg(b + p);
+        T diagonal = T(0);
+        V xi = V(0);
+        int self = s_base[1][c] + (p - s_lo[1][c]);
+#pragma unroll
+        for (int k = 0; k < 27; ++k) {
+          if (cc[k] < 0) continue;
+          int dx = k / 9 - 1, dy = (k / 3) % 3 - 1, j = k % 3;
+          int cn = ((px + dx) & 1) + 2 * ((py + dy) & 1);
+          int fi = s_base[j][cn] + (cc[k] - s_lo[j][cn]);
+          if (fi < 0 || fi >= s_total) {  // not the k-th neighbour: malformed operator
+            atomicExch(L.error, 3);
+            continue;
+          }
+          V xn = foot[fi];
+          T a = __ldg(vals + int64_t(p) * kSlotsR + k);
+          r = r - xn * V(a);
+          if (k == 13) {
+            diagonal = a;
+            xi = xn;
+          }
+        }
+        if (diagonal != T(0)) foot[self] = xi + r * (V(1.0) / V(diagonal));
+      }
+      __syncthreads();
+    }
+    // Publish the strip's own rows (x in [x0, x0+S)) as visit t.
+    V* out = (t & 1) ? xb1 : xb0;
+    for (int c = 0; c < 4; ++c) {
+      const int32_t* xs = L.xstart + int64_t(z * 4 + c) * nx;
+      int p0 = xs[min(x0, L.n + 1)], p1 = xs[min(x0 + L.width, L.n + 1)];
+      int base = s_base[1][c] - s_lo[1][c];
+      for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) __stcg(out + p, foot[base + p]);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(L.done + z, 1);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ level preparation
+// xstart[(z*4+c)*(n+2) + X] = first schedule position of group 4z+c whose x >= X.
+__global__ void xstart_kernel(const int64_t* skeys, const int32_t* group_off, int n, int32_t* xstart) {
+  int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  int nx = n + 2;
+  int64_t total = int64_t(n + 1) * 4 * nx;
+  if (idx >= total) return;
+  int X = int(idx % nx);
+  int g = int(idx / nx);
+  int lo = group_off[g], hi = group_off[g + 1];
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    int x = int((skeys[mid] >> 32) & 65535);
+    if (x < X)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  xstart[idx] = lo;
+}
+
+__global__ void footprint_kernel(const int32_t* xstart, int n, int strips, int width, int* maxfp) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (n + 1) * strips) return;
+  int z = idx / strips, s = idx % strips, x0 = s * width, nx = n + 2;
+  int total = 0;
+  for (int j = -1; j <= 1; ++j) {
+    int zz = z + j;
+    if (zz < 0 || zz > n) continue;
+    for (int c = 0; c < 4; ++c) {
+      const int32_t* xs = xstart + int64_t(zz * 4 + c) * nx;
+      total += xs[min(x0 + width + 4, n + 1)] - xs[max(x0 - 4, 0)];
+    }
+  }
+  atomicMax(maxfp, total);
+}
+
+__global__ void inverse_kernel(const int32_t* perm, int64_t n, int32_t* inv) {
+  int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (p < n) inv[perm[p]] = int32_t(p);
+}
+
+// Gathers an ELL operator (key order) into schedule order, columns as schedule positions.
+template <class T, class V>
+__global__ void reorder_kernel(const int32_t* perm, const int32_t* inv, int64_t n, const int32_t* cols, const T* vals,
+                               const V* b, const V* x, const int64_t* keys, int32_t* scols, T* svals, V* sb, V* sx,
+                               int64_t* skeys) {
+  int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (p >= n) return;
+  int64_t row = perm[p];
+  for (int k = 0; k < kSlotsR; ++k) {
+    int32_t c = cols[row * kSlotsR + k];
+    scols[p * kSlotsR + k] = c >= 0 ? inv[c] : -1;
+    svals[p * kSlotsR + k] = vals[row * kSlotsR + k];
+  }
+  sb[p] = b[row];
+  sx[p] = x[row];
+  skeys[p] = keys[row];
+}
+
+template <class V>
+__global__ void scatter_back_kernel(const int32_t* perm, int64_t n, const V* sx, V* x) {
+  int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (p < n) x[perm[p]] = sx[p];
+}
+
+__global__ void slice_groups_kernel(const int64_t* keys, int64_t n, uint32_t* groups, int32_t* ids) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int c[3];
+  key_coords(keys[i], c);
+  groups[i] = uint32_t((c[0] & 1) + 2 * (c[1] & 1) + 4 * c[2]);
+  ids[i] = int32_t(i);
+}
+
+__global__ void group_bounds_kernel(const uint32_t* sorted, int64_t n, int count, int32_t* off) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g > count) return;
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) / 2;
+    if (sorted[mid] < uint32_t(g))
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  off[g] = int32_t(lo);
+}
+
+static int device_sms() {
+  static int count = 0;
+  if (!count) {
+    int dev = 0;
+    PSR_CUDA(cudaGetDevice(&dev));
+    PSR_CUDA(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev));
+  }
+  return count;
+}
+
+// Ordered sliced relaxation of one level given as slot-ELL rows in key order.  x (key
+// order) holds the initial guess and receives the result.
+template <class T, class V>
+void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int32_t* cols, const T* vals,
+                         const V* b, V* x, int iters, cudaStream_t s, float* ms) {
+  if (iters <= 0 || rows <= 0) return;
+  const int n = 1 << depth;
+  const int groups = 4 * (n + 1);
+  // Schedule order: stable sort by group (slice, colour); rows of a group stay in key order.
+  DBuf<uint32_t> g(rows, s), sg(rows, s);
+  DBuf<int32_t> ids(rows, s), perm(rows, s), inv(rows, s), off(groups + 1, s);
+  slice_groups_kernel<<<blocks_for(rows), kThreads, 0, s>>>(keys, rows, g.p, ids.p);
+  PSR_LAUNCH_CHECK();
+  sort_pairs(g.p, sg.p, ids.p, perm.p, rows, bits_for(uint64_t(groups)), s);
+  group_bounds_kernel<<<blocks_for(groups + 1), kThreads, 0, s>>>(sg.p, rows, groups, off.p);
+  PSR_LAUNCH_CHECK();
+  inverse_kernel<<<blocks_for(rows), kThreads, 0, s>>>(perm.p, rows, inv.p);
+  PSR_LAUNCH_CHECK();
+  DBuf<int32_t> scols(kSlotsR * rows, s);
+  DBuf<T> svals(kSlotsR * rows, s);
+  DBuf<V> sb(rows, s), x0(rows, s), x1(rows, s);
+  DBuf<int64_t> skeys(rows, s);
+  reorder_kernel<T, V><<<blocks_for(rows), kThreads, 0, s>>>(perm.p, inv.p, rows, cols, vals, b, x, keys, scols.p,
+                                                            svals.p, sb.p, x1.p, skeys.p);
+  PSR_LAUNCH_CHECK();
+  const int nx = n + 2;
+  DBuf<int32_t> xstart(int64_t(n + 1) * 4 * nx, s);
+  xstart_kernel<<<blocks_for(int64_t(n + 1) * 4 * nx), kThreads, 0, s>>>(skeys.p, off.p, n, xstart.p);
+  PSR_LAUNCH_CHECK();
+  // Strip width: about 32 strips per slice, at least 8 columns.
+  int width = 8;
+  while (width * 32 < n + 1) width *= 2;
+  int strips = (n + 1 + width - 1) / width;
+  DBuf<int> flags(n + 1 + 3, s);
+  flags.zero();
+  footprint_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, n, strips, width, flags.p + n + 3);
+  PSR_LAUNCH_CHECK();
+  int maxfp = read_scalar(flags.p + n + 3, s);
+  std::vector<int2> visits;
+  for (int front = n; front > -iters; --front)
+    for (int z = std::max(front, 0); z < std::min(front + iters, n + 1); ++z) visits.push_back(make_int2(z, z - front));
+  DBuf<int2> dvisits(int64_t(visits.size()), s);
+  PSR_CUDA(cudaMemcpyAsync(dvisits.p, visits.data(), visits.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+  const int smem_cap_bytes = 96 * 1024;
+  StripLevel L{};
+  L.n = n;
+  L.strips = strips;
+  L.width = width;
+  L.iters = iters;
+  L.cols = scols.p;
+  L.vals = svals.p;
+  L.b = sb.p;
+  L.xb0 = x0.p;
+  L.xb1 = x1.p;
+  L.keys = skeys.p;
+  L.xstart = xstart.p;
+  L.visits = dvisits.p;
+  L.nvisits = int(visits.size());
+  L.done = flags.p;
+  L.counter = flags.p + n + 1;
+  L.error = flags.p + n + 2;
+  int64_t need = int64_t(maxfp) * int64_t(sizeof(V));
+  int smem = 0;
+  L.use_scratch = need > smem_cap_bytes;
+  L.cap = std::max(maxfp, 1);
+  if (!L.use_scratch) smem = int(std::max<int64_t>(need, 16));
+  auto kernel = strip_gs_kernel<T, V>;
+  PSR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap_bytes));
+  int per_sm = 0;
+  PSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem));
+  int64_t total_tasks = int64_t(visits.size()) * strips;
+  int grid = int(std::min<int64_t>(total_tasks, int64_t(std::max(per_sm, 1)) * device_sms()));
+  DBuf<V> scratch;
+  if (L.use_scratch) {
+    scratch.alloc(int64_t(grid) * L.cap, s);
+    L.scratch = scratch.p;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ms) {
+    PSR_CUDA(cudaEventCreate(&e0));
+    PSR_CUDA(cudaEventCreate(&e1));
+    PSR_CUDA(cudaEventRecord(e0, s));
+  }
+  kernel<<<grid, 256, smem, s>>>(L);
+  PSR_LAUNCH_CHECK();
+  if (ms) PSR_CUDA(cudaEventRecord(e1, s));
+  scatter_back_kernel<V><<<blocks_for(rows), kThreads, 0, s>>>(perm.p, rows, ((iters - 1) & 1) ? x1.p : x0.p, x);
+  PSR_LAUNCH_CHECK();
+  int err = read_scalar(L.error, s);
+  if (ms) {
+    PSR_CUDA(cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  if (err == 2) throw Error(4, "ordered relaxation: footprint exceeds its capacity");
+  if (err == 3) throw Error(1, "ordered relaxation: an operator column is not its slot's neighbour");
+  if (err) throw Error(4, "ordered relaxation: a dependency wait timed out");
+}
+
+template void relax_sliced_strips<float, float>(const int64_t*, int64_t, int, const int32_t*, const float*,
+                                                const float*, float*, int, cudaStream_t, float*);
+template void relax_sliced_strips<double, double>(const int64_t*, int64_t, int, const int32_t*, const double*,
+                                                  const double*, double*, int, cudaStream_t, float*);
+template void relax_sliced_strips<float, double>(const int64_t*, int64_t, int, const int32_t*, const float*,
+                                                 const double*, double*, int, cudaStream_t, float*);
+
+}  // namespace psr

@@ -1081,7 +1081,6 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
                                                                          ctable.p, pv, cumulative.p, b.p);
       PSR_LAUNCH_CHECK();
       if (sink) sink->put("rhs_" + std::to_string(d), b.p, n, s);
-      Schedule sch = make_schedule(keys_at(d), n, d, true, s);
       float ms = 0;
       if (sizeof(T) == 8 && p.precision == 1) {
         // Mixed precision: float32 operator storage, float64 vector arithmetic.
@@ -1089,9 +1088,9 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
         narrow_kernel<T><<<blocks_for(kSlots * n), kThreads, 0, s>>>(vals.p, kSlots * n, v32.p);
         PSR_LAUNCH_CHECK();
         vals.release();
-        relax_sliced_ell<float, T>(cols.p, v32.p, b.p, x, sch.rows.p, sch.off.p, d, p.iters, s, stats ? &ms : nullptr);
+        relax_sliced_strips<float, T>(keys_at(d), n, d, cols.p, v32.p, b.p, x, p.iters, s, stats ? &ms : nullptr);
       } else {
-        relax_sliced_ell<T, T>(cols.p, vals.p, b.p, x, sch.rows.p, sch.off.p, d, p.iters, s, stats ? &ms : nullptr);
+        relax_sliced_strips<T, T>(keys_at(d), n, d, cols.p, vals.p, b.p, x, p.iters, s, stats ? &ms : nullptr);
       }
       if (stats) {
         stats->relax_ms += ms;
