@@ -48,6 +48,28 @@ def test_every_coupled_pair_keeps_its_visit_sequence(depth, iters):
             assert [t for t in par if t[0] in pair] == [t for t in seq if t[0] in pair]
 
 
+def wave_order(depth, iters):
+    n = 1 << depth
+    out = []
+    for q in range(n + 2 * (iters - 1) + 1):
+        first, last = max(0, (q - n + 1) // 2), min(iters - 1, q // 2)
+        out.extend((n - q + 2 * t, t) for t in range(first, last + 1))
+    return out
+
+
+@pytest.mark.parametrize("depth", [0, 1, 3, 5, 9])
+@pytest.mark.parametrize("iters", [1, 2, 8])
+def test_wave_dequeue_order_is_complete_and_deadlock_free(depth, iters):
+    seq = sequential(depth, iters)
+    waves = wave_order(depth, iters)
+    assert sorted(waves) == sorted(seq) and len(set(waves)) == len(waves)
+    pos = {task: i for i, task in enumerate(waves)}
+    for (z, t), i in pos.items():
+        for dep in ((z + 1, t), (z - 1, t - 1), (z, t - 1)):
+            if dep in pos:
+                assert pos[dep] < i
+
+
 def test_tasks_only_wait_on_earlier_tasks():
     # Deadlock freedom: every dependency of a task precedes it in the dequeue order.
     for depth in range(6):

@@ -328,9 +328,14 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
   footprint_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, n, strips, width, flags.p + n + 3);
   PSR_LAUNCH_CHECK();
   int maxfp = read_scalar(flags.p + n + 3, s);
+  // Slice-visits in wave order (relaxation.py:128-143): wave q = 2t + n - z holds slices two
+  // apart; every dependency of a wave-q task lies in wave q-1 or q-2, so dequeuing by wave
+  // is deadlock-free and keeps a whole wave (up to `iters` slice-visits) in flight.
   std::vector<int2> visits;
-  for (int front = n; front > -iters; --front)
-    for (int z = std::max(front, 0); z < std::min(front + iters, n + 1); ++z) visits.push_back(make_int2(z, z - front));
+  for (int q = 0; q <= n + 2 * (iters - 1); ++q) {
+    int first = std::max(0, (q - n + 1) / 2), last = std::min(iters - 1, q / 2);
+    for (int t = first; t <= last; ++t) visits.push_back(make_int2(n - q + 2 * t, t));
+  }
   DBuf<int2> dvisits(int64_t(visits.size()), s);
   PSR_CUDA(cudaMemcpyAsync(dvisits.p, visits.data(), visits.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
   const int smem_cap_bytes = 96 * 1024;
