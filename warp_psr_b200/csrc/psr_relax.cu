@@ -64,6 +64,28 @@ __device__ __forceinline__ bool wait_at_least(const int* p, int v, const int* er
   return false;
 }
 
+// All 28 slots of a row with 16-byte loads (rows are 16-byte aligned: 28 * 4 or 28 * 8 bytes).
+__device__ __forceinline__ void load_row(const float* src, float out[kSlotsR]) {
+  const float4* v = reinterpret_cast<const float4*>(src);
+#pragma unroll
+  for (int q = 0; q < kSlotsR / 4; ++q) {
+    float4 w = __ldg(v + q);
+    out[4 * q] = w.x;
+    out[4 * q + 1] = w.y;
+    out[4 * q + 2] = w.z;
+    out[4 * q + 3] = w.w;
+  }
+}
+__device__ __forceinline__ void load_row(const double* src, double out[kSlotsR]) {
+  const double2* v = reinterpret_cast<const double2*>(src);
+#pragma unroll
+  for (int q = 0; q < kSlotsR / 2; ++q) {
+    double2 w = __ldg(v + q);
+    out[2 * q] = w.x;
+    out[2 * q + 1] = w.y;
+  }
+}
+
 template <class T, class V>
 __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -149,6 +171,8 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
           cc[4 * q + 2] = v.z;
           cc[4 * q + 3] = v.w;
         }
+        T aa[kSlotsR];
+        load_row(vals + int64_t(p) * kSlotsR, aa);
         V r = __ldg(b + p);
         T diagonal = T(0);
         V xi = V(0);
@@ -164,7 +188,7 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
             continue;
           }
           V xn = foot[fi];
-          T a = __ldg(vals + int64_t(p) * kSlotsR + k);
+          T a = aa[k];
           r = r - xn * V(a);
           if (k == 13) {
             diagonal = a;
