@@ -34,6 +34,7 @@ struct StripLevel {
   int iters;
   int cap;        // footprint capacity (elements) per CTA
   int use_scratch;
+  int row_cap;    // update rows staged in shared memory per task (0: read rows from global)
   const int32_t* cols;       // schedule positions, slot k = lexicographic neighbour k, -1 absent
   const void* vals;          // T[rows*28]
   const void* b;             // V[rows]
@@ -86,16 +87,33 @@ __device__ __forceinline__ void load_row(const double* src, double out[kSlotsR])
   }
 }
 
+// Range r of a flattened index i (bases ascending, count entries + a final total).
+__device__ __forceinline__ int range_of(const int* base, int count, int i) {
+  int r = 0;
+  while (r + 1 < count && base[r + 1] <= i) ++r;
+  return r;
+}
+
 template <class T, class V>
 __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ int s_task, s_fail, s_lo[3][4], s_hi[3][4], s_base[3][4], s_total;
+  // Per task: footprint ranges (j = slice z-1+j, colour c), update ranges (colour c, halo
+  // 3-c) and own ranges (colour c, no halo), all as schedule positions.
+  __shared__ int s_task, s_fail, s_total, s_rows;
+  __shared__ int s_lo[12], s_hi[12], s_base[13];
+  __shared__ int s_p0[4], s_p1[4], s_rbase[5], s_o0[4], s_o1[4], s_obase[5];
   const T* __restrict__ vals = reinterpret_cast<const T*>(L.vals);
   const V* __restrict__ b = reinterpret_cast<const V*>(L.b);
   V* xb0 = reinterpret_cast<V*>(L.xb0);
   V* xb1 = reinterpret_cast<V*>(L.xb1);
   V* foot = L.use_scratch ? reinterpret_cast<V*>(L.scratch) + int64_t(blockIdx.x) * L.cap
                           : reinterpret_cast<V*>(smem_raw);
+  // Staged rows (when L.row_cap > 0): cols, values, b and packed (x, y) of the update rows.
+  unsigned char* rows_raw = smem_raw + (L.use_scratch ? 0 : ((int64_t(L.cap) * sizeof(V) + 15) & ~int64_t(15)));
+  int32_t* r_cols = reinterpret_cast<int32_t*>(rows_raw);
+  T* r_vals = reinterpret_cast<T*>(rows_raw + int64_t(L.row_cap) * kSlotsR * 4);
+  V* r_b = reinterpret_cast<V*>(rows_raw + int64_t(L.row_cap) * kSlotsR * (4 + sizeof(T)));
+  int32_t* r_xy = reinterpret_cast<int32_t*>(rows_raw + int64_t(L.row_cap) * (kSlotsR * (4 + sizeof(T)) + sizeof(V)));
   const int nx = L.n + 2;
   const int total_tasks = L.nvisits * L.strips;
   while (true) {
@@ -110,79 +128,166 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
     const int2 zt = L.visits[task / L.strips];
     const int z = zt.x, t = zt.y, s = task % L.strips;
     const int x0 = s * L.width;
-    // Footprint ranges: slices z-1, z, z+1 (j = 0, 1, 2), colours 0..3, x in [x0-4, x0+S+4).
-    if (threadIdx.x < 12) {
-      int j = threadIdx.x >> 2, c = threadIdx.x & 3, zz = z + j - 1;
-      int lo = 0, hi = 0;
-      if (zz >= 0 && zz <= L.n) {
-        const int32_t* xs = L.xstart + int64_t(zz * 4 + c) * nx;
-        lo = xs[max(x0 - 4, 0)];
-        hi = xs[min(x0 + L.width + 4, L.n + 1)];
+    // All range lookups in one round: 24 footprint bounds, 8 update bounds, 8 own bounds.
+    if (threadIdx.x < 40) {
+      int i = threadIdx.x;
+      if (i < 24) {
+        int r = i >> 1, j = r >> 2, c = r & 3, zz = z + j - 1;
+        int v = 0;
+        if (zz >= 0 && zz <= L.n) {
+          int X = (i & 1) ? min(x0 + L.width + 4, L.n + 1) : max(x0 - 4, 0);
+          v = L.xstart[int64_t(zz * 4 + c) * nx + X];
+        }
+        if (i & 1)
+          s_hi[r] = v;
+        else
+          s_lo[r] = v;
+      } else {
+        int k = i - 24, c = (k >> 1) & 3, own = k >= 8, h = own ? 0 : 3 - c;
+        int X = (k & 1) ? min(x0 + L.width + h, L.n + 1) : max(min(x0 - h, L.n + 1), 0);
+        int v = L.xstart[int64_t(z * 4 + c) * nx + X];
+        if (own) {
+          if (k & 1)
+            s_o1[c] = v;
+          else
+            s_o0[c] = v;
+        } else {
+          if (k & 1)
+            s_p1[c] = v;
+          else
+            s_p0[c] = v;
+        }
       }
-      s_lo[j][c] = lo;
-      s_hi[j][c] = hi;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
       int total = 0;
-      for (int j = 0; j < 3; ++j)
-        for (int c = 0; c < 4; ++c) {
-          s_base[j][c] = total;
-          total += s_hi[j][c] - s_lo[j][c];
-        }
+      for (int r = 0; r < 12; ++r) {
+        s_base[r] = total;
+        total += s_hi[r] - s_lo[r];
+      }
+      s_base[12] = total;
       s_total = total;
-      bool ok = total <= L.cap;
-      if (!ok) atomicExch(L.error, 2);
-      if (ok && z + 1 <= L.n) ok = wait_at_least(L.done + z + 1, (t + 1) * L.strips, L.error);
+      int rows = 0, owns = 0;
+      for (int c = 0; c < 4; ++c) {
+        s_rbase[c] = rows;
+        rows += s_p1[c] - s_p0[c];
+        s_obase[c] = owns;
+        owns += s_o1[c] - s_o0[c];
+      }
+      s_rbase[4] = rows;
+      s_obase[4] = owns;
+      s_rows = rows;
+      if (total > L.cap || (L.row_cap > 0 && rows > L.row_cap)) {
+        atomicExch(L.error, 2);
+        s_fail = 1;
+      }
+    }
+    __syncthreads();
+    if (s_fail) return;
+    // Stage the update rows' data before waiting: it does not depend on x.
+    if (L.row_cap > 0) {
+      for (int i = threadIdx.x; i < s_rows; i += blockDim.x) {
+        int c = range_of(s_rbase, 4, i);
+        int p = s_p0[c] + (i - s_rbase[c]);
+        const int4* cs = reinterpret_cast<const int4*>(L.cols + int64_t(p) * kSlotsR);
+        int4* cd = reinterpret_cast<int4*>(r_cols + int64_t(i) * kSlotsR);
+#pragma unroll
+        for (int q = 0; q < kSlotsR / 4; ++q) cd[q] = __ldg(cs + q);
+        const int4* vs = reinterpret_cast<const int4*>(vals + int64_t(p) * kSlotsR);
+        int4* vd = reinterpret_cast<int4*>(r_vals + int64_t(i) * kSlotsR);
+#pragma unroll
+        for (int q = 0; q < kSlotsR * int(sizeof(T)) / 16; ++q) vd[q] = __ldg(vs + q);
+        r_b[i] = __ldg(b + p);
+        int64_t key = __ldg(L.keys + p);
+        r_xy[i] = (int((key >> 32) & 65535) << 16) | int((key >> 16) & 65535);
+      }
+    }
+    if (threadIdx.x == 0) {
+      bool ok = true;
+      if (z + 1 <= L.n) ok = wait_at_least(L.done + z + 1, (t + 1) * L.strips, L.error);
       if (ok && z > 0) ok = wait_at_least(L.done + z - 1, t * L.strips, L.error);
       if (ok) ok = wait_at_least(L.done + z, t * L.strips, L.error);
       if (!ok) {
-        atomicExch(L.error, max(1, *(volatile int*)L.error));
+        atomicCAS(L.error, 0, 1);
         s_fail = 1;
       }
     }
     __syncthreads();
     if (s_fail) return;
     // Stage the footprint: slice z+1 after visit t, slices z and z-1 after visit t-1.
-    const V* cur = (t & 1) ? xb1 : xb0;
-    const V* prev = (t & 1) ? xb0 : xb1;
-    for (int r = 0; r < 12; ++r) {
-      int j = r >> 2, c = r & 3;
-      int lo = s_lo[j][c], cnt = s_hi[j][c] - lo, base = s_base[j][c];
-      const V* src = j == 2 ? cur : prev;
-      for (int i = threadIdx.x; i < cnt; i += blockDim.x) foot[base + i] = __ldcg(src + lo + i);
+    {
+      const V* cur = (t & 1) ? xb1 : xb0;
+      const V* prev = (t & 1) ? xb0 : xb1;
+      const int total = s_total;
+      for (int i0 = threadIdx.x; i0 < total; i0 += 4 * blockDim.x) {
+        V v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          int i = i0 + u * blockDim.x;
+          if (i < total) {
+            int r = range_of(s_base, 12, i);
+            v[u] = __ldcg(((r >> 2) == 2 ? cur : prev) + s_lo[r] + (i - s_base[r]));
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          int i = i0 + u * blockDim.x;
+          if (i < total) foot[i] = v[u];
+        }
+      }
     }
     __syncthreads();
     // Colour phases on the staged footprint (halo 3-c).
     for (int c = 0; c < 4; ++c) {
-      int h = 3 - c;
-      const int32_t* xs = L.xstart + int64_t(z * 4 + c) * nx;
-      int p0 = xs[max(x0 - h, 0)], p1 = xs[min(x0 + L.width + h, L.n + 1)];
+      const int p0 = s_p0[c], p1 = s_p1[c], rb = s_rbase[c];
       for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
-        int64_t key = __ldg(L.keys + p);
-        int px = int((key >> 32) & 65535), py = int((key >> 16) & 65535);
-        const int4* cr = reinterpret_cast<const int4*>(L.cols + int64_t(p) * kSlotsR);
         int cc[kSlotsR];
-#pragma unroll
-        for (int q = 0; q < kSlotsR / 4; ++q) {
-          int4 v = __ldg(cr + q);
-          cc[4 * q] = v.x;
-          cc[4 * q + 1] = v.y;
-          cc[4 * q + 2] = v.z;
-          cc[4 * q + 3] = v.w;
-        }
         T aa[kSlotsR];
-        load_row(vals + int64_t(p) * kSlotsR, aa);
-        V r = __ldg(b + p);
+        V r;
+        int px, py;
+        if (L.row_cap > 0) {
+          int i = rb + (p - p0);
+          const int4* cs = reinterpret_cast<const int4*>(r_cols + int64_t(i) * kSlotsR);
+#pragma unroll
+          for (int q = 0; q < kSlotsR / 4; ++q) {
+            int4 w = cs[q];
+            cc[4 * q] = w.x;
+            cc[4 * q + 1] = w.y;
+            cc[4 * q + 2] = w.z;
+            cc[4 * q + 3] = w.w;
+          }
+#pragma unroll
+          for (int q = 0; q < kSlotsR; ++q) aa[q] = r_vals[int64_t(i) * kSlotsR + q];
+          r = r_b[i];
+          px = r_xy[i] >> 16;
+          py = r_xy[i] & 65535;
+        } else {
+          const int4* cr = reinterpret_cast<const int4*>(L.cols + int64_t(p) * kSlotsR);
+#pragma unroll
+          for (int q = 0; q < kSlotsR / 4; ++q) {
+            int4 w = __ldg(cr + q);
+            cc[4 * q] = w.x;
+            cc[4 * q + 1] = w.y;
+            cc[4 * q + 2] = w.z;
+            cc[4 * q + 3] = w.w;
+          }
+          load_row(vals + int64_t(p) * kSlotsR, aa);
+          r = __ldg(b + p);
+          int64_t key = __ldg(L.keys + p);
+          px = int((key >> 32) & 65535);
+          py = int((key >> 16) & 65535);
+        }
         T diagonal = T(0);
         V xi = V(0);
-        int self = s_base[1][c] + (p - s_lo[1][c]);
+        int self = s_base[4 + c] + (p - s_lo[4 + c]);
 #pragma unroll
         for (int k = 0; k < 27; ++k) {
           if (cc[k] < 0) continue;
           int dx = k / 9 - 1, dy = (k / 3) % 3 - 1, j = k % 3;
           int cn = ((px + dx) & 1) + 2 * ((py + dy) & 1);
-          int fi = s_base[j][cn] + (cc[k] - s_lo[j][cn]);
+          int rr = j * 4 + cn;
+          int fi = s_base[rr] + (cc[k] - s_lo[rr]);
           if (fi < 0 || fi >= s_total) {  // not the k-th neighbour: malformed operator
             atomicExch(L.error, 3);
             continue;
@@ -200,12 +305,14 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
       __syncthreads();
     }
     // Publish the strip's own rows (x in [x0, x0+S)) as visit t.
-    V* out = (t & 1) ? xb1 : xb0;
-    for (int c = 0; c < 4; ++c) {
-      const int32_t* xs = L.xstart + int64_t(z * 4 + c) * nx;
-      int p0 = xs[min(x0, L.n + 1)], p1 = xs[min(x0 + L.width, L.n + 1)];
-      int base = s_base[1][c] - s_lo[1][c];
-      for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) __stcg(out + p, foot[base + p]);
+    {
+      V* out = (t & 1) ? xb1 : xb0;
+      const int owns = s_obase[4];
+      for (int i = threadIdx.x; i < owns; i += blockDim.x) {
+        int c = range_of(s_obase, 4, i);
+        int p = s_o0[c] + (i - s_obase[c]);
+        __stcg(out + p, foot[s_base[4 + c] + (p - s_lo[4 + c])]);
+      }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -240,6 +347,13 @@ __global__ void footprint_kernel(const int32_t* xstart, int n, int strips, int w
   int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (n + 1) * strips) return;
   int z = idx / strips, s = idx % strips, x0 = s * width, nx = n + 2;
+  int rows = 0;
+  for (int c = 0; c < 4; ++c) {
+    const int32_t* xs = xstart + int64_t(z * 4 + c) * nx;
+    int h = 3 - c;
+    rows += xs[min(x0 + width + h, n + 1)] - xs[max(min(x0 - h, n + 1), 0)];
+  }
+  atomicMax(maxfp + 1, rows);
   int total = 0;
   for (int j = -1; j <= 1; ++j) {
     int zz = z + j;
@@ -347,11 +461,12 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
   int width = 8;
   while (width * 32 < n + 1) width *= 2;
   int strips = (n + 1 + width - 1) / width;
-  DBuf<int> flags(n + 1 + 3, s);
+  DBuf<int> flags(n + 1 + 4, s);
   flags.zero();
-  footprint_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, n, strips, width, flags.p + n + 3);
+  footprint_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, n, strips, width, flags.p + n + 2 + 1);
   PSR_LAUNCH_CHECK();
-  int maxfp = read_scalar(flags.p + n + 3, s);
+  std::vector<int> caps = read_vector(flags.p + n + 3, 2, s);
+  int maxfp = caps[0], maxrows = caps[1];
   // Slice-visits in wave order (relaxation.py:128-143): wave q = 2t + n - z holds slices two
   // apart; every dependency of a wave-q task lies in wave q-1 or q-2, so dequeuing by wave
   // is deadlock-free and keeps a whole wave (up to `iters` slice-visits) in flight.
@@ -362,7 +477,7 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
   }
   DBuf<int2> dvisits(int64_t(visits.size()), s);
   PSR_CUDA(cudaMemcpyAsync(dvisits.p, visits.data(), visits.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
-  const int smem_cap_bytes = 96 * 1024;
+  const int smem_cap_bytes = 112 * 1024;
   StripLevel L{};
   L.n = n;
   L.strips = strips;
@@ -380,15 +495,25 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
   L.done = flags.p;
   L.counter = flags.p + n + 1;
   L.error = flags.p + n + 2;
-  int64_t need = int64_t(maxfp) * int64_t(sizeof(V));
-  int smem = 0;
-  L.use_scratch = need > smem_cap_bytes;
+  // Shared memory: the x footprint, plus the update rows' operator data when it fits.
+  int64_t fp_bytes = (int64_t(maxfp) * int64_t(sizeof(V)) + 15) & ~int64_t(15);
+  int64_t row_bytes = int64_t(maxrows) * (kSlotsR * (4 + int64_t(sizeof(T))) + int64_t(sizeof(V)) + 4);
+  int64_t smem = 0;
   L.cap = std::max(maxfp, 1);
-  if (!L.use_scratch) smem = int(std::max<int64_t>(need, 16));
+  L.use_scratch = fp_bytes > smem_cap_bytes;
+  L.row_cap = 0;
+  if (!L.use_scratch) {
+    smem = fp_bytes;
+    if (fp_bytes + row_bytes <= smem_cap_bytes) {
+      L.row_cap = std::max(maxrows, 1);
+      smem = fp_bytes + row_bytes;
+    }
+    smem = std::max<int64_t>(smem, 16);
+  }
   auto kernel = strip_gs_kernel<T, V>;
   PSR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap_bytes));
   int per_sm = 0;
-  PSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem));
+  PSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, int(smem)));
   int64_t total_tasks = int64_t(visits.size()) * strips;
   int grid = int(std::min<int64_t>(total_tasks, int64_t(std::max(per_sm, 1)) * device_sms()));
   DBuf<V> scratch;
@@ -402,7 +527,7 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
     PSR_CUDA(cudaEventCreate(&e1));
     PSR_CUDA(cudaEventRecord(e0, s));
   }
-  kernel<<<grid, 256, smem, s>>>(L);
+  kernel<<<grid, 256, size_t(smem), s>>>(L);
   PSR_LAUNCH_CHECK();
   if (ms) PSR_CUDA(cudaEventRecord(e1, s));
   scatter_back_kernel<V><<<blocks_for(rows), kThreads, 0, s>>>(perm.p, rows, ((iters - 1) & 1) ? x1.p : x0.p, x);
