@@ -22,15 +22,18 @@
 #include "psr_internal.cuh"
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 
 namespace psr {
 
 constexpr int kSlotsR = 28;
+constexpr int kPad = 32;
 
 struct StripLevel {
   int n;          // 2^depth (slices 0..n)
-  int strips;     // NS
-  int width;      // S
+  int strips;     // NS (per slice; boundaries balance the rows)
+  const int32_t* bounds;     // [(n+1)*(NS+1)] x boundaries of the strips of each slice
   int iters;
   int cap;        // footprint capacity (elements) per CTA
   int use_scratch;
@@ -44,11 +47,18 @@ struct StripLevel {
   const int32_t* xstart;     // [(n+1)*4][n+2]: first position of group (z,c) with x >= X
   const int2* visits;        // slice-visits (z, t) in the sequential order
   int nvisits;
-  int* done;                 // [n+1] completed strip tasks per slice
+  int* done;                 // completed strip tasks of slice z at done[z * kPad] (one 128-byte line each)
+  long long* trace;          // optional: 8 timestamps per task (PSR_RELAX_TRACE_FILE)
   int* counter;
   int* error;
   void* scratch;             // V[grid*cap] when use_scratch
 };
+
+__device__ __forceinline__ long long globaltimer() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ int ld_acquire_r(const int* p) {
   int v;
@@ -125,9 +135,14 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
     __syncthreads();
     const int task = s_task;
     if (task >= total_tasks) return;
+    long long* tr = (L.trace && threadIdx.x == 0) ? L.trace + int64_t(task) * 8 : nullptr;
+    if (tr) {
+      tr[0] = globaltimer();
+      tr[7] = blockIdx.x;
+    }
     const int2 zt = L.visits[task / L.strips];
     const int z = zt.x, t = zt.y, s = task % L.strips;
-    const int x0 = s * L.width;
+    const int x0 = L.bounds[z * (L.strips + 1) + s], x1 = L.bounds[z * (L.strips + 1) + s + 1];
     // All range lookups in one round: 24 footprint bounds, 8 update bounds, 8 own bounds.
     if (threadIdx.x < 40) {
       int i = threadIdx.x;
@@ -135,7 +150,7 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
         int r = i >> 1, j = r >> 2, c = r & 3, zz = z + j - 1;
         int v = 0;
         if (zz >= 0 && zz <= L.n) {
-          int X = (i & 1) ? min(x0 + L.width + 4, L.n + 1) : max(x0 - 4, 0);
+          int X = (i & 1) ? min(x1 + 4, L.n + 1) : max(x0 - 4, 0);
           v = L.xstart[int64_t(zz * 4 + c) * nx + X];
         }
         if (i & 1)
@@ -144,7 +159,7 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
           s_lo[r] = v;
       } else {
         int k = i - 24, c = (k >> 1) & 3, own = k >= 8, h = own ? 0 : 3 - c;
-        int X = (k & 1) ? min(x0 + L.width + h, L.n + 1) : max(min(x0 - h, L.n + 1), 0);
+        int X = (k & 1) ? min(x1 + h, L.n + 1) : max(min(x0 - h, L.n + 1), 0);
         int v = L.xstart[int64_t(z * 4 + c) * nx + X];
         if (own) {
           if (k & 1)
@@ -178,15 +193,16 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
       s_rbase[4] = rows;
       s_obase[4] = owns;
       s_rows = rows;
-      if (total > L.cap || (L.row_cap > 0 && rows > L.row_cap)) {
+      if (total > L.cap) {
         atomicExch(L.error, 2);
         s_fail = 1;
       }
     }
     __syncthreads();
     if (s_fail) return;
-    // Stage the update rows' data before waiting: it does not depend on x.
-    if (L.row_cap > 0) {
+    // Stage the update rows' data before waiting (it does not depend on x) when it fits.
+    const bool staged = s_rows <= L.row_cap;
+    if (staged) {
       for (int i = threadIdx.x; i < s_rows; i += blockDim.x) {
         int c = range_of(s_rbase, 4, i);
         int p = s_p0[c] + (i - s_rbase[c]);
@@ -203,18 +219,21 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
         r_xy[i] = (int((key >> 32) & 65535) << 16) | int((key >> 16) & 65535);
       }
     }
+    if (tr) tr[1] = globaltimer();
     if (threadIdx.x == 0) {
       bool ok = true;
-      if (z + 1 <= L.n) ok = wait_at_least(L.done + z + 1, (t + 1) * L.strips, L.error);
-      if (ok && z > 0) ok = wait_at_least(L.done + z - 1, t * L.strips, L.error);
-      if (ok) ok = wait_at_least(L.done + z, t * L.strips, L.error);
+      if (z + 1 <= L.n) ok = wait_at_least(L.done + (z + 1) * kPad, (t + 1) * L.strips, L.error);
+      if (ok && z > 0) ok = wait_at_least(L.done + (z - 1) * kPad, t * L.strips, L.error);
+      if (ok) ok = wait_at_least(L.done + z * kPad, t * L.strips, L.error);
       if (!ok) {
         atomicCAS(L.error, 0, 1);
         s_fail = 1;
       }
+      if (tr) tr[2] = globaltimer();
     }
     __syncthreads();
     if (s_fail) return;
+    if (tr) tr[3] = globaltimer();
     // Stage the footprint: slice z+1 after visit t, slices z and z-1 after visit t-1.
     {
       const V* cur = (t & 1) ? xb1 : xb0;
@@ -238,6 +257,7 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
       }
     }
     __syncthreads();
+    if (tr) tr[4] = globaltimer();
     // Colour phases on the staged footprint (halo 3-c).
     for (int c = 0; c < 4; ++c) {
       const int p0 = s_p0[c], p1 = s_p1[c], rb = s_rbase[c];
@@ -246,7 +266,7 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
         T aa[kSlotsR];
         V r;
         int px, py;
-        if (L.row_cap > 0) {
+        if (staged) {
           int i = rb + (p - p0);
           const int4* cs = reinterpret_cast<const int4*>(r_cols + int64_t(i) * kSlotsR);
 #pragma unroll
@@ -304,7 +324,8 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
       }
       __syncthreads();
     }
-    // Publish the strip's own rows (x in [x0, x0+S)) as visit t.
+    if (tr) tr[5] = globaltimer();
+    // Publish the strip's own rows (x in [x0, x1)) as visit t.
     {
       V* out = (t & 1) ? xb1 : xb0;
       const int owns = s_obase[4];
@@ -317,7 +338,8 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
-      atomicAdd(L.done + z, 1);
+      atomicAdd(L.done + z * kPad, 1);
+      if (tr) tr[6] = globaltimer();
     }
   }
 }
@@ -343,15 +365,35 @@ __global__ void xstart_kernel(const int64_t* skeys, const int32_t* group_off, in
   xstart[idx] = lo;
 }
 
-__global__ void footprint_kernel(const int32_t* xstart, int n, int strips, int width, int* maxfp) {
+// Row-balanced strip boundaries: slice z's rows split into NS runs of x of about equal size.
+__global__ void strip_bounds_kernel(const int32_t* xstart, int n, int strips, int32_t* bounds) {
+  int z = blockIdx.x * blockDim.x + threadIdx.x;
+  if (z > n) return;
+  int nx = n + 2;
+  const int32_t* xs = xstart + int64_t(z * 4) * nx;
+  int total = 0;
+  for (int c = 0; c < 4; ++c) total += xs[c * nx + n + 1] - xs[c * nx];
+  int32_t* out = bounds + int64_t(z) * (strips + 1);
+  out[0] = 0;
+  int k = 1, below = 0;
+  for (int X = 0; X <= n && k < strips; ++X) {
+    for (int c = 0; c < 4; ++c) below += xs[c * nx + X + 1] - xs[c * nx + X];
+    while (k < strips && int64_t(below) * strips >= int64_t(k) * total) out[k++] = X + 1;
+  }
+  while (k < strips) out[k++] = n + 1;
+  out[strips] = n + 1;
+}
+
+__global__ void footprint_kernel(const int32_t* xstart, const int32_t* bounds, int n, int strips, int* maxfp) {
   int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (n + 1) * strips) return;
-  int z = idx / strips, s = idx % strips, x0 = s * width, nx = n + 2;
+  int z = idx / strips, s = idx % strips, nx = n + 2;
+  int x0 = bounds[z * (strips + 1) + s], x1 = bounds[z * (strips + 1) + s + 1];
   int rows = 0;
   for (int c = 0; c < 4; ++c) {
     const int32_t* xs = xstart + int64_t(z * 4 + c) * nx;
     int h = 3 - c;
-    rows += xs[min(x0 + width + h, n + 1)] - xs[max(min(x0 - h, n + 1), 0)];
+    rows += xs[min(x1 + h, n + 1)] - xs[max(min(x0 - h, n + 1), 0)];
   }
   atomicMax(maxfp + 1, rows);
   int total = 0;
@@ -360,7 +402,7 @@ __global__ void footprint_kernel(const int32_t* xstart, int n, int strips, int w
     if (zz < 0 || zz > n) continue;
     for (int c = 0; c < 4; ++c) {
       const int32_t* xs = xstart + int64_t(zz * 4 + c) * nx;
-      total += xs[min(x0 + width + 4, n + 1)] - xs[max(x0 - 4, 0)];
+      total += xs[min(x1 + 4, n + 1)] - xs[max(x0 - 4, 0)];
     }
   }
   atomicMax(maxfp, total);
@@ -457,15 +499,22 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
   DBuf<int32_t> xstart(int64_t(n + 1) * 4 * nx, s);
   xstart_kernel<<<blocks_for(int64_t(n + 1) * 4 * nx), kThreads, 0, s>>>(skeys.p, off.p, n, xstart.p);
   PSR_LAUNCH_CHECK();
-  // Strip width: about 32 strips per slice, at least 8 columns.
-  int width = 8;
-  while (width * 32 < n + 1) width *= 2;
-  int strips = (n + 1 + width - 1) / width;
-  DBuf<int> flags(n + 1 + 4, s);
-  flags.zero();
-  footprint_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, n, strips, width, flags.p + n + 2 + 1);
+  // Strips per slice: enough tasks per wave (iters x strips) to fill the persistent grid,
+  // at least ~96 rows per strip.
+  int strips = int(std::max<int64_t>(1, std::min<int64_t>(int64_t(2 * device_sms() + iters - 1) / iters,
+                                                          rows / (int64_t(n + 1) * 96))));
+  DBuf<int32_t> bounds(int64_t(n + 1) * (strips + 1), s);
+  strip_bounds_kernel<<<blocks_for(n + 1), kThreads, 0, s>>>(xstart.p, n, strips, bounds.p);
   PSR_LAUNCH_CHECK();
-  std::vector<int> caps = read_vector(flags.p + n + 3, 2, s);
+  const int64_t pad_end = int64_t(n + 1) * kPad;
+  DBuf<int> flags(pad_end + 4 * kPad, s);
+  flags.zero();
+  int* counter = flags.p + pad_end;
+  int* error = flags.p + pad_end + kPad;
+  int* caps_dev = flags.p + pad_end + 2 * kPad;
+  footprint_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, bounds.p, n, strips, caps_dev);
+  PSR_LAUNCH_CHECK();
+  std::vector<int> caps = read_vector(caps_dev, 2, s);
   int maxfp = caps[0], maxrows = caps[1];
   // Slice-visits in wave order (relaxation.py:128-143): wave q = 2t + n - z holds slices two
   // apart; every dependency of a wave-q task lies in wave q-1 or q-2, so dequeuing by wave
@@ -481,7 +530,7 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
   StripLevel L{};
   L.n = n;
   L.strips = strips;
-  L.width = width;
+  L.bounds = bounds.p;
   L.iters = iters;
   L.cols = scols.p;
   L.vals = svals.p;
@@ -493,22 +542,19 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
   L.visits = dvisits.p;
   L.nvisits = int(visits.size());
   L.done = flags.p;
-  L.counter = flags.p + n + 1;
-  L.error = flags.p + n + 2;
-  // Shared memory: the x footprint, plus the update rows' operator data when it fits.
+  L.counter = counter;
+  L.error = error;
+  // Shared memory: the x footprint, plus the update rows' operator data of tasks whose rows
+  // fit (other tasks read their rows from global memory).
+  const int64_t per_row = kSlotsR * (4 + int64_t(sizeof(T))) + int64_t(sizeof(V)) + 4;
   int64_t fp_bytes = (int64_t(maxfp) * int64_t(sizeof(V)) + 15) & ~int64_t(15);
-  int64_t row_bytes = int64_t(maxrows) * (kSlotsR * (4 + int64_t(sizeof(T))) + int64_t(sizeof(V)) + 4);
   int64_t smem = 0;
   L.cap = std::max(maxfp, 1);
   L.use_scratch = fp_bytes > smem_cap_bytes;
   L.row_cap = 0;
   if (!L.use_scratch) {
-    smem = fp_bytes;
-    if (fp_bytes + row_bytes <= smem_cap_bytes) {
-      L.row_cap = std::max(maxrows, 1);
-      smem = fp_bytes + row_bytes;
-    }
-    smem = std::max<int64_t>(smem, 16);
+    L.row_cap = int(std::min<int64_t>(maxrows, (smem_cap_bytes - fp_bytes) / per_row));
+    smem = std::max<int64_t>(fp_bytes + L.row_cap * per_row, 16);
   }
   auto kernel = strip_gs_kernel<T, V>;
   PSR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap_bytes));
@@ -516,6 +562,13 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
   PSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, int(smem)));
   int64_t total_tasks = int64_t(visits.size()) * strips;
   int grid = int(std::min<int64_t>(total_tasks, int64_t(std::max(per_sm, 1)) * device_sms()));
+  const char* trace_file = std::getenv("PSR_RELAX_TRACE_FILE");
+  DBuf<long long> trace;
+  if (trace_file) {
+    trace.alloc(total_tasks * 8, s);
+    trace.zero();
+    L.trace = trace.p;
+  }
   DBuf<V> scratch;
   if (L.use_scratch) {
     scratch.alloc(int64_t(grid) * L.cap, s);
@@ -537,6 +590,16 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
     PSR_CUDA(cudaEventElapsedTime(ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+  }
+  if (trace_file) {
+    std::vector<long long> h = read_vector(trace.p, total_tasks * 8, s);
+    if (FILE* f = std::fopen(trace_file, "ab")) {
+      long long header[6] = {depth, n, strips, L.row_cap, grid, total_tasks};
+      std::fwrite(header, sizeof(header), 1, f);
+      std::fwrite(visits.data(), sizeof(int2), visits.size(), f);
+      std::fwrite(h.data(), sizeof(long long), h.size(), f);
+      std::fclose(f);
+    }
   }
   if (err == 2) throw Error(4, "ordered relaxation: footprint exceeds its capacity");
   if (err == 3) throw Error(1, "ordered relaxation: an operator column is not its slot's neighbour");
