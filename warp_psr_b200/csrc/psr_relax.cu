@@ -118,12 +118,12 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
   V* xb1 = reinterpret_cast<V*>(L.xb1);
   V* foot = L.use_scratch ? reinterpret_cast<V*>(L.scratch) + int64_t(blockIdx.x) * L.cap
                           : reinterpret_cast<V*>(smem_raw);
-  // Staged rows (when L.row_cap > 0): cols, values, b and packed (x, y) of the update rows.
+  // Staged rows (tasks with at most L.row_cap update rows): operator values, footprint
+  // indices of the 27 neighbours (-1 absent), b and the row's own footprint index.
   unsigned char* rows_raw = smem_raw + (L.use_scratch ? 0 : ((int64_t(L.cap) * sizeof(V) + 15) & ~int64_t(15)));
-  int32_t* r_cols = reinterpret_cast<int32_t*>(rows_raw);
-  T* r_vals = reinterpret_cast<T*>(rows_raw + int64_t(L.row_cap) * kSlotsR * 4);
-  V* r_b = reinterpret_cast<V*>(rows_raw + int64_t(L.row_cap) * kSlotsR * (4 + sizeof(T)));
-  int32_t* r_xy = reinterpret_cast<int32_t*>(rows_raw + int64_t(L.row_cap) * (kSlotsR * (4 + sizeof(T)) + sizeof(V)));
+  T* r_vals = reinterpret_cast<T*>(rows_raw);
+  V* r_b = reinterpret_cast<V*>(rows_raw + int64_t(L.row_cap) * kSlotsR * sizeof(T));
+  int16_t* r_fidx = reinterpret_cast<int16_t*>(rows_raw + int64_t(L.row_cap) * (kSlotsR * sizeof(T) + sizeof(V)));
   const int nx = L.n + 2;
   const int total_tasks = L.nvisits * L.strips;
   while (true) {
@@ -201,22 +201,39 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
     __syncthreads();
     if (s_fail) return;
     // Stage the update rows' data before waiting (it does not depend on x) when it fits.
-    const bool staged = s_rows <= L.row_cap;
+    const bool staged = s_rows <= L.row_cap && s_total < 32768;
     if (staged) {
       for (int i = threadIdx.x; i < s_rows; i += blockDim.x) {
         int c = range_of(s_rbase, 4, i);
         int p = s_p0[c] + (i - s_rbase[c]);
-        const int4* cs = reinterpret_cast<const int4*>(L.cols + int64_t(p) * kSlotsR);
-        int4* cd = reinterpret_cast<int4*>(r_cols + int64_t(i) * kSlotsR);
-#pragma unroll
-        for (int q = 0; q < kSlotsR / 4; ++q) cd[q] = __ldg(cs + q);
         const int4* vs = reinterpret_cast<const int4*>(vals + int64_t(p) * kSlotsR);
         int4* vd = reinterpret_cast<int4*>(r_vals + int64_t(i) * kSlotsR);
 #pragma unroll
         for (int q = 0; q < kSlotsR * int(sizeof(T)) / 16; ++q) vd[q] = __ldg(vs + q);
         r_b[i] = __ldg(b + p);
         int64_t key = __ldg(L.keys + p);
-        r_xy[i] = (int((key >> 32) & 65535) << 16) | int((key >> 16) & 65535);
+        int px = int((key >> 32) & 65535), py = int((key >> 16) & 65535);
+        const int4* cr = reinterpret_cast<const int4*>(L.cols + int64_t(p) * kSlotsR);
+        int16_t* fd = r_fidx + int64_t(i) * kSlotsR;
+#pragma unroll
+        for (int q = 0; q < kSlotsR / 4; ++q) {
+          int4 w = __ldg(cr + q);
+          int cw[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            int k = 4 * q + u, fi = -1;
+            if (k < 27 && cw[u] >= 0) {
+              int rr = (k % 3) * 4 + ((px + k / 9 - 1) & 1) + 2 * ((py + (k / 3) % 3 - 1) & 1);
+              fi = s_base[rr] + (cw[u] - s_lo[rr]);
+              if (fi < 0 || fi >= s_base[12]) {  // not the k-th neighbour: malformed operator
+                atomicExch(L.error, 3);
+                fi = -1;
+              }
+            }
+            fd[k] = int16_t(fi);
+          }
+        }
+        fd[27] = int16_t(s_base[4 + c] + (p - s_lo[4 + c]));  // the row itself
       }
     }
     if (tr) tr[1] = globaltimer();
@@ -262,27 +279,39 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
     for (int c = 0; c < 4; ++c) {
       const int p0 = s_p0[c], p1 = s_p1[c], rb = s_rbase[c];
       for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+        T diagonal = T(0);
+        V xi = V(0);
+        int self;
+        if (staged) {
+          // Staged row: 27 independent shared-memory loads, then the ordered subtraction.
+          int i = rb + (p - p0);
+          const int16_t* fd = r_fidx + int64_t(i) * kSlotsR;
+          const T* av = r_vals + int64_t(i) * kSlotsR;
+          V xs[27];
+          T aa[27];
+#pragma unroll
+          for (int k = 0; k < 27; ++k) {
+            int fi = fd[k];
+            xs[k] = fi >= 0 ? foot[fi] : V(0);
+            aa[k] = av[k];
+          }
+          V r = r_b[i];
+#pragma unroll
+          for (int k = 0; k < 27; ++k)
+            if (fd[k] >= 0) r = r - xs[k] * V(aa[k]);
+          if (fd[13] >= 0) {
+            diagonal = aa[13];
+            xi = xs[13];
+          }
+          self = fd[27];
+          if (diagonal != T(0)) foot[self] = xi + r * (V(1.0) / V(diagonal));
+          continue;
+        }
         int cc[kSlotsR];
         T aa[kSlotsR];
         V r;
         int px, py;
-        if (staged) {
-          int i = rb + (p - p0);
-          const int4* cs = reinterpret_cast<const int4*>(r_cols + int64_t(i) * kSlotsR);
-#pragma unroll
-          for (int q = 0; q < kSlotsR / 4; ++q) {
-            int4 w = cs[q];
-            cc[4 * q] = w.x;
-            cc[4 * q + 1] = w.y;
-            cc[4 * q + 2] = w.z;
-            cc[4 * q + 3] = w.w;
-          }
-#pragma unroll
-          for (int q = 0; q < kSlotsR; ++q) aa[q] = r_vals[int64_t(i) * kSlotsR + q];
-          r = r_b[i];
-          px = r_xy[i] >> 16;
-          py = r_xy[i] & 65535;
-        } else {
+        {
           const int4* cr = reinterpret_cast<const int4*>(L.cols + int64_t(p) * kSlotsR);
 #pragma unroll
           for (int q = 0; q < kSlotsR / 4; ++q) {
@@ -298,9 +327,7 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
           px = int((key >> 32) & 65535);
           py = int((key >> 16) & 65535);
         }
-        T diagonal = T(0);
-        V xi = V(0);
-        int self = s_base[4 + c] + (p - s_lo[4 + c]);
+        self = s_base[4 + c] + (p - s_lo[4 + c]);
 #pragma unroll
         for (int k = 0; k < 27; ++k) {
           if (cc[k] < 0) continue;
@@ -526,7 +553,7 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
   }
   DBuf<int2> dvisits(int64_t(visits.size()), s);
   PSR_CUDA(cudaMemcpyAsync(dvisits.p, visits.data(), visits.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
-  const int smem_cap_bytes = 112 * 1024;
+  const int smem_cap_bytes = 72 * 1024;  // three CTAs per SM
   StripLevel L{};
   L.n = n;
   L.strips = strips;
@@ -546,7 +573,7 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
   L.error = error;
   // Shared memory: the x footprint, plus the update rows' operator data of tasks whose rows
   // fit (other tasks read their rows from global memory).
-  const int64_t per_row = kSlotsR * (4 + int64_t(sizeof(T))) + int64_t(sizeof(V)) + 4;
+  const int64_t per_row = kSlotsR * (int64_t(sizeof(T)) + 2) + int64_t(sizeof(V));
   int64_t fp_bytes = (int64_t(maxfp) * int64_t(sizeof(V)) + 15) & ~int64_t(15);
   int64_t smem = 0;
   L.cap = std::max(maxfp, 1);
