@@ -553,7 +553,7 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
   }
   DBuf<int2> dvisits(int64_t(visits.size()), s);
   PSR_CUDA(cudaMemcpyAsync(dvisits.p, visits.data(), visits.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
-  const int smem_cap_bytes = 72 * 1024;  // three CTAs per SM
+  const int smem_cap_bytes = 110 * 1024;  // two CTAs per SM
   StripLevel L{};
   L.n = n;
   L.strips = strips;
