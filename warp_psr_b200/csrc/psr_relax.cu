@@ -121,9 +121,11 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
   // Staged rows (tasks with at most L.row_cap update rows): operator values, footprint
   // indices of the 27 neighbours (-1 absent), b and the row's own footprint index.
   unsigned char* rows_raw = smem_raw + (L.use_scratch ? 0 : ((int64_t(L.cap) * sizeof(V) + 15) & ~int64_t(15)));
+  // Layout (every part 16-byte aligned): values T[28] per row (112 or 224 bytes), footprint
+  // indices int16[32] per row (64 bytes: slots 0..26, the row itself at 27, padding), b.
   T* r_vals = reinterpret_cast<T*>(rows_raw);
-  V* r_b = reinterpret_cast<V*>(rows_raw + int64_t(L.row_cap) * kSlotsR * sizeof(T));
-  int16_t* r_fidx = reinterpret_cast<int16_t*>(rows_raw + int64_t(L.row_cap) * (kSlotsR * sizeof(T) + sizeof(V)));
+  int16_t* r_fidx = reinterpret_cast<int16_t*>(rows_raw + int64_t(L.row_cap) * kSlotsR * sizeof(T));
+  V* r_b = reinterpret_cast<V*>(rows_raw + int64_t(L.row_cap) * (kSlotsR * sizeof(T) + 64));
   const int nx = L.n + 2;
   const int total_tasks = L.nvisits * L.strips;
   while (true) {
@@ -214,26 +216,37 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
         int64_t key = __ldg(L.keys + p);
         int px = int((key >> 32) & 65535), py = int((key >> 16) & 65535);
         const int4* cr = reinterpret_cast<const int4*>(L.cols + int64_t(p) * kSlotsR);
-        int16_t* fd = r_fidx + int64_t(i) * kSlotsR;
+        int cw[kSlotsR];
 #pragma unroll
         for (int q = 0; q < kSlotsR / 4; ++q) {
           int4 w = __ldg(cr + q);
-          int cw[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            int k = 4 * q + u, fi = -1;
-            if (k < 27 && cw[u] >= 0) {
-              int rr = (k % 3) * 4 + ((px + k / 9 - 1) & 1) + 2 * ((py + (k / 3) % 3 - 1) & 1);
-              fi = s_base[rr] + (cw[u] - s_lo[rr]);
-              if (fi < 0 || fi >= s_base[12]) {  // not the k-th neighbour: malformed operator
-                atomicExch(L.error, 3);
-                fi = -1;
-              }
-            }
-            fd[k] = int16_t(fi);
-          }
+          cw[4 * q] = w.x;
+          cw[4 * q + 1] = w.y;
+          cw[4 * q + 2] = w.z;
+          cw[4 * q + 3] = w.w;
         }
-        fd[27] = int16_t(s_base[4 + c] + (p - s_lo[4 + c]));  // the row itself
+        int16_t f[32];
+        bool bad = false;
+#pragma unroll
+        for (int k = 0; k < 27; ++k) {
+          int fi = -1;
+          if (cw[k] >= 0) {
+            int rr = (k % 3) * 4 + ((px + k / 9 - 1) & 1) + 2 * ((py + (k / 3) % 3 - 1) & 1);
+            fi = s_base[rr] + (cw[k] - s_lo[rr]);
+            if (fi < 0 || fi >= s_base[12]) {  // not the k-th neighbour: malformed operator
+              bad = true;
+              fi = -1;
+            }
+          }
+          f[k] = int16_t(fi);
+        }
+        f[27] = int16_t(s_base[4 + c] + (p - s_lo[4 + c]));  // the row itself
+        f[28] = f[29] = f[30] = f[31] = -1;
+        int4* fd = reinterpret_cast<int4*>(r_fidx + int64_t(i) * 32);
+        const int4* fs = reinterpret_cast<const int4*>(f);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) fd[q] = fs[q];
+        if (bad) atomicExch(L.error, 3);
       }
     }
     if (tr) tr[1] = globaltimer();
@@ -252,24 +265,23 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
     if (s_fail) return;
     if (tr) tr[3] = globaltimer();
     // Stage the footprint: slice z+1 after visit t, slices z and z-1 after visit t-1.
+    // One warp per contiguous range.
     {
       const V* cur = (t & 1) ? xb1 : xb0;
       const V* prev = (t & 1) ? xb0 : xb1;
-      const int total = s_total;
-      for (int i0 = threadIdx.x; i0 < total; i0 += 4 * blockDim.x) {
-        V v[4];
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+      for (int r = warp; r < 12; r += nwarps) {
+        const V* src = ((r >> 2) == 2 ? cur : prev) + s_lo[r];
+        V* dst = foot + s_base[r];
+        const int cnt = s_hi[r] - s_lo[r];
+        for (int i0 = lane; i0 < cnt; i0 += 128) {
+          V v[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          int i = i0 + u * blockDim.x;
-          if (i < total) {
-            int r = range_of(s_base, 12, i);
-            v[u] = __ldcg(((r >> 2) == 2 ? cur : prev) + s_lo[r] + (i - s_base[r]));
-          }
-        }
+          for (int u = 0; u < 4; ++u)
+            if (i0 + 32 * u < cnt) v[u] = __ldcg(src + i0 + 32 * u);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          int i = i0 + u * blockDim.x;
-          if (i < total) foot[i] = v[u];
+          for (int u = 0; u < 4; ++u)
+            if (i0 + 32 * u < cnt) dst[i0 + 32 * u] = v[u];
         }
       }
     }
@@ -285,15 +297,25 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
         if (staged) {
           // Staged row: 27 independent shared-memory loads, then the ordered subtraction.
           int i = rb + (p - p0);
-          const int16_t* fd = r_fidx + int64_t(i) * kSlotsR;
-          const T* av = r_vals + int64_t(i) * kSlotsR;
+          int16_t fd[32];
+          {
+            const int4* fs = reinterpret_cast<const int4*>(r_fidx + int64_t(i) * 32);
+            int4* fl = reinterpret_cast<int4*>(fd);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) fl[q] = fs[q];
+          }
+          T aa[kSlotsR];
+          {
+            const int4* vs = reinterpret_cast<const int4*>(r_vals + int64_t(i) * kSlotsR);
+            int4* vl = reinterpret_cast<int4*>(aa);
+#pragma unroll
+            for (int q = 0; q < kSlotsR * int(sizeof(T)) / 16; ++q) vl[q] = vs[q];
+          }
           V xs[27];
-          T aa[27];
 #pragma unroll
           for (int k = 0; k < 27; ++k) {
             int fi = fd[k];
             xs[k] = fi >= 0 ? foot[fi] : V(0);
-            aa[k] = av[k];
           }
           V r = r_b[i];
 #pragma unroll
@@ -355,11 +377,10 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
     // Publish the strip's own rows (x in [x0, x1)) as visit t.
     {
       V* out = (t & 1) ? xb1 : xb0;
-      const int owns = s_obase[4];
-      for (int i = threadIdx.x; i < owns; i += blockDim.x) {
-        int c = range_of(s_obase, 4, i);
-        int p = s_o0[c] + (i - s_obase[c]);
-        __stcg(out + p, foot[s_base[4 + c] + (p - s_lo[4 + c])]);
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+      for (int c = warp; c < 4; c += nwarps) {
+        const int o0 = s_o0[c], o1 = s_o1[c], base = s_base[4 + c] - s_lo[4 + c];
+        for (int p = o0 + lane; p < o1; p += 32) __stcg(out + p, foot[base + p]);
       }
     }
     __syncthreads();
@@ -573,7 +594,7 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
   L.error = error;
   // Shared memory: the x footprint, plus the update rows' operator data of tasks whose rows
   // fit (other tasks read their rows from global memory).
-  const int64_t per_row = kSlotsR * (int64_t(sizeof(T)) + 2) + int64_t(sizeof(V));
+  const int64_t per_row = kSlotsR * int64_t(sizeof(T)) + 64 + int64_t(sizeof(V));
   int64_t fp_bytes = (int64_t(maxfp) * int64_t(sizeof(V)) + 15) & ~int64_t(15);
   int64_t smem = 0;
   L.cap = std::max(maxfp, 1);
