@@ -4,21 +4,30 @@
 // Sequential definition: for front = 2^d .. -iters+1, for z in [max(front,0),
 // min(front+iters, 2^d+1)), for colour 0..3 (colour = (x&1) + 2(y&1)): update every row of
 // slice z with that colour (rows of one colour in one slice never couple).  Visit t of slice
-// z needs visit t of z+1 and visit t-1 of z-1 (relaxation.py:128-135).
+// z needs visit t of z+1 and visit t-1 of z-1 (relaxation.py:128-135).  Any execution that
+// honours those edges is bitwise identical to the sequential order.
 //
 // B200 mapping:
-//  * each slice-visit (z, t) is split into NS x-strips; strip tasks run on independent CTAs;
+//  * rows are permuted into schedule order (slice, colour, x, y): the rows of one slice and
+//    colour within an x-window are one contiguous position range;
+//  * each slice-visit (z, t) is split into row-balanced x-strips; a strip task runs on one
+//    CTA (one CTA per SM, persistent), tasks are taken in wave order (wave q = 2t + 2^d - z);
 //  * a strip recomputes a halo of width 3-c around itself in colour phase c, so the four
-//    colour phases need no synchronisation with neighbouring strips (the halo values are
-//    the same arithmetic on the same inputs, hence bit-identical to the neighbour's);
-//  * the strip's x footprint (three slices, x within 4 of the strip) is staged in shared
-//    memory once the dependencies are met; the phases then run on shared memory only;
+//    colour phases need no synchronisation with neighbouring strips (the halo values are the
+//    same arithmetic on the same inputs, hence bit-identical to the neighbour's);
+//  * right after a task is taken, one thread issues bulk copies (cp.async.bulk, completion on
+//    an mbarrier) of the task's operator rows, neighbour indices and right-hand side into
+//    shared memory; they land while the task waits for its dependencies;
+//  * once the dependencies are met the x footprint (three slices, x within 4 of the strip)
+//    is staged in shared memory and the four phases run on shared memory only;
+//  * neighbours are addressed by their index inside their (slice, colour) group; since the
+//    colour of a phase is fixed, the footprint range of slot k is a compile-time function of
+//    (colour, k) and a neighbour's footprint index is one addition;
 //  * x is double-buffered by visit parity: visit t of a slice is written to buffer t&1, so a
 //    strip never overwrites values another strip of the same visit still reads.  The slice
-//    dependency edges order every reader of buffer t&1's previous contents before the write;
-//  * rows are permuted into schedule order (slice, colour, x, y), so every footprint is 12
-//    contiguous position ranges, found through a per-(slice, colour) x-start table.
-// Waits are bounded; a timeout sets an error word and every CTA exits.
+//    dependency edges order every reader of buffer t&1's previous contents before the write.
+// Every wait is bounded; a timeout sets an error word, waits (bounded) for its own copies in
+// flight, and every CTA exits.
 #include "psr_internal.cuh"
 
 #include <algorithm>
@@ -28,30 +37,30 @@
 namespace psr {
 
 constexpr int kSlotsR = 28;
-constexpr int kPad = 32;
+constexpr int kIdxSlots = 32;  // neighbour index rows: slots 0..26, own index at 27, padding
+constexpr int kPad = 32;       // one 128-byte line per slice counter
+constexpr int kRelaxThreads = 512;
 
 struct StripLevel {
-  int n;          // 2^depth (slices 0..n)
-  int strips;     // NS (per slice; boundaries balance the rows)
-  const int32_t* bounds;     // [(n+1)*(NS+1)] x boundaries of the strips of each slice
-  int iters;
-  int cap;        // footprint capacity (elements) per CTA
-  int use_scratch;
-  int row_cap;    // update rows staged in shared memory per task (0: read rows from global)
-  const int32_t* cols;       // schedule positions, slot k = lexicographic neighbour k, -1 absent
-  const void* vals;          // T[rows*28]
-  const void* b;             // V[rows]
+  int n;                 // 2^depth (slices 0..n)
+  int strips;            // strips per slice
+  int nvisits;
+  int cap;               // footprint capacity (elements) per CTA
+  int row_cap;           // staged update rows per task
+  int b_cap;             // staged right-hand-side elements per task
+  const int32_t* bounds;     // [(n+1)*(strips+1)] x boundaries of the strips of each slice
+  const int32_t* group_off;  // [4(n+1)+1] schedule position of each (slice, colour) group
+  const void* vals;          // T[rows*28]   schedule order
+  const void* nidx;          // I[rows*32]   neighbour index within its group, -1 absent; [27] = own
+  const void* b;             // V[rows + slack]
   void* xb0;                 // V[rows]  even visits
   void* xb1;                 // V[rows]  odd visits (holds the initial x)
-  const int64_t* keys;       // schedule order
   const int32_t* xstart;     // [(n+1)*4][n+2]: first position of group (z,c) with x >= X
-  const int2* visits;        // slice-visits (z, t) in the sequential order
-  int nvisits;
-  int* done;                 // completed strip tasks of slice z at done[z * kPad] (one 128-byte line each)
-  long long* trace;          // optional: 8 timestamps per task (PSR_RELAX_TRACE_FILE)
+  const int2* visits;        // slice-visits (z, t) in wave order
+  int* done;                 // completed strip tasks of slice z at done[z * kPad]
   int* counter;
   int* error;
-  void* scratch;             // V[grid*cap] when use_scratch
+  long long* trace;          // optional: 8 timestamps per task
 };
 
 __device__ __forceinline__ long long globaltimer() {
@@ -60,7 +69,7 @@ __device__ __forceinline__ long long globaltimer() {
   return t;
 }
 
-__device__ __forceinline__ int ld_acquire_r(const int* p) {
+__device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
   asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
@@ -68,66 +77,142 @@ __device__ __forceinline__ int ld_acquire_r(const int* p) {
 
 __device__ __forceinline__ bool wait_at_least(const int* p, int v, const int* error) {
   for (long long it = 0; it < (1LL << 26); ++it) {
-    if (ld_acquire_r(p) >= v) return true;
+    if (ld_acquire(p) >= v) return true;
     if ((it & 63) == 63 && *(volatile const int*)error) return false;
     __nanosleep(it < 512 ? 32 : 256);
   }
   return false;
 }
 
-// All 28 slots of a row with 16-byte loads (rows are 16-byte aligned: 28 * 4 or 28 * 8 bytes).
-__device__ __forceinline__ void load_row(const float* src, float out[kSlotsR]) {
-  const float4* v = reinterpret_cast<const float4*>(src);
-#pragma unroll
-  for (int q = 0; q < kSlotsR / 4; ++q) {
-    float4 w = __ldg(v + q);
-    out[4 * q] = w.x;
-    out[4 * q + 1] = w.y;
-    out[4 * q + 2] = w.z;
-    out[4 * q + 3] = w.w;
-  }
+// ---- mbarrier and 1-D bulk copy (global -> shared), no multicast
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-__device__ __forceinline__ void load_row(const double* src, double out[kSlotsR]) {
-  const double2* v = reinterpret_cast<const double2*>(src);
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+// Bounded wait for the phase with the given parity; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (long long it = 0; it < (1LL << 26); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Footprint range (j * 4 + colour) of slot k for a row of colour C: slice z-1+(k%3),
+// colour of (x + k/9 - 1, y + (k/3)%3 - 1).
+template <int C>
+__device__ __forceinline__ constexpr int slot_range(int k) {
+  return (k % 3) * 4 + (((C & 1) + k / 9 + 1) & 1) + 2 * (((C >> 1) + (k / 3) % 3 + 1) & 1);
+}
+
+template <class T>
+__device__ __forceinline__ void load_vals(const T* src, T out[kSlotsR]) {
+  const int4* s = reinterpret_cast<const int4*>(src);
+  int4* d = reinterpret_cast<int4*>(out);
 #pragma unroll
-  for (int q = 0; q < kSlotsR / 2; ++q) {
-    double2 w = __ldg(v + q);
-    out[2 * q] = w.x;
-    out[2 * q + 1] = w.y;
+  for (int q = 0; q < kSlotsR * int(sizeof(T)) / 16; ++q) d[q] = s[q];
+}
+template <class I>
+__device__ __forceinline__ void load_idx(const I* src, I out[kIdxSlots]) {
+  const int4* s = reinterpret_cast<const int4*>(src);
+  int4* d = reinterpret_cast<int4*>(out);
+#pragma unroll
+  for (int q = 0; q < kIdxSlots * int(sizeof(I)) / 16; ++q) d[q] = s[q];
+}
+
+// One row of colour C: r = b - sum_k x_k A_k in slot order; x_self += r / A_self.
+// A neighbour index outside the staged footprint (only possible for an operator whose slot
+// k is not the k-th neighbour) is reported through `error` and not accessed.
+template <int C, class T, class V, class I>
+__device__ __forceinline__ void update_row(const I* nrow, const T* arow, V bv, V* foot, const int* delta,
+                                           unsigned total, int* error) {
+  I n[kIdxSlots];
+  load_idx(nrow, n);
+  T a[kSlotsR];
+  load_vals(arow, a);
+  V xs[27];
+  bool bad = false;
+#pragma unroll
+  for (int k = 0; k < 27; ++k) {
+    unsigned fi = unsigned(int(n[k]) + delta[slot_range<C>(k)]);
+    bool ok = n[k] >= 0 && fi < total;
+    bad |= n[k] >= 0 && fi >= total;
+    xs[k] = ok ? foot[fi] : V(0);
+  }
+  V r = bv;
+#pragma unroll
+  for (int k = 0; k < 27; ++k)
+    if (n[k] >= 0) r = r - xs[k] * V(a[k]);
+  unsigned self = unsigned(int(n[27]) + delta[4 + C]);
+  bad |= self >= total;
+  if (bad) {
+    atomicExch(error, 3);
+    return;
+  }
+  if (n[13] >= 0 && a[13] != T(0)) foot[self] = xs[13] + r * (V(1.0) / V(a[13]));
+}
+
+template <int C, class T, class V, class I>
+__device__ __forceinline__ void phase(const StripLevel& L, bool staged, int p0, int p1, int rbase, int bshift,
+                                      const I* s_idx, const T* s_vals, const V* s_b, V* foot, const int* delta,
+                                      unsigned total) {
+  const I* gidx = reinterpret_cast<const I*>(L.nidx);
+  const T* gvals = reinterpret_cast<const T*>(L.vals);
+  const V* gb = reinterpret_cast<const V*>(L.b);
+  for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+    if (staged) {
+      int i = rbase + (p - p0);
+      update_row<C>(s_idx + int64_t(i) * kIdxSlots, s_vals + int64_t(i) * kSlotsR, s_b[bshift + (p - p0)], foot,
+                    delta, total, L.error);
+    } else {
+      update_row<C>(gidx + int64_t(p) * kIdxSlots, gvals + int64_t(p) * kSlotsR, gb[p], foot, delta, total, L.error);
+    }
   }
 }
 
-// Range r of a flattened index i (bases ascending, count entries + a final total).
-__device__ __forceinline__ int range_of(const int* base, int count, int i) {
-  int r = 0;
-  while (r + 1 < count && base[r + 1] <= i) ++r;
-  return r;
-}
-
-template <class T, class V>
-__global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  // Per task: footprint ranges (j = slice z-1+j, colour c), update ranges (colour c, halo
-  // 3-c) and own ranges (colour c, no halo), all as schedule positions.
-  __shared__ int s_task, s_fail, s_total, s_rows;
-  __shared__ int s_lo[12], s_hi[12], s_base[13];
-  __shared__ int s_p0[4], s_p1[4], s_rbase[5], s_o0[4], s_o1[4], s_obase[5];
-  const T* __restrict__ vals = reinterpret_cast<const T*>(L.vals);
-  const V* __restrict__ b = reinterpret_cast<const V*>(L.b);
+template <class T, class V, class I>
+__global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t s_bar;
+  __shared__ int s_task, s_fail, s_total, s_rows, s_staged;
+  __shared__ int s_lo[12], s_hi[12], s_base[13], s_delta[12];
+  __shared__ int s_p0[4], s_p1[4], s_rbase[5], s_bshift[4], s_o0[4], s_o1[4];
+  // Shared layout (each part 16-byte aligned): footprint V[cap] | values T[row_cap*28] |
+  // neighbour indices I[row_cap*32] | right-hand side V[b_cap].
+  V* foot = reinterpret_cast<V*>(smem_raw);
+  const int64_t fp_bytes = (int64_t(L.cap) * sizeof(V) + 15) & ~int64_t(15);
+  T* s_vals = reinterpret_cast<T*>(smem_raw + fp_bytes);
+  I* s_idx = reinterpret_cast<I*>(smem_raw + fp_bytes + int64_t(L.row_cap) * kSlotsR * sizeof(T));
+  V* s_b = reinterpret_cast<V*>(smem_raw + fp_bytes +
+                                int64_t(L.row_cap) * (kSlotsR * sizeof(T) + kIdxSlots * sizeof(I)));
+  const T* gvals = reinterpret_cast<const T*>(L.vals);
+  const I* gidx = reinterpret_cast<const I*>(L.nidx);
+  const V* gb = reinterpret_cast<const V*>(L.b);
   V* xb0 = reinterpret_cast<V*>(L.xb0);
   V* xb1 = reinterpret_cast<V*>(L.xb1);
-  V* foot = L.use_scratch ? reinterpret_cast<V*>(L.scratch) + int64_t(blockIdx.x) * L.cap
-                          : reinterpret_cast<V*>(smem_raw);
-  // Staged rows (tasks with at most L.row_cap update rows): operator values, footprint
-  // indices of the 27 neighbours (-1 absent), b and the row's own footprint index.
-  unsigned char* rows_raw = smem_raw + (L.use_scratch ? 0 : ((int64_t(L.cap) * sizeof(V) + 15) & ~int64_t(15)));
-  // Layout (every part 16-byte aligned): values T[28] per row (112 or 224 bytes), footprint
-  // indices int16[32] per row (64 bytes: slots 0..26, the row itself at 27, padding), b.
-  T* r_vals = reinterpret_cast<T*>(rows_raw);
-  int16_t* r_fidx = reinterpret_cast<int16_t*>(rows_raw + int64_t(L.row_cap) * kSlotsR * sizeof(T));
-  V* r_b = reinterpret_cast<V*>(rows_raw + int64_t(L.row_cap) * (kSlotsR * sizeof(T) + 64));
   const int nx = L.n + 2;
   const int total_tasks = L.nvisits * L.strips;
+  constexpr int per16 = 16 / int(sizeof(V));  // right-hand-side elements per 16 bytes
+  uint32_t parity = 0;
+  if (threadIdx.x == 0) mbar_init(&s_bar);
+  __syncthreads();
   while (true) {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -182,77 +267,56 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
       for (int r = 0; r < 12; ++r) {
         s_base[r] = total;
         total += s_hi[r] - s_lo[r];
+        int j = r >> 2, c = r & 3, zz = z + j - 1;
+        int gstart = (zz >= 0 && zz <= L.n) ? L.group_off[zz * 4 + c] : 0;
+        s_delta[r] = s_base[r] + gstart - s_lo[r];
       }
       s_base[12] = total;
       s_total = total;
-      int rows = 0, owns = 0;
+      int rows = 0, bsum = 0;
       for (int c = 0; c < 4; ++c) {
         s_rbase[c] = rows;
         rows += s_p1[c] - s_p0[c];
-        s_obase[c] = owns;
-        owns += s_o1[c] - s_o0[c];
+        int a0 = s_p0[c] - s_p0[c] % per16, a1 = (s_p1[c] + per16 - 1) / per16 * per16;
+        s_bshift[c] = bsum + (s_p0[c] - a0);
+        bsum += s_p1[c] > s_p0[c] ? a1 - a0 : 0;
       }
       s_rbase[4] = rows;
-      s_obase[4] = owns;
       s_rows = rows;
       if (total > L.cap) {
         atomicExch(L.error, 2);
         s_fail = 1;
       }
-    }
-    __syncthreads();
-    if (s_fail) return;
-    // Stage the update rows' data before waiting (it does not depend on x) when it fits.
-    const bool staged = s_rows <= L.row_cap && s_total < 32768;
-    if (staged) {
-      for (int i = threadIdx.x; i < s_rows; i += blockDim.x) {
-        int c = range_of(s_rbase, 4, i);
-        int p = s_p0[c] + (i - s_rbase[c]);
-        const int4* vs = reinterpret_cast<const int4*>(vals + int64_t(p) * kSlotsR);
-        int4* vd = reinterpret_cast<int4*>(r_vals + int64_t(i) * kSlotsR);
-#pragma unroll
-        for (int q = 0; q < kSlotsR * int(sizeof(T)) / 16; ++q) vd[q] = __ldg(vs + q);
-        r_b[i] = __ldg(b + p);
-        int64_t key = __ldg(L.keys + p);
-        int px = int((key >> 32) & 65535), py = int((key >> 16) & 65535);
-        const int4* cr = reinterpret_cast<const int4*>(L.cols + int64_t(p) * kSlotsR);
-        int cw[kSlotsR];
-#pragma unroll
-        for (int q = 0; q < kSlotsR / 4; ++q) {
-          int4 w = __ldg(cr + q);
-          cw[4 * q] = w.x;
-          cw[4 * q + 1] = w.y;
-          cw[4 * q + 2] = w.z;
-          cw[4 * q + 3] = w.w;
+      s_staged = !s_fail && rows <= L.row_cap && bsum <= L.b_cap;
+      if (s_staged) {
+        // Operator rows do not depend on x: copy them while the dependencies are pending.
+        fence_proxy_async();
+        uint32_t bytes = 0;
+        for (int c = 0; c < 4; ++c) {
+          int cnt = s_p1[c] - s_p0[c];
+          if (cnt <= 0) continue;
+          bytes += uint32_t(cnt) * (kSlotsR * sizeof(T) + kIdxSlots * sizeof(I));
+          int a0 = s_p0[c] - s_p0[c] % per16, a1 = (s_p1[c] + per16 - 1) / per16 * per16;
+          bytes += uint32_t(a1 - a0) * sizeof(V);
         }
-        int16_t f[32];
-        bool bad = false;
-#pragma unroll
-        for (int k = 0; k < 27; ++k) {
-          int fi = -1;
-          if (cw[k] >= 0) {
-            int rr = (k % 3) * 4 + ((px + k / 9 - 1) & 1) + 2 * ((py + (k / 3) % 3 - 1) & 1);
-            fi = s_base[rr] + (cw[k] - s_lo[rr]);
-            if (fi < 0 || fi >= s_base[12]) {  // not the k-th neighbour: malformed operator
-              bad = true;
-              fi = -1;
-            }
-          }
-          f[k] = int16_t(fi);
+        mbar_expect_tx(&s_bar, bytes);
+        int bpos = 0;
+        for (int c = 0; c < 4; ++c) {
+          int cnt = s_p1[c] - s_p0[c];
+          if (cnt <= 0) continue;
+          int p0 = s_p0[c];
+          bulk_copy(s_vals + int64_t(s_rbase[c]) * kSlotsR, gvals + int64_t(p0) * kSlotsR,
+                    uint32_t(cnt) * kSlotsR * sizeof(T), &s_bar);
+          bulk_copy(s_idx + int64_t(s_rbase[c]) * kIdxSlots, gidx + int64_t(p0) * kIdxSlots,
+                    uint32_t(cnt) * kIdxSlots * sizeof(I), &s_bar);
+          int a0 = p0 - p0 % per16, a1 = (s_p1[c] + per16 - 1) / per16 * per16;
+          bulk_copy(s_b + bpos, gb + a0, uint32_t(a1 - a0) * sizeof(V), &s_bar);
+          bpos += a1 - a0;
         }
-        f[27] = int16_t(s_base[4 + c] + (p - s_lo[4 + c]));  // the row itself
-        f[28] = f[29] = f[30] = f[31] = -1;
-        int4* fd = reinterpret_cast<int4*>(r_fidx + int64_t(i) * 32);
-        const int4* fs = reinterpret_cast<const int4*>(f);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) fd[q] = fs[q];
-        if (bad) atomicExch(L.error, 3);
       }
-    }
-    if (tr) tr[1] = globaltimer();
-    if (threadIdx.x == 0) {
-      bool ok = true;
-      if (z + 1 <= L.n) ok = wait_at_least(L.done + (z + 1) * kPad, (t + 1) * L.strips, L.error);
+      if (tr) tr[1] = globaltimer();
+      bool ok = !s_fail;
+      if (ok && z + 1 <= L.n) ok = wait_at_least(L.done + (z + 1) * kPad, (t + 1) * L.strips, L.error);
       if (ok && z > 0) ok = wait_at_least(L.done + (z - 1) * kPad, t * L.strips, L.error);
       if (ok) ok = wait_at_least(L.done + z * kPad, t * L.strips, L.error);
       if (!ok) {
@@ -262,10 +326,13 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
       if (tr) tr[2] = globaltimer();
     }
     __syncthreads();
-    if (s_fail) return;
+    const bool staged = s_staged;
+    if (s_fail) {
+      if (staged) mbar_wait(&s_bar, parity);  // never leave with copies in flight
+      return;
+    }
     if (tr) tr[3] = globaltimer();
     // Stage the footprint: slice z+1 after visit t, slices z and z-1 after visit t-1.
-    // One warp per contiguous range.
     {
       const V* cur = (t & 1) ? xb1 : xb0;
       const V* prev = (t & 1) ? xb0 : xb1;
@@ -285,94 +352,25 @@ __global__ void __launch_bounds__(256) strip_gs_kernel(StripLevel L) {
         }
       }
     }
+    if (staged && !mbar_wait(&s_bar, parity)) {
+      if (threadIdx.x == 0) atomicExch(L.error, 4);
+      return;
+    }
+    if (staged) parity ^= 1;
     __syncthreads();
     if (tr) tr[4] = globaltimer();
-    // Colour phases on the staged footprint (halo 3-c).
-    for (int c = 0; c < 4; ++c) {
-      const int p0 = s_p0[c], p1 = s_p1[c], rb = s_rbase[c];
-      for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
-        T diagonal = T(0);
-        V xi = V(0);
-        int self;
-        if (staged) {
-          // Staged row: 27 independent shared-memory loads, then the ordered subtraction.
-          int i = rb + (p - p0);
-          int16_t fd[32];
-          {
-            const int4* fs = reinterpret_cast<const int4*>(r_fidx + int64_t(i) * 32);
-            int4* fl = reinterpret_cast<int4*>(fd);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) fl[q] = fs[q];
-          }
-          T aa[kSlotsR];
-          {
-            const int4* vs = reinterpret_cast<const int4*>(r_vals + int64_t(i) * kSlotsR);
-            int4* vl = reinterpret_cast<int4*>(aa);
-#pragma unroll
-            for (int q = 0; q < kSlotsR * int(sizeof(T)) / 16; ++q) vl[q] = vs[q];
-          }
-          V xs[27];
-#pragma unroll
-          for (int k = 0; k < 27; ++k) {
-            int fi = fd[k];
-            xs[k] = fi >= 0 ? foot[fi] : V(0);
-          }
-          V r = r_b[i];
-#pragma unroll
-          for (int k = 0; k < 27; ++k)
-            if (fd[k] >= 0) r = r - xs[k] * V(aa[k]);
-          if (fd[13] >= 0) {
-            diagonal = aa[13];
-            xi = xs[13];
-          }
-          self = fd[27];
-          if (diagonal != T(0)) foot[self] = xi + r * (V(1.0) / V(diagonal));
-          continue;
-        }
-        int cc[kSlotsR];
-        T aa[kSlotsR];
-        V r;
-        int px, py;
-        {
-          const int4* cr = reinterpret_cast<const int4*>(L.cols + int64_t(p) * kSlotsR);
-#pragma unroll
-          for (int q = 0; q < kSlotsR / 4; ++q) {
-            int4 w = __ldg(cr + q);
-            cc[4 * q] = w.x;
-            cc[4 * q + 1] = w.y;
-            cc[4 * q + 2] = w.z;
-            cc[4 * q + 3] = w.w;
-          }
-          load_row(vals + int64_t(p) * kSlotsR, aa);
-          r = __ldg(b + p);
-          int64_t key = __ldg(L.keys + p);
-          px = int((key >> 32) & 65535);
-          py = int((key >> 16) & 65535);
-        }
-        self = s_base[4 + c] + (p - s_lo[4 + c]);
-#pragma unroll
-        for (int k = 0; k < 27; ++k) {
-          if (cc[k] < 0) continue;
-          int dx = k / 9 - 1, dy = (k / 3) % 3 - 1, j = k % 3;
-          int cn = ((px + dx) & 1) + 2 * ((py + dy) & 1);
-          int rr = j * 4 + cn;
-          int fi = s_base[rr] + (cc[k] - s_lo[rr]);
-          if (fi < 0 || fi >= s_total) {  // not the k-th neighbour: malformed operator
-            atomicExch(L.error, 3);
-            continue;
-          }
-          V xn = foot[fi];
-          T a = aa[k];
-          r = r - xn * V(a);
-          if (k == 13) {
-            diagonal = a;
-            xi = xn;
-          }
-        }
-        if (diagonal != T(0)) foot[self] = xi + r * (V(1.0) / V(diagonal));
-      }
-      __syncthreads();
-    }
+    phase<0, T, V, I>(L, staged, s_p0[0], s_p1[0], s_rbase[0], s_bshift[0], s_idx, s_vals, s_b, foot, s_delta,
+                        unsigned(s_total));
+    __syncthreads();
+    phase<1, T, V, I>(L, staged, s_p0[1], s_p1[1], s_rbase[1], s_bshift[1], s_idx, s_vals, s_b, foot, s_delta,
+                        unsigned(s_total));
+    __syncthreads();
+    phase<2, T, V, I>(L, staged, s_p0[2], s_p1[2], s_rbase[2], s_bshift[2], s_idx, s_vals, s_b, foot, s_delta,
+                        unsigned(s_total));
+    __syncthreads();
+    phase<3, T, V, I>(L, staged, s_p0[3], s_p1[3], s_rbase[3], s_bshift[3], s_idx, s_vals, s_b, foot, s_delta,
+                        unsigned(s_total));
+    __syncthreads();
     if (tr) tr[5] = globaltimer();
     // Publish the strip's own rows (x in [x0, x1)) as visit t.
     {
@@ -413,7 +411,7 @@ __global__ void xstart_kernel(const int64_t* skeys, const int32_t* group_off, in
   xstart[idx] = lo;
 }
 
-// Row-balanced strip boundaries: slice z's rows split into NS runs of x of about equal size.
+// Row-balanced strip boundaries: slice z's rows split into `strips` runs of x of about equal size.
 __global__ void strip_bounds_kernel(const int32_t* xstart, int n, int strips, int32_t* bounds) {
   int z = blockIdx.x * blockDim.x + threadIdx.x;
   if (z > n) return;
@@ -432,18 +430,23 @@ __global__ void strip_bounds_kernel(const int32_t* xstart, int n, int strips, in
   out[strips] = n + 1;
 }
 
-__global__ void footprint_kernel(const int32_t* xstart, const int32_t* bounds, int n, int strips, int* maxfp) {
+// Largest footprint, update-row count and staged right-hand-side span over all tasks.
+__global__ void footprint_kernel(const int32_t* xstart, const int32_t* bounds, int n, int strips, int per16,
+                                 int* caps) {
   int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (n + 1) * strips) return;
   int z = idx / strips, s = idx % strips, nx = n + 2;
   int x0 = bounds[z * (strips + 1) + s], x1 = bounds[z * (strips + 1) + s + 1];
-  int rows = 0;
+  int rows = 0, bspan = 0;
   for (int c = 0; c < 4; ++c) {
     const int32_t* xs = xstart + int64_t(z * 4 + c) * nx;
     int h = 3 - c;
-    rows += xs[min(x1 + h, n + 1)] - xs[max(min(x0 - h, n + 1), 0)];
+    int p0 = xs[max(min(x0 - h, n + 1), 0)], p1 = xs[min(x1 + h, n + 1)];
+    rows += p1 - p0;
+    if (p1 > p0) bspan += (p1 + per16 - 1) / per16 * per16 - (p0 - p0 % per16);
   }
-  atomicMax(maxfp + 1, rows);
+  atomicMax(caps + 1, rows);
+  atomicMax(caps + 2, bspan);
   int total = 0;
   for (int j = -1; j <= 1; ++j) {
     int zz = z + j;
@@ -453,7 +456,7 @@ __global__ void footprint_kernel(const int32_t* xstart, const int32_t* bounds, i
       total += xs[min(x1 + 4, n + 1)] - xs[max(x0 - 4, 0)];
     }
   }
-  atomicMax(maxfp, total);
+  atomicMax(caps, total);
 }
 
 __global__ void inverse_kernel(const int32_t* perm, int64_t n, int32_t* inv) {
@@ -461,19 +464,30 @@ __global__ void inverse_kernel(const int32_t* perm, int64_t n, int32_t* inv) {
   if (p < n) inv[perm[p]] = int32_t(p);
 }
 
-// Gathers an ELL operator (key order) into schedule order, columns as schedule positions.
-template <class T, class V>
-__global__ void reorder_kernel(const int32_t* perm, const int32_t* inv, int64_t n, const int32_t* cols, const T* vals,
-                               const V* b, const V* x, const int64_t* keys, int32_t* scols, T* svals, V* sb, V* sx,
-                               int64_t* skeys) {
+__device__ __forceinline__ int group_of(int64_t key) {
+  int c[3];
+  key_coords(key, c);
+  return 4 * c[2] + (c[0] & 1) + 2 * (c[1] & 1);
+}
+
+// Gathers a slot-ELL operator (key order) into schedule order; neighbours become indices
+// inside their (slice, colour) group.
+template <class T, class V, class I>
+__global__ void reorder_kernel(const int32_t* perm, const int32_t* inv, const int32_t* group_off, int64_t n,
+                               const int32_t* cols, const T* vals, const V* b, const V* x, const int64_t* keys,
+                               I* sidx, T* svals, V* sb, V* sx, int64_t* skeys) {
   int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (p >= n) return;
   int64_t row = perm[p];
   for (int k = 0; k < kSlotsR; ++k) {
-    int32_t c = cols[row * kSlotsR + k];
-    scols[p * kSlotsR + k] = c >= 0 ? inv[c] : -1;
-    svals[p * kSlotsR + k] = vals[row * kSlotsR + k];
+    int32_t c = k < 27 ? cols[row * kSlotsR + k] : -1;
+    int32_t idx = -1;
+    if (c >= 0) idx = inv[c] - group_off[group_of(keys[c])];
+    svals[p * kSlotsR + k] = k < 27 ? vals[row * kSlotsR + k] : T(0);
+    sidx[p * kIdxSlots + k] = I(idx);
   }
+  sidx[p * kIdxSlots + 27] = I(p - group_off[group_of(keys[row])]);
+  for (int k = 28; k < kIdxSlots; ++k) sidx[p * kIdxSlots + k] = I(-1);
   sb[p] = b[row];
   sx[p] = x[row];
   skeys[p] = keys[row];
@@ -488,9 +502,7 @@ __global__ void scatter_back_kernel(const int32_t* perm, int64_t n, const V* sx,
 __global__ void slice_groups_kernel(const int64_t* keys, int64_t n, uint32_t* groups, int32_t* ids) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
-  int c[3];
-  key_coords(keys[i], c);
-  groups[i] = uint32_t((c[0] & 1) + 2 * (c[1] & 1) + 4 * c[2]);
+  groups[i] = uint32_t(group_of(keys[i]));
   ids[i] = int32_t(i);
 }
 
@@ -508,6 +520,11 @@ __global__ void group_bounds_kernel(const uint32_t* sorted, int64_t n, int count
   off[g] = int32_t(lo);
 }
 
+__global__ void max_group_kernel(const int32_t* off, int count, int* out) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < count) atomicMax(out, off[g + 1] - off[g]);
+}
+
 static int device_sms() {
   static int count = 0;
   if (!count) {
@@ -516,6 +533,135 @@ static int device_sms() {
     PSR_CUDA(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev));
   }
   return count;
+}
+
+static int device_smem_optin() {
+  static int bytes = 0;
+  if (!bytes) {
+    int dev = 0;
+    PSR_CUDA(cudaGetDevice(&dev));
+    PSR_CUDA(cudaDeviceGetAttribute(&bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  }
+  return bytes;
+}
+
+template <class T, class V, class I>
+static void run_strips(const int64_t* keys, int64_t rows, int depth, const int32_t* cols, const T* vals, const V* b,
+                       V* x, int iters, cudaStream_t s, float* ms, const int32_t* perm, const int32_t* inv,
+                       const int32_t* off) {
+  const int n = 1 << depth;
+  const int nx = n + 2;
+  const int per16 = 16 / int(sizeof(V));
+  DBuf<I> sidx(kIdxSlots * rows, s);
+  DBuf<T> svals(kSlotsR * rows, s);
+  DBuf<V> sb(rows + 2 * per16, s), x0(rows, s), x1(rows, s);
+  DBuf<int64_t> skeys(rows, s);
+  sb.zero();
+  reorder_kernel<T, V, I><<<blocks_for(rows), kThreads, 0, s>>>(perm, inv, off, rows, cols, vals, b, x, keys, sidx.p,
+                                                               svals.p, sb.p, x1.p, skeys.p);
+  PSR_LAUNCH_CHECK();
+  DBuf<int32_t> xstart(int64_t(n + 1) * 4 * nx, s);
+  xstart_kernel<<<blocks_for(int64_t(n + 1) * 4 * nx), kThreads, 0, s>>>(skeys.p, off, n, xstart.p);
+  PSR_LAUNCH_CHECK();
+  // Strips per slice: about two waves of tasks (iters x strips each) per persistent grid,
+  // at least ~128 rows per strip.
+  const int sms = device_sms();
+  int strips = int(std::max<int64_t>(
+      1, std::min<int64_t>(std::max(1, sms / (2 * iters)), rows / (int64_t(n + 1) * 128))));
+  DBuf<int32_t> bounds(int64_t(n + 1) * (strips + 1), s);
+  strip_bounds_kernel<<<blocks_for(n + 1), kThreads, 0, s>>>(xstart.p, n, strips, bounds.p);
+  PSR_LAUNCH_CHECK();
+  const int64_t pad_end = int64_t(n + 1) * kPad;
+  DBuf<int> flags(pad_end + 4 * kPad, s);
+  flags.zero();
+  int* counter = flags.p + pad_end;
+  int* error = flags.p + pad_end + kPad;
+  int* caps_dev = flags.p + pad_end + 2 * kPad;
+  footprint_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, bounds.p, n, strips, per16, caps_dev);
+  PSR_LAUNCH_CHECK();
+  std::vector<int> caps = read_vector(caps_dev, 3, s);
+  const int maxfp = caps[0], maxrows = caps[1], maxb = caps[2];
+  // Slice-visits in wave order (relaxation.py:128-143): wave q = 2t + n - z holds slices two
+  // apart; every dependency of a wave-q task lies in wave q-1 or q-2, so dequeuing by wave is
+  // deadlock-free and keeps whole waves in flight.
+  std::vector<int2> visits;
+  for (int q = 0; q <= n + 2 * (iters - 1); ++q) {
+    int first = std::max(0, (q - n + 1) / 2), last = std::min(iters - 1, q / 2);
+    for (int t = first; t <= last; ++t) visits.push_back(make_int2(n - q + 2 * t, t));
+  }
+  DBuf<int2> dvisits(int64_t(visits.size()), s);
+  PSR_CUDA(cudaMemcpyAsync(dvisits.p, visits.data(), visits.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+  StripLevel L{};
+  L.n = n;
+  L.strips = strips;
+  L.nvisits = int(visits.size());
+  L.bounds = bounds.p;
+  L.group_off = off;
+  L.vals = svals.p;
+  L.nidx = sidx.p;
+  L.b = sb.p;
+  L.xb0 = x0.p;
+  L.xb1 = x1.p;
+  L.xstart = xstart.p;
+  L.visits = dvisits.p;
+  L.done = flags.p;
+  L.counter = counter;
+  L.error = error;
+  // Shared memory: the footprint, plus the staged rows of tasks that fit.
+  const int64_t budget = std::min<int64_t>(device_smem_optin() - 4096, 220 * 1024);
+  const int64_t fp_bytes = (int64_t(std::max(maxfp, 1)) * int64_t(sizeof(V)) + 15) & ~int64_t(15);
+  if (fp_bytes > budget) throw Error(4, "ordered relaxation: a strip footprint exceeds shared memory");
+  const int64_t per_row = kSlotsR * int64_t(sizeof(T)) + kIdxSlots * int64_t(sizeof(I)) + int64_t(sizeof(V));
+  L.cap = std::max(maxfp, 1);
+  int64_t rc = std::min<int64_t>(maxrows, (budget - fp_bytes - 4 * 16) / per_row);
+  rc = std::max<int64_t>(rc, 0);
+  L.row_cap = int(rc);
+  L.b_cap = int(std::min<int64_t>(maxb, rc + 4 * per16) / per16 * per16);
+  int64_t smem = fp_bytes + rc * (kSlotsR * int64_t(sizeof(T)) + kIdxSlots * int64_t(sizeof(I))) +
+                 ((int64_t(L.b_cap) * int64_t(sizeof(V)) + 15) & ~int64_t(15));
+  smem = std::max<int64_t>(smem, 16);
+  auto kernel = strip_gs_kernel<T, V, I>;
+  PSR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  const int64_t total_tasks = int64_t(visits.size()) * strips;
+  const int grid = int(std::min<int64_t>(total_tasks, sms));
+  const char* trace_file = std::getenv("PSR_RELAX_TRACE_FILE");
+  DBuf<long long> trace;
+  if (trace_file) {
+    trace.alloc(total_tasks * 8, s);
+    trace.zero();
+    L.trace = trace.p;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ms) {
+    PSR_CUDA(cudaEventCreate(&e0));
+    PSR_CUDA(cudaEventCreate(&e1));
+    PSR_CUDA(cudaEventRecord(e0, s));
+  }
+  kernel<<<grid, kRelaxThreads, size_t(smem), s>>>(L);
+  PSR_LAUNCH_CHECK();
+  if (ms) PSR_CUDA(cudaEventRecord(e1, s));
+  scatter_back_kernel<V><<<blocks_for(rows), kThreads, 0, s>>>(perm, rows, ((iters - 1) & 1) ? x1.p : x0.p, x);
+  PSR_LAUNCH_CHECK();
+  int err = read_scalar(L.error, s);
+  if (ms) {
+    PSR_CUDA(cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  if (trace_file) {
+    std::vector<long long> h = read_vector(trace.p, total_tasks * 8, s);
+    if (FILE* f = std::fopen(trace_file, "ab")) {
+      long long header[6] = {depth, n, strips, L.row_cap, grid, total_tasks};
+      std::fwrite(header, sizeof(header), 1, f);
+      std::fwrite(visits.data(), sizeof(int2), visits.size(), f);
+      std::fwrite(h.data(), sizeof(long long), h.size(), f);
+      std::fclose(f);
+    }
+  }
+  if (err == 2) throw Error(4, "ordered relaxation: footprint exceeds its capacity");
+  if (err == 3) throw Error(1, "ordered relaxation: an operator column is not its slot's neighbour");
+  if (err == 4) throw Error(4, "ordered relaxation: a bulk copy did not complete");
+  if (err) throw Error(4, "ordered relaxation: a dependency wait timed out");
 }
 
 // Ordered sliced relaxation of one level given as slot-ELL rows in key order.  x (key
@@ -536,122 +682,15 @@ void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int
   PSR_LAUNCH_CHECK();
   inverse_kernel<<<blocks_for(rows), kThreads, 0, s>>>(perm.p, rows, inv.p);
   PSR_LAUNCH_CHECK();
-  DBuf<int32_t> scols(kSlotsR * rows, s);
-  DBuf<T> svals(kSlotsR * rows, s);
-  DBuf<V> sb(rows, s), x0(rows, s), x1(rows, s);
-  DBuf<int64_t> skeys(rows, s);
-  reorder_kernel<T, V><<<blocks_for(rows), kThreads, 0, s>>>(perm.p, inv.p, rows, cols, vals, b, x, keys, scols.p,
-                                                            svals.p, sb.p, x1.p, skeys.p);
+  DBuf<int> gmax(1, s);
+  gmax.zero();
+  max_group_kernel<<<blocks_for(groups), kThreads, 0, s>>>(off.p, groups, gmax.p);
   PSR_LAUNCH_CHECK();
-  const int nx = n + 2;
-  DBuf<int32_t> xstart(int64_t(n + 1) * 4 * nx, s);
-  xstart_kernel<<<blocks_for(int64_t(n + 1) * 4 * nx), kThreads, 0, s>>>(skeys.p, off.p, n, xstart.p);
-  PSR_LAUNCH_CHECK();
-  // Strips per slice: enough tasks per wave (iters x strips) to fill the persistent grid,
-  // at least ~96 rows per strip.
-  int strips = int(std::max<int64_t>(1, std::min<int64_t>(int64_t(2 * device_sms() + iters - 1) / iters,
-                                                          rows / (int64_t(n + 1) * 96))));
-  DBuf<int32_t> bounds(int64_t(n + 1) * (strips + 1), s);
-  strip_bounds_kernel<<<blocks_for(n + 1), kThreads, 0, s>>>(xstart.p, n, strips, bounds.p);
-  PSR_LAUNCH_CHECK();
-  const int64_t pad_end = int64_t(n + 1) * kPad;
-  DBuf<int> flags(pad_end + 4 * kPad, s);
-  flags.zero();
-  int* counter = flags.p + pad_end;
-  int* error = flags.p + pad_end + kPad;
-  int* caps_dev = flags.p + pad_end + 2 * kPad;
-  footprint_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, bounds.p, n, strips, caps_dev);
-  PSR_LAUNCH_CHECK();
-  std::vector<int> caps = read_vector(caps_dev, 2, s);
-  int maxfp = caps[0], maxrows = caps[1];
-  // Slice-visits in wave order (relaxation.py:128-143): wave q = 2t + n - z holds slices two
-  // apart; every dependency of a wave-q task lies in wave q-1 or q-2, so dequeuing by wave
-  // is deadlock-free and keeps a whole wave (up to `iters` slice-visits) in flight.
-  std::vector<int2> visits;
-  for (int q = 0; q <= n + 2 * (iters - 1); ++q) {
-    int first = std::max(0, (q - n + 1) / 2), last = std::min(iters - 1, q / 2);
-    for (int t = first; t <= last; ++t) visits.push_back(make_int2(n - q + 2 * t, t));
-  }
-  DBuf<int2> dvisits(int64_t(visits.size()), s);
-  PSR_CUDA(cudaMemcpyAsync(dvisits.p, visits.data(), visits.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
-  const int smem_cap_bytes = 110 * 1024;  // two CTAs per SM
-  StripLevel L{};
-  L.n = n;
-  L.strips = strips;
-  L.bounds = bounds.p;
-  L.iters = iters;
-  L.cols = scols.p;
-  L.vals = svals.p;
-  L.b = sb.p;
-  L.xb0 = x0.p;
-  L.xb1 = x1.p;
-  L.keys = skeys.p;
-  L.xstart = xstart.p;
-  L.visits = dvisits.p;
-  L.nvisits = int(visits.size());
-  L.done = flags.p;
-  L.counter = counter;
-  L.error = error;
-  // Shared memory: the x footprint, plus the update rows' operator data of tasks whose rows
-  // fit (other tasks read their rows from global memory).
-  const int64_t per_row = kSlotsR * int64_t(sizeof(T)) + 64 + int64_t(sizeof(V));
-  int64_t fp_bytes = (int64_t(maxfp) * int64_t(sizeof(V)) + 15) & ~int64_t(15);
-  int64_t smem = 0;
-  L.cap = std::max(maxfp, 1);
-  L.use_scratch = fp_bytes > smem_cap_bytes;
-  L.row_cap = 0;
-  if (!L.use_scratch) {
-    L.row_cap = int(std::min<int64_t>(maxrows, (smem_cap_bytes - fp_bytes) / per_row));
-    smem = std::max<int64_t>(fp_bytes + L.row_cap * per_row, 16);
-  }
-  auto kernel = strip_gs_kernel<T, V>;
-  PSR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap_bytes));
-  int per_sm = 0;
-  PSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, int(smem)));
-  int64_t total_tasks = int64_t(visits.size()) * strips;
-  int grid = int(std::min<int64_t>(total_tasks, int64_t(std::max(per_sm, 1)) * device_sms()));
-  const char* trace_file = std::getenv("PSR_RELAX_TRACE_FILE");
-  DBuf<long long> trace;
-  if (trace_file) {
-    trace.alloc(total_tasks * 8, s);
-    trace.zero();
-    L.trace = trace.p;
-  }
-  DBuf<V> scratch;
-  if (L.use_scratch) {
-    scratch.alloc(int64_t(grid) * L.cap, s);
-    L.scratch = scratch.p;
-  }
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (ms) {
-    PSR_CUDA(cudaEventCreate(&e0));
-    PSR_CUDA(cudaEventCreate(&e1));
-    PSR_CUDA(cudaEventRecord(e0, s));
-  }
-  kernel<<<grid, 256, size_t(smem), s>>>(L);
-  PSR_LAUNCH_CHECK();
-  if (ms) PSR_CUDA(cudaEventRecord(e1, s));
-  scatter_back_kernel<V><<<blocks_for(rows), kThreads, 0, s>>>(perm.p, rows, ((iters - 1) & 1) ? x1.p : x0.p, x);
-  PSR_LAUNCH_CHECK();
-  int err = read_scalar(L.error, s);
-  if (ms) {
-    PSR_CUDA(cudaEventElapsedTime(ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-  }
-  if (trace_file) {
-    std::vector<long long> h = read_vector(trace.p, total_tasks * 8, s);
-    if (FILE* f = std::fopen(trace_file, "ab")) {
-      long long header[6] = {depth, n, strips, L.row_cap, grid, total_tasks};
-      std::fwrite(header, sizeof(header), 1, f);
-      std::fwrite(visits.data(), sizeof(int2), visits.size(), f);
-      std::fwrite(h.data(), sizeof(long long), h.size(), f);
-      std::fclose(f);
-    }
-  }
-  if (err == 2) throw Error(4, "ordered relaxation: footprint exceeds its capacity");
-  if (err == 3) throw Error(1, "ordered relaxation: an operator column is not its slot's neighbour");
-  if (err) throw Error(4, "ordered relaxation: a dependency wait timed out");
+  // Group-relative neighbour indices fit 16 bits unless a (slice, colour) group is huge.
+  if (read_scalar(gmax.p, s) < 32767)
+    run_strips<T, V, int16_t>(keys, rows, depth, cols, vals, b, x, iters, s, ms, perm.p, inv.p, off.p);
+  else
+    run_strips<T, V, int32_t>(keys, rows, depth, cols, vals, b, x, iters, s, ms, perm.p, inv.p, off.p);
 }
 
 template void relax_sliced_strips<float, float>(const int64_t*, int64_t, int, const int32_t*, const float*,
