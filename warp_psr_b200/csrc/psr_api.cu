@@ -32,6 +32,26 @@ __global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, i
     h = (h + 1) & mask;
   }
 }
+
+// Column heads of sorted keys: (depth, x, y) changes.
+__global__ void column_insert_kernel(const int64_t* __restrict__ keys, int64_t n, int64_t* hkeys, int32_t* hvals,
+                                     uint64_t mask) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int64_t k = keys[i];
+  if (i > 0 && (keys[i - 1] >> 16) == (k >> 16)) return;
+  int64_t key = (k >> 16) << 16;
+  uint64_t h = HashView::mix(uint64_t(key)) & mask;
+  while (true) {
+    unsigned long long prev = atomicCAS(reinterpret_cast<unsigned long long*>(hkeys + h), ~0ULL,
+                                        static_cast<unsigned long long>(key));
+    if (prev == ~0ULL || prev == static_cast<unsigned long long>(key)) {
+      hvals[h] = int32_t(i);
+      return;
+    }
+    h = (h + 1) & mask;
+  }
+}
 }  // namespace psr
 
 struct psr_result {

@@ -207,6 +207,54 @@ struct HashMap {
   }
 };
 
+// ------------------------------------------------------------------ column index over sorted keys
+// Keys sorted by (depth, x, y, z) form contiguous z-runs per (depth, x, y) column.  The
+// column index maps a column to the position of its first key, so a box of neighbours costs
+// one probe per (x, y) column plus a short scan in z instead of one probe per key.
+struct ColumnView {
+  HashView h;
+  const int64_t* keys = nullptr;
+  int64_t n = 0;
+  __host__ __device__ static __forceinline__ int64_t column_key(int d, int x, int y) { return basis_key(d, x, y, 0); }
+  // Index of the key (d, x, y, z), or -1.
+  __device__ __forceinline__ int32_t find(int d, int x, int y, int z) const {
+    int32_t j = h.find(column_key(d, x, y));
+    if (j < 0) return -1;
+    int64_t want = basis_key(d, x, y, z), col = column_key(d, x, y) >> 16;
+    for (; j < n; ++j) {
+      int64_t k = __ldg(keys + j);
+      if ((k >> 16) != col || k > want) return -1;
+      if (k == want) return j;
+    }
+    return -1;
+  }
+};
+
+__global__ void column_insert_kernel(const int64_t* __restrict__ keys, int64_t n, int64_t* hkeys, int32_t* hvals,
+                                     uint64_t mask);
+
+struct ColumnIndex {
+  HashMap map;
+  ColumnView view_;
+  void build(const int64_t* keys, int64_t n, cudaStream_t s) {
+    map.count = n;
+    uint64_t cap = 16;
+    while (cap < uint64_t(2 * n + 1)) cap <<= 1;
+    map.mask = cap - 1;
+    map.keys.alloc(int64_t(cap), s);
+    map.vals.alloc(int64_t(cap), s);
+    PSR_CUDA(cudaMemsetAsync(map.keys.p, 0xff, cap * sizeof(int64_t), s));
+    if (n > 0) {
+      column_insert_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, map.keys.p, map.vals.p, map.mask);
+      PSR_LAUNCH_CHECK();
+    }
+    view_.h = map.view();
+    view_.keys = keys;
+    view_.n = n;
+  }
+  ColumnView view() const { return view_; }
+};
+
 // ------------------------------------------------------------------ CUB wrappers
 // Stable LSD radix sort of (key, value) pairs on key bits [0, end_bit).
 template <class K, class V>

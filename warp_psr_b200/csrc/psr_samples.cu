@@ -502,24 +502,37 @@ __global__ void normal_reduce_kernel(const uint64_t* keys, const int32_t* order,
   out_values[4 * g + 3] = -T(0);
 }
 
-// normals.py:411-425 contributions, summed in fixed 1024-item chunks (serial inside a
-// chunk, then serially over chunk totals) — the order the oracle restates.
+// normals.py:411-425 contributions (raw depth * w, splat weight * w, w) in first-index
+// order; zero for groups whose mean normal vanishes.
 template <class T>
-__global__ void average_chunks_kernel(const int32_t* order, int64_t n, const T* nsums, const T* weights, const T* dw,
-                                      T* partial) {
+__global__ void average_contrib_kernel(const int32_t* order, int64_t n, const T* nsums, const T* weights, const T* dw,
+                                       T* contrib) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int64_t src = order[i];
+  T w = weights[src];
+  T nm[3] = {nsums[3 * src] / w, nsums[3 * src + 1] / w, nsums[3 * src + 2] / w};
+  bool ok = sqrt(nm[0] * nm[0] + nm[1] * nm[1] + nm[2] * nm[2]) > T(0);
+  contrib[3 * i] = ok ? dw[2 * src] * w : T(0);
+  contrib[3 * i + 1] = ok ? dw[2 * src + 1] * w : T(0);
+  contrib[3 * i + 2] = ok ? w : T(0);
+}
+
+// Fixed 1024-item chunks summed serially (in T, input order) — the order the oracle
+// restates — then the chunk totals serially.
+template <class T>
+__global__ void average_chunks_kernel(const T* contrib, int64_t n, T* partial) {
   int64_t chunk = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   int64_t begin = chunk * 1024;
   if (begin >= n) return;
   int64_t end = begin + 1024 < n ? begin + 1024 : n;
   T part[3] = {T(0), T(0), T(0)};
   for (int64_t i = begin; i < end; ++i) {
-    int64_t src = order[i];
-    T w = weights[src];
-    T nm[3] = {nsums[3 * src] / w, nsums[3 * src + 1] / w, nsums[3 * src + 2] / w};
-    if (sqrt(nm[0] * nm[0] + nm[1] * nm[1] + nm[2] * nm[2]) > T(0) && w > T(0)) {
-      part[0] = part[0] + dw[2 * src] * w;
-      part[1] = part[1] + dw[2 * src + 1] * w;
-      part[2] = part[2] + w;
+    T c2 = contrib[3 * i + 2];
+    if (c2 > T(0)) {
+      part[0] = part[0] + contrib[3 * i];
+      part[1] = part[1] + contrib[3 * i + 1];
+      part[2] = part[2] + c2;
     }
   }
   for (int a = 0; a < 3; ++a) partial[3 * chunk + a] = part[a];
@@ -583,9 +596,11 @@ NormalData<T> build_normals(const SampleGroups<T>& g, const DensityData<T>& D, i
     PSR_LAUNCH_CHECK();
   }
   int64_t chunks = (n + 1023) / 1024;
-  DBuf<T> partial(3 * chunks, s);
-  average_chunks_kernel<T><<<blocks_for(chunks, 128), 128, 0, s>>>(order.p, n, g.normal_sums.p, g.weights.p, D.dw.p,
-                                                                  partial.p);
+  DBuf<T> partial(3 * chunks, s), contrib(3 * n, s);
+  average_contrib_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(order.p, n, g.normal_sums.p, g.weights.p, D.dw.p,
+                                                               contrib.p);
+  PSR_LAUNCH_CHECK();
+  average_chunks_kernel<T><<<blocks_for(chunks, 64), 64, 0, s>>>(contrib.p, n, partial.p);
   PSR_LAUNCH_CHECK();
   N.average.alloc(3, s);
   average_finish_kernel<T><<<1, 32, 0, s>>>(partial.p, chunks, N.average.p);

@@ -102,10 +102,44 @@ __global__ void normal_table_kernel(int test_depth, int normal_depth, int first,
                     table + (i * width + k) * 2);
 }
 
+// Columns of the 27 neighbours q = ctr + (dx, dy, dz) at depth d (slot order), found with
+// one column probe per (dx, dy) and a scan over three consecutive z.
+__device__ __forceinline__ uint32_t neighbours27(const ColumnView& cv, int d, const int ctr[3], int64_t off,
+                                                 int32_t col[27]) {
+  const int lim = 1 << d;
+  uint32_t present = 0;
+#pragma unroll
+  for (int k = 0; k < 27; ++k) col[k] = -1;
+  for (int dx = 0; dx < 3; ++dx) {
+    int qx = ctr[0] + dx - 1;
+    if (qx < 0 || qx > lim) continue;
+    for (int dy = 0; dy < 3; ++dy) {
+      int qy = ctr[1] + dy - 1;
+      if (qy < 0 || qy > lim) continue;
+      int32_t j = cv.h.find(ColumnView::column_key(d, qx, qy));
+      if (j < 0) continue;
+      int64_t colk = ColumnView::column_key(d, qx, qy) >> 16;
+      int z0 = ctr[2] - 1;
+      for (; j < cv.n; ++j) {
+        int64_t key = __ldg(cv.keys + j);
+        if ((key >> 16) != colk) break;
+        int dz = int(key & 65535) - z0;
+        if (dz > 2) break;
+        if (dz >= 0) {
+          int k = dx * 9 + dy * 3 + dz;
+          col[k] = int32_t(j - off);
+          present |= 1u << k;
+        }
+      }
+    }
+  }
+  return present;
+}
+
 // ------------------------------------------------------------------ A6 normal loads (normal_stencils.py:210-260)
 // `nvals` are 4-wide normal coefficients indexed by (hash result - noff).
 template <class T>
-__global__ void normal_stencil_kernel(const int64_t* keys, int64_t n, int test_depth, int normal_depth, HashView nh,
+__global__ void normal_stencil_kernel(const int64_t* keys, int64_t n, int test_depth, int normal_depth, ColumnView cv,
                                       int64_t noff, const T* nvals, const double* table, int width, int first,
                                       double* out) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
@@ -115,6 +149,7 @@ __global__ void normal_stencil_kernel(const int64_t* keys, int64_t n, int test_d
   int ctr[3] = {normal_center(c[0], test_depth, normal_depth), normal_center(c[1], test_depth, normal_depth),
                 normal_center(c[2], test_depth, normal_depth)};
   int lim = 1 << normal_depth;
+  int z0 = ctr[2] + first;
   double value = 0.0;
   for (int x = 0; x < width; ++x) {
     int nx = ctr[0] + x + first;
@@ -123,12 +158,16 @@ __global__ void normal_stencil_kernel(const int64_t* keys, int64_t n, int test_d
     for (int y = 0; y < width; ++y) {
       int ny = ctr[1] + y + first;
       if (ny < 0 || ny >= lim) continue;
+      int32_t j = cv.h.find(ColumnView::column_key(normal_depth, nx, ny));
+      if (j < 0) continue;
       const double* iy = table + (c[1] * width + y) * 2;
-      for (int z = 0; z < width; ++z) {
-        int nz = ctr[2] + z + first;
-        if (nz < 0 || nz >= lim) continue;
-        int32_t j = nh.find(basis_key(normal_depth, nx, ny, nz));
-        if (j < 0) continue;
+      int64_t colk = ColumnView::column_key(normal_depth, nx, ny) >> 16;
+      for (; j < cv.n; ++j) {  // ascending z: the reference's innermost loop order
+        int64_t key = __ldg(cv.keys + j);
+        if ((key >> 16) != colk) break;
+        int z = int(key & 65535) - z0;
+        if (z >= width) break;
+        if (z < 0 || int(key & 65535) >= lim) continue;
         const double* iz = table + (c[2] * width + z) * 2;
         const T* v = nvals + 4 * (int64_t(j) - noff);
         value += double(v[0]) * ix[1] * iy[0] * iz[0];
@@ -175,23 +214,23 @@ __global__ void prolong_normals_kernel(const int64_t* keys, int64_t n, int d, Ha
 // next[i] = (P^T finer)[i] + next[i] over the 27 fine neighbours 2c+{-1,0,1}^3 (the
 // transposed trilinear prolongation, ascending fine index), with weights rounded in T.
 template <class T, class V>
-__global__ void restrict_add_kernel(const int64_t* coarse_keys, int64_t n, int d /*fine depth*/, HashView bh,
+__global__ void restrict_add_kernel(const int64_t* coarse_keys, int64_t n, int d /*fine depth*/, ColumnView cv,
                                     int64_t fine_off, const V* finer, V* next, bool accumulate) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   int c[3];
   key_coords(coarse_keys[i], c);
-  int lim = 1 << d;
+  int ctr[3] = {2 * c[0], 2 * c[1], 2 * c[2]};
+  int32_t col[27];
+  uint32_t present = neighbours27(cv, d, ctr, fine_off, col);
   V s = V(0);
   for (int k = 0; k < 27; ++k) {
-    int f[3] = {2 * c[0] + k / 9 - 1, 2 * c[1] + (k / 3) % 3 - 1, 2 * c[2] + k % 3 - 1};
-    if (dmin(f[0], dmin(f[1], f[2])) < 0 || dmax(f[0], dmax(f[1], f[2])) > lim) continue;
-    int32_t g = bh.find(basis_key(d, f[0], f[1], f[2]));
-    if (g < 0) continue;
+    if (!((present >> k) & 1)) continue;
+    int f[3] = {ctr[0] + k / 9 - 1, ctr[1] + (k / 3) % 3 - 1, ctr[2] + k % 3 - 1};
     T h[3];
     for (int a = 0; a < 3; ++a) h[a] = T(1.0) - fabs(T(f[a]) * T(0.5) - T(c[a]));
     T w = h[0] * h[1] * h[2];
-    s = s + V(w) * finer[int64_t(g) - fine_off];
+    s = s + V(w) * finer[col[k]];
   }
   next[i] = accumulate ? s + next[i] : s;
 }
@@ -284,11 +323,15 @@ __device__ __forceinline__ T hat3(const T p[3], const int c[3], int depth) {  //
 }
 
 // Float64 screening sums of one row (screening_stencils.py:34-71): acc[k] for the row's
-// present slots, and the point load.
+// present slots (slot k = trial function q0 + (k/9, (k/3)%3, k%3)), and the point load.
+// Only the eight corners of the point's cell at the trial depth can have a nonzero trial
+// hat; every other slot would receive exactly +0.0, so skipping them leaves each
+// accumulator's sequence of nonzero additions, and hence its value, unchanged.
 template <class T>
 __device__ __forceinline__ double screening_row(const PointsView<T>& P, const int c[3], int d, int trial_depth,
                                                 const int q0[3], uint32_t present, double acc[27]) {
   double rhs = 0.0;
+  const int nt = 1 << trial_depth;
   for (int k8 = 0; k8 < 8; ++k8) {
     int cell[3] = {c[0] - k8 / 4, c[1] - (k8 / 2) % 2, c[2] - k8 % 2};
     if (dmin(cell[0], dmin(cell[1], cell[2])) < 0 || dmax(cell[0], dmax(cell[1], cell[2])) >= (1 << d)) continue;
@@ -301,10 +344,15 @@ __device__ __forceinline__ double screening_row(const PointsView<T>& P, const in
       if (weight == T(0)) continue;
       T phi = hat3(p, c, d);
       rhs += double(phi * weight);
+      int f[3];
+      for (int a = 0; a < 3; ++a) f[a] = min(max(int(floor(p[a] * T(nt))), 0), nt - 1) - q0[a];
 #pragma unroll
-      for (int k = 0; k < 27; ++k) {
+      for (int e = 0; e < 8; ++e) {
+        int s0 = f[0] + e / 4, s1 = f[1] + (e / 2) % 2, s2 = f[2] + e % 2;
+        if (s0 < 0 || s0 > 2 || s1 < 0 || s1 > 2 || s2 < 0 || s2 > 2) continue;
+        int k = s0 * 9 + s1 * 3 + s2;
         if (!((present >> k) & 1)) continue;
-        int q[3] = {q0[0] + k / 9, q0[1] + (k / 3) % 3, q0[2] + k % 3};
+        int q[3] = {q0[0] + s0, q0[1] + s1, q0[2] + s2};
         T trial = hat3(p, q, trial_depth);
         acc[k] += double(phi * trial * weight);
       }
@@ -316,26 +364,15 @@ __device__ __forceinline__ double screening_row(const PointsView<T>& P, const in
 // ------------------------------------------------------------------ A5/A7 level assembly
 // Same-level operator rows (stiffness.py:309-380 + screening) and b = T(load) + 0.5*T(point load).
 template <class T, bool SCREEN>
-__global__ void assemble_level_kernel(const int64_t* keys, int64_t n, int d, HashView bh, int64_t off,
+__global__ void assemble_level_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t off,
                                       const double* table, PointsView<T> P, const double* load, int32_t* cols,
                                       T* vals, T* b) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   int c[3];
   key_coords(keys[i], c);
-  int lim = 1 << d;
-  uint32_t present = 0;
   int32_t col[27];
-  for (int k = 0; k < 27; ++k) {
-    int q[3] = {c[0] + k / 9 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k % 3 - 1};
-    int32_t idx = -1;
-    if (dmin(q[0], dmin(q[1], q[2])) >= 0 && dmax(q[0], dmax(q[1], q[2])) <= lim) {
-      int32_t g = bh.find(basis_key(d, q[0], q[1], q[2]));
-      idx = g >= 0 ? int32_t(g - off) : -1;
-    }
-    col[k] = idx;
-    if (idx >= 0) present |= 1u << k;
-  }
+  uint32_t present = neighbours27(cv, d, c, off, col);
   double acc[27];
   for (int k = 0; k < 27; ++k) acc[k] = 0.0;
   double pl = 0.0;
@@ -363,26 +400,15 @@ __global__ void assemble_level_kernel(const int64_t* keys, int64_t n, int d, Has
 // Cross operator (rows at d, trial functions at d-1; stiffness + screening, rounded to T)
 // applied to the coarser cumulative solution: b = b - C cumulative (solver.py:428-446).
 template <class T, bool SCREEN>
-__global__ void cross_apply_kernel(const int64_t* keys, int64_t n, int d, HashView bh, int64_t coff,
+__global__ void cross_apply_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t coff,
                                    const double* table, PointsView<T> P, const T* cumulative, T* b) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   int c[3];
   key_coords(keys[i], c);
   int ctr[3] = {c[0] >> 1, c[1] >> 1, c[2] >> 1};
-  int lim = 1 << (d - 1);
-  uint32_t present = 0;
   int32_t col[27];
-  for (int k = 0; k < 27; ++k) {
-    int q[3] = {ctr[0] + k / 9 - 1, ctr[1] + (k / 3) % 3 - 1, ctr[2] + k % 3 - 1};
-    int32_t idx = -1;
-    if (dmin(q[0], dmin(q[1], q[2])) >= 0 && dmax(q[0], dmax(q[1], q[2])) <= lim) {
-      int32_t g = bh.find(basis_key(d - 1, q[0], q[1], q[2]));
-      idx = g >= 0 ? int32_t(g - coff) : -1;
-    }
-    col[k] = idx;
-    if (idx >= 0) present |= 1u << k;
-  }
+  uint32_t present = neighbours27(cv, d - 1, ctr, coff, col);
   double acc[27];
   for (int k = 0; k < 27; ++k) acc[k] = 0.0;
   if (SCREEN) {
@@ -899,10 +925,14 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
   HashMap nhash;
   nhash.build(N.keys.p, N.count, s);
   HashView nh = nhash.view();
+  ColumnIndex ncols, bcols;
+  ncols.build(N.keys.p, N.count, s);
+  bcols.build(all_keys, level_offsets.back(), s);
+  const ColumnView ncv = ncols.view(), bcv = bcols.view();
 
   // ---- A6 normal loads through the finest depth (normal_loads.py:66-190)
   std::vector<DBuf<double>> same(finest + 1), from_child(finest + 1), from_parent(finest + 1);
-  auto stencil = [&](int test_d, int normal_d, HashView h, int64_t noff, const T* nvals, int64_t nrec,
+  auto stencil = [&](int test_d, int normal_d, const ColumnView& h, int64_t noff, const T* nvals, int64_t nrec,
                      DBuf<double>& out) {
     int64_t n = count_at(test_d);
     out.alloc(n, s);
@@ -923,8 +953,8 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
     int64_t nrec = N.offsets[d + 1] - N.offsets[d];
     has_cumulative = has_cumulative || nrec > 0;
     if (d >= base) {
-      stencil(d, d, nh, 0, N.values.p, nrec, same[d]);
-      if (d > base) stencil(d - 1, d, nh, 0, N.values.p, nrec, from_child[d - 1]);
+      stencil(d, d, ncv, 0, N.values.p, nrec, same[d]);
+      if (d > base) stencil(d - 1, d, ncv, 0, N.values.p, nrec, from_child[d - 1]);
     }
     if (d < finest) {
       int64_t n = count_at(d);
@@ -934,7 +964,7 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
                                                                      d > 0 ? level_offsets[d - 1] : 0, prev.p, cum.p);
         PSR_LAUNCH_CHECK();
       }
-      if (d >= base && has_cumulative) stencil(d + 1, d, bh, level_offsets[d], cum.p, n, from_parent[d + 1]);
+      if (d >= base && has_cumulative) stencil(d + 1, d, bcv, level_offsets[d], cum.p, n, from_parent[d + 1]);
       prev = std::move(cum);
     }
   }
@@ -955,7 +985,7 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
         DBuf<double> next(nc, s);
         if (nc) {
           PSR_CUDA(cudaMemcpyAsync(next.p, from_child[d - 1].p, nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
-          restrict_add_kernel<T, double><<<blocks_for(nc), kThreads, 0, s>>>(keys_at(d - 1), nc, d, bh, level_offsets[d],
+          restrict_add_kernel<T, double><<<blocks_for(nc), kThreads, 0, s>>>(keys_at(d - 1), nc, d, bcv, level_offsets[d],
                                                                              finer.p, next.p, true);
           PSR_LAUNCH_CHECK();
         }
@@ -997,10 +1027,10 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
     DBuf<int32_t> cols(kSlots * n, s);
     DBuf<T> vals(kSlots * n, s), b(n, s);
     if (screened)
-      assemble_level_kernel<T, true><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bh, level_offsets[d],
+      assemble_level_kernel<T, true><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d],
                                                                          table.p, pv, loads[d].p, cols.p, vals.p, b.p);
     else
-      assemble_level_kernel<T, false><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bh, level_offsets[d],
+      assemble_level_kernel<T, false><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d],
                                                                           table.p, pv, loads[d].p, cols.p, vals.p, b.p);
     PSR_LAUNCH_CHECK();
     T* x = coefficients + level_offsets[d];
@@ -1048,7 +1078,7 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
           residual_kernel<T><<<blocks_for(nl), kThreads, 0, s>>>(Cl(l), Vl(l), Rl(l), Xl(l), nl, r.p);
           PSR_LAUNCH_CHECK();
           int64_t nc = count_at(l - 1);
-          restrict_add_kernel<T, T><<<blocks_for(nc), kThreads, 0, s>>>(keys_at(l - 1), nc, l, bh, level_offsets[l], r.p,
+          restrict_add_kernel<T, T><<<blocks_for(nc), kThreads, 0, s>>>(keys_at(l - 1), nc, l, bcv, level_offsets[l], r.p,
                                                                         rhs[l - 1].p, false);
           PSR_LAUNCH_CHECK();
           PSR_CUDA(cudaMemsetAsync(xs[l - 1].p, 0, nc * sizeof(T), s));
@@ -1074,10 +1104,10 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
       stiffness_table_kernel<<<blocks_for(res + 1), kThreads, 0, s>>>(d, d - 1, ctable.p);
       PSR_LAUNCH_CHECK();
       if (screened)
-        cross_apply_kernel<T, true><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bh, level_offsets[d - 1],
+        cross_apply_kernel<T, true><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d - 1],
                                                                         ctable.p, pv, cumulative.p, b.p);
       else
-        cross_apply_kernel<T, false><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bh, level_offsets[d - 1],
+        cross_apply_kernel<T, false><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d - 1],
                                                                          ctable.p, pv, cumulative.p, b.p);
       PSR_LAUNCH_CHECK();
       if (sink) sink->put("rhs_" + std::to_string(d), b.p, n, s);
