@@ -103,6 +103,24 @@ template <class T, class V>
 void relax_sliced_ell(const int32_t* cols, const T* vals, const V* b, V* x, const int32_t* rows,
                       const int32_t* group_off, int depth, int iters, cudaStream_t s, float* ms);
 
+// Schedule order of a sliced level: rows sorted by (slice, colour), key order inside a group.
+struct StripSchedule {
+  int64_t rows = 0;
+  int depth = 0;
+  bool wide = false;          // a (slice, colour) group too large for 16-bit neighbour indices
+  DBuf<int32_t> perm, inv;    // schedule position -> key-order row, and back
+  DBuf<int32_t> off;          // 4*(2^depth+1)+1 group offsets
+  DBuf<int64_t> skeys;        // keys in schedule order
+};
+void build_strip_schedule(const int64_t* keys, int64_t rows, int depth, StripSchedule& S, cudaStream_t s);
+
+// Strip-scheduled relaxation of operator rows already in schedule order: values T[28] and
+// group-relative neighbour indices I[32] per row, b with 16 bytes of slack; x in key order
+// holds the initial guess and receives the result.
+template <class T, class V, class I>
+void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sidx, const V* sb, V* x, int iters,
+                            cudaStream_t s, float* ms);
+
 // Strip-scheduled ordered relaxation (psr_relax.cu): slot-ELL rows in key order, x in key
 // order holds the initial guess and receives the result.
 template <class T, class V>

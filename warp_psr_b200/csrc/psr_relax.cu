@@ -143,9 +143,9 @@ __device__ __forceinline__ void load_idx(const I* src, I out[kIdxSlots]) {
 template <int C, class T, class V, class I>
 __device__ __forceinline__ void update_row(const I* nrow, const T* arow, V bv, V* foot, const int* delta,
                                            unsigned total, int* error) {
-  I n[kIdxSlots];
+  __align__(16) I n[kIdxSlots];  // filled with 16-byte vector loads
   load_idx(nrow, n);
-  T a[kSlotsR];
+  __align__(16) T a[kSlotsR];
   load_vals(arow, a);
   V xs[27];
   bool bad = false;
@@ -520,6 +520,11 @@ __global__ void group_bounds_kernel(const uint32_t* sorted, int64_t n, int count
   off[g] = int32_t(lo);
 }
 
+__global__ void permute_keys_kernel(const int32_t* perm, int64_t n, const int64_t* keys, int64_t* skeys) {
+  int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (p < n) skeys[p] = keys[perm[p]];
+}
+
 __global__ void max_group_kernel(const int32_t* off, int count, int* out) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g < count) atomicMax(out, off[g + 1] - off[g]);
@@ -545,23 +550,29 @@ static int device_smem_optin() {
   return bytes;
 }
 
+template <class V>
+__global__ void gather_x_kernel(const int32_t* perm, int64_t n, const V* x, V* sx) {
+  int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (p < n) sx[p] = x[perm[p]];
+}
+
 template <class T, class V, class I>
-static void run_strips(const int64_t* keys, int64_t rows, int depth, const int32_t* cols, const T* vals, const V* b,
-                       V* x, int iters, cudaStream_t s, float* ms, const int32_t* perm, const int32_t* inv,
-                       const int32_t* off) {
+void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sidx, const V* sb, V* x, int iters,
+                            cudaStream_t s, float* ms) {
+  const int64_t rows = S.rows;
+  if (iters <= 0 || rows <= 0) return;
+  const int depth = S.depth;
   const int n = 1 << depth;
   const int nx = n + 2;
   const int per16 = 16 / int(sizeof(V));
-  DBuf<I> sidx(kIdxSlots * rows, s);
-  DBuf<T> svals(kSlotsR * rows, s);
-  DBuf<V> sb(rows + 2 * per16, s), x0(rows, s), x1(rows, s);
-  DBuf<int64_t> skeys(rows, s);
-  sb.zero();
-  reorder_kernel<T, V, I><<<blocks_for(rows), kThreads, 0, s>>>(perm, inv, off, rows, cols, vals, b, x, keys, sidx.p,
-                                                               svals.p, sb.p, x1.p, skeys.p);
+  const int32_t* perm = S.perm.p;
+  const int32_t* off = S.off.p;
+  DBuf<V> x0(rows, s), x1(rows, s);
+  gather_x_kernel<V><<<blocks_for(rows), kThreads, 0, s>>>(perm, rows, x, x1.p);
   PSR_LAUNCH_CHECK();
+  const int64_t* skeys_p = S.skeys.p;
   DBuf<int32_t> xstart(int64_t(n + 1) * 4 * nx, s);
-  xstart_kernel<<<blocks_for(int64_t(n + 1) * 4 * nx), kThreads, 0, s>>>(skeys.p, off, n, xstart.p);
+  xstart_kernel<<<blocks_for(int64_t(n + 1) * 4 * nx), kThreads, 0, s>>>(skeys_p, off, n, xstart.p);
   PSR_LAUNCH_CHECK();
   // Strips per slice: about two waves of tasks (iters x strips each) per persistent grid,
   // at least ~128 rows per strip.
@@ -597,9 +608,9 @@ static void run_strips(const int64_t* keys, int64_t rows, int depth, const int32
   L.nvisits = int(visits.size());
   L.bounds = bounds.p;
   L.group_off = off;
-  L.vals = svals.p;
-  L.nidx = sidx.p;
-  L.b = sb.p;
+  L.vals = svals;
+  L.nidx = sidx;
+  L.b = sb;
   L.xb0 = x0.p;
   L.xb1 = x1.p;
   L.xstart = xstart.p;
@@ -664,33 +675,63 @@ static void run_strips(const int64_t* keys, int64_t rows, int depth, const int32
   if (err) throw Error(4, "ordered relaxation: a dependency wait timed out");
 }
 
+void build_strip_schedule(const int64_t* keys, int64_t rows, int depth, StripSchedule& S, cudaStream_t s) {
+  const int n = 1 << depth;
+  const int groups = 4 * (n + 1);
+  S.rows = rows;
+  S.depth = depth;
+  // Schedule order: stable sort by group (slice, colour); rows of a group stay in key order.
+  DBuf<uint32_t> g(rows, s), sg(rows, s);
+  DBuf<int32_t> ids(rows, s);
+  S.perm.alloc(rows, s);
+  S.inv.alloc(rows, s);
+  S.off.alloc(groups + 1, s);
+  S.skeys.alloc(rows, s);
+  slice_groups_kernel<<<blocks_for(rows), kThreads, 0, s>>>(keys, rows, g.p, ids.p);
+  PSR_LAUNCH_CHECK();
+  sort_pairs(g.p, sg.p, ids.p, S.perm.p, rows, bits_for(uint64_t(groups)), s);
+  group_bounds_kernel<<<blocks_for(groups + 1), kThreads, 0, s>>>(sg.p, rows, groups, S.off.p);
+  PSR_LAUNCH_CHECK();
+  inverse_kernel<<<blocks_for(rows), kThreads, 0, s>>>(S.perm.p, rows, S.inv.p);
+  PSR_LAUNCH_CHECK();
+  permute_keys_kernel<<<blocks_for(rows), kThreads, 0, s>>>(S.perm.p, rows, keys, S.skeys.p);
+  PSR_LAUNCH_CHECK();
+  DBuf<int> gmax(1, s);
+  gmax.zero();
+  max_group_kernel<<<blocks_for(groups), kThreads, 0, s>>>(S.off.p, groups, gmax.p);
+  PSR_LAUNCH_CHECK();
+  // Group-relative neighbour indices fit 16 bits unless a (slice, colour) group is huge.
+  S.wide = read_scalar(gmax.p, s) >= 32767;
+}
+
+template <class T, class V, class I>
+static void reorder_and_relax(const StripSchedule& S, const int64_t* keys, const int32_t* cols, const T* vals,
+                              const V* b, V* x, int iters, cudaStream_t s, float* ms) {
+  const int64_t rows = S.rows;
+  const int per16 = 16 / int(sizeof(V));
+  DBuf<I> sidx(kIdxSlots * rows, s);
+  DBuf<T> svals(kSlotsR * rows, s);
+  DBuf<V> sb(rows + 2 * per16, s), sx(rows, s);
+  DBuf<int64_t> skeys(rows, s);
+  sb.zero();
+  reorder_kernel<T, V, I><<<blocks_for(rows), kThreads, 0, s>>>(S.perm.p, S.inv.p, S.off.p, rows, cols, vals, b, x,
+                                                               keys, sidx.p, svals.p, sb.p, sx.p, skeys.p);
+  PSR_LAUNCH_CHECK();
+  relax_strips_scheduled<T, V, I>(S, svals.p, sidx.p, sb.p, x, iters, s, ms);
+}
+
 // Ordered sliced relaxation of one level given as slot-ELL rows in key order.  x (key
 // order) holds the initial guess and receives the result.
 template <class T, class V>
 void relax_sliced_strips(const int64_t* keys, int64_t rows, int depth, const int32_t* cols, const T* vals,
                          const V* b, V* x, int iters, cudaStream_t s, float* ms) {
   if (iters <= 0 || rows <= 0) return;
-  const int n = 1 << depth;
-  const int groups = 4 * (n + 1);
-  // Schedule order: stable sort by group (slice, colour); rows of a group stay in key order.
-  DBuf<uint32_t> g(rows, s), sg(rows, s);
-  DBuf<int32_t> ids(rows, s), perm(rows, s), inv(rows, s), off(groups + 1, s);
-  slice_groups_kernel<<<blocks_for(rows), kThreads, 0, s>>>(keys, rows, g.p, ids.p);
-  PSR_LAUNCH_CHECK();
-  sort_pairs(g.p, sg.p, ids.p, perm.p, rows, bits_for(uint64_t(groups)), s);
-  group_bounds_kernel<<<blocks_for(groups + 1), kThreads, 0, s>>>(sg.p, rows, groups, off.p);
-  PSR_LAUNCH_CHECK();
-  inverse_kernel<<<blocks_for(rows), kThreads, 0, s>>>(perm.p, rows, inv.p);
-  PSR_LAUNCH_CHECK();
-  DBuf<int> gmax(1, s);
-  gmax.zero();
-  max_group_kernel<<<blocks_for(groups), kThreads, 0, s>>>(off.p, groups, gmax.p);
-  PSR_LAUNCH_CHECK();
-  // Group-relative neighbour indices fit 16 bits unless a (slice, colour) group is huge.
-  if (read_scalar(gmax.p, s) < 32767)
-    run_strips<T, V, int16_t>(keys, rows, depth, cols, vals, b, x, iters, s, ms, perm.p, inv.p, off.p);
+  StripSchedule S;
+  build_strip_schedule(keys, rows, depth, S, s);
+  if (!S.wide)
+    reorder_and_relax<T, V, int16_t>(S, keys, cols, vals, b, x, iters, s, ms);
   else
-    run_strips<T, V, int32_t>(keys, rows, depth, cols, vals, b, x, iters, s, ms, perm.p, inv.p, off.p);
+    reorder_and_relax<T, V, int32_t>(S, keys, cols, vals, b, x, iters, s, ms);
 }
 
 template void relax_sliced_strips<float, float>(const int64_t*, int64_t, int, const int32_t*, const float*,
@@ -700,4 +741,16 @@ template void relax_sliced_strips<double, double>(const int64_t*, int64_t, int, 
 template void relax_sliced_strips<float, double>(const int64_t*, int64_t, int, const int32_t*, const float*,
                                                  const double*, double*, int, cudaStream_t, float*);
 
+}  // namespace psr
+
+namespace psr {
+#define PSR_SCHED(T, V, I)                                                                                       \
+  template void relax_strips_scheduled<T, V, I>(const StripSchedule&, const T*, const I*, const V*, V*, int,  \
+                                                cudaStream_t, float*);
+PSR_SCHED(float, float, int16_t)
+PSR_SCHED(float, float, int32_t)
+PSR_SCHED(double, double, int16_t)
+PSR_SCHED(double, double, int32_t)
+PSR_SCHED(float, double, int16_t)
+PSR_SCHED(float, double, int32_t)
 }  // namespace psr

@@ -397,11 +397,61 @@ __global__ void assemble_level_kernel(const int64_t* keys, int64_t n, int d, Col
   b[i] = T(load[i]) + T(0.5) * T(pl);
 }
 
+// Same-level operator rows of a sliced level written straight into schedule order: values
+// rounded to T then stored as S (float32 storage in the mixed precision), neighbours as
+// indices inside their (slice, colour) group (slot 27 = the row's own index), and
+// b = T(load) + 0.5*T(point load).
+template <class T, class S, class I, bool SCREEN>
+__global__ void assemble_sliced_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t off,
+                                       const double* table, PointsView<T> P, const double* load, const int32_t* inv,
+                                       const int32_t* group_off, S* svals, I* sidx, T* sb) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int c[3];
+  key_coords(keys[i], c);
+  int32_t col[27];
+  uint32_t present = neighbours27(cv, d, c, off, col);
+  double acc[27];
+  for (int k = 0; k < 27; ++k) acc[k] = 0.0;
+  double pl = 0.0;
+  if (SCREEN) {
+    int q0[3] = {c[0] - 1, c[1] - 1, c[2] - 1};
+    pl = screening_row(P, c, d, d, q0, present, acc);
+  }
+  const int64_t p = inv[i];
+  __align__(16) S v[28];  // written to global memory as 16-byte vectors
+  __align__(16) I idx[32];
+  for (int k = 0; k < 27; ++k) {
+    v[k] = S(0);
+    idx[k] = I(-1);
+    if (col[k] >= 0) {
+      const double* x = table + (c[0] * 3 + k / 9) * 2;
+      const double* y = table + (c[1] * 3 + (k / 3) % 3) * 2;
+      const double* z = table + (c[2] * 3 + k % 3) * 2;
+      double stiff = x[1] * y[0] * z[0] + x[0] * y[1] * z[0] + x[0] * y[0] * z[1];
+      v[k] = S(T(SCREEN ? stiff + acc[k] : stiff));
+      int g = 4 * (c[2] + k % 3 - 1) + ((c[0] + k / 9 - 1) & 1) + 2 * ((c[1] + (k / 3) % 3 - 1) & 1);
+      idx[k] = I(inv[col[k]] - group_off[g]);
+    }
+  }
+  v[27] = S(0);
+  idx[27] = I(p - group_off[4 * c[2] + (c[0] & 1) + 2 * (c[1] & 1)]);
+  for (int k = 28; k < 32; ++k) idx[k] = I(-1);
+  int4* vd = reinterpret_cast<int4*>(svals + p * 28);
+  const int4* vs = reinterpret_cast<const int4*>(v);
+  for (int q = 0; q < 28 * int(sizeof(S)) / 16; ++q) vd[q] = vs[q];
+  int4* id = reinterpret_cast<int4*>(sidx + p * 32);
+  const int4* is = reinterpret_cast<const int4*>(idx);
+  for (int q = 0; q < 32 * int(sizeof(I)) / 16; ++q) id[q] = is[q];
+  sb[p] = T(load[i]) + T(0.5) * T(pl);
+}
+
 // Cross operator (rows at d, trial functions at d-1; stiffness + screening, rounded to T)
 // applied to the coarser cumulative solution: b = b - C cumulative (solver.py:428-446).
 template <class T, bool SCREEN>
 __global__ void cross_apply_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t coff,
-                                   const double* table, PointsView<T> P, const T* cumulative, T* b) {
+                                   const double* table, PointsView<T> P, const T* cumulative, T* b,
+                                   const int32_t* inv) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   int c[3];
@@ -425,7 +475,8 @@ __global__ void cross_apply_kernel(const int64_t* keys, int64_t n, int d, Column
     T v = T(SCREEN ? stiff + acc[k] : stiff);
     s = s + v * cumulative[col[k]];
   }
-  b[i] = -s + b[i];
+  const int64_t p = inv ? inv[i] : i;
+  b[p] = -s + b[p];
 }
 
 // ------------------------------------------------------------------ A9 transfers (transfer_stencils.py:116-151)
@@ -864,6 +915,12 @@ __global__ void root_solve_kernel(const int64_t* keys, int nk, const int32_t* co
 }
 
 template <class T>
+__global__ void unpermute_kernel(const int32_t* perm, int64_t n, const T* in, T* out) {
+  int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (p < n) out[perm[p]] = in[p];
+}
+
+template <class T>
 __global__ void narrow_kernel(const T* in, int64_t n, float* out) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i < n) out[i] = float(in[i]);
@@ -1024,15 +1081,60 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
     DBuf<double> table(int64_t(res + 1) * 6, s);
     stiffness_table_kernel<<<blocks_for(res + 1), kThreads, 0, s>>>(d, d, table.p);
     PSR_LAUNCH_CHECK();
-    DBuf<int32_t> cols(kSlots * n, s);
-    DBuf<T> vals(kSlots * n, s), b(n, s);
-    if (screened)
-      assemble_level_kernel<T, true><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d],
-                                                                         table.p, pv, loads[d].p, cols.p, vals.p, b.p);
-    else
-      assemble_level_kernel<T, false><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d],
-                                                                          table.p, pv, loads[d].p, cols.p, vals.p, b.p);
-    PSR_LAUNCH_CHECK();
+    // The base level keeps key-order rows for its multigrid; finer levels are assembled
+    // straight into the schedule order of the strip-scheduled relaxation.
+    const bool sliced = d > base;
+    const bool mixed = sizeof(T) == 8 && p.precision == 1;
+    DBuf<int32_t> cols;
+    DBuf<T> vals, b;
+    StripSchedule sched;
+    DBuf<char> svals, sidx;
+    if (!sliced) {
+      cols.alloc(kSlots * n, s);
+      vals.alloc(kSlots * n, s);
+      b.alloc(n, s);
+      if (screened)
+        assemble_level_kernel<T, true><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d],
+                                                                           table.p, pv, loads[d].p, cols.p, vals.p,
+                                                                           b.p);
+      else
+        assemble_level_kernel<T, false><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d],
+                                                                            table.p, pv, loads[d].p, cols.p, vals.p,
+                                                                            b.p);
+      PSR_LAUNCH_CHECK();
+    } else {
+      build_strip_schedule(keys_at(d), n, d, sched, s);
+      const int sbytes = mixed ? 4 : int(sizeof(T));
+      const int ibytes = sched.wide ? 4 : 2;
+      svals.alloc(kSlots * n * sbytes, s);
+      sidx.alloc(32 * n * ibytes, s);
+      b.alloc(n + 4, s);
+      b.zero();
+      auto launch = [&](auto s_tag, auto i_tag) {
+        using S = decltype(s_tag);
+        using I = decltype(i_tag);
+        S* sv = reinterpret_cast<S*>(svals.p);
+        I* si = reinterpret_cast<I*>(sidx.p);
+        if (screened)
+          assemble_sliced_kernel<T, S, I, true><<<blocks_for(n, 128), 128, 0, s>>>(
+              keys_at(d), n, d, bcv, level_offsets[d], table.p, pv, loads[d].p, sched.inv.p, sched.off.p, sv, si, b.p);
+        else
+          assemble_sliced_kernel<T, S, I, false><<<blocks_for(n, 128), 128, 0, s>>>(
+              keys_at(d), n, d, bcv, level_offsets[d], table.p, pv, loads[d].p, sched.inv.p, sched.off.p, sv, si, b.p);
+        PSR_LAUNCH_CHECK();
+      };
+      if (mixed) {
+        if (sched.wide)
+          launch(float(), int32_t());
+        else
+          launch(float(), int16_t());
+      } else {
+        if (sched.wide)
+          launch(T(), int32_t());
+        else
+          launch(T(), int16_t());
+      }
+    }
     T* x = coefficients + level_offsets[d];
     PSR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), s));
     if (sink) sink->put("normal_load_" + std::to_string(d), loads[d].p, n, s);
@@ -1105,22 +1207,34 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
       PSR_LAUNCH_CHECK();
       if (screened)
         cross_apply_kernel<T, true><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d - 1],
-                                                                        ctable.p, pv, cumulative.p, b.p);
+                                                                        ctable.p, pv, cumulative.p, b.p, sched.inv.p);
       else
         cross_apply_kernel<T, false><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d - 1],
-                                                                         ctable.p, pv, cumulative.p, b.p);
+                                                                         ctable.p, pv, cumulative.p, b.p,
+                                                                         sched.inv.p);
       PSR_LAUNCH_CHECK();
-      if (sink) sink->put("rhs_" + std::to_string(d), b.p, n, s);
-      float ms = 0;
-      if (sizeof(T) == 8 && p.precision == 1) {
-        // Mixed precision: float32 operator storage, float64 vector arithmetic.
-        DBuf<float> v32(kSlots * n, s);
-        narrow_kernel<T><<<blocks_for(kSlots * n), kThreads, 0, s>>>(vals.p, kSlots * n, v32.p);
+      if (sink && sink->on) {  // kept in key order, like every other stage
+        DBuf<T> kb(n, s);
+        unpermute_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(sched.perm.p, n, b.p, kb.p);
         PSR_LAUNCH_CHECK();
-        vals.release();
-        relax_sliced_strips<float, T>(keys_at(d), n, d, cols.p, v32.p, b.p, x, p.iters, s, stats ? &ms : nullptr);
+        sink->put("rhs_" + std::to_string(d), kb.p, n, s);
+      }
+      float ms = 0;
+      float* msp = stats ? &ms : nullptr;
+      if (mixed) {
+        if (sched.wide)
+          relax_strips_scheduled<float, T, int32_t>(sched, reinterpret_cast<const float*>(svals.p),
+                                                    reinterpret_cast<const int32_t*>(sidx.p), b.p, x, p.iters, s, msp);
+        else
+          relax_strips_scheduled<float, T, int16_t>(sched, reinterpret_cast<const float*>(svals.p),
+                                                    reinterpret_cast<const int16_t*>(sidx.p), b.p, x, p.iters, s, msp);
       } else {
-        relax_sliced_strips<T, T>(keys_at(d), n, d, cols.p, vals.p, b.p, x, p.iters, s, stats ? &ms : nullptr);
+        if (sched.wide)
+          relax_strips_scheduled<T, T, int32_t>(sched, reinterpret_cast<const T*>(svals.p),
+                                                reinterpret_cast<const int32_t*>(sidx.p), b.p, x, p.iters, s, msp);
+        else
+          relax_strips_scheduled<T, T, int16_t>(sched, reinterpret_cast<const T*>(svals.p),
+                                                reinterpret_cast<const int16_t*>(sidx.p), b.p, x, p.iters, s, msp);
       }
       if (stats) {
         stats->relax_ms += ms;
