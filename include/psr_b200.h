@@ -124,6 +124,16 @@ int psr_result_stage(const psr_result* result, const char* name, const void** da
 /* Weighted mean sum(v*w)/sum(w) with float64 accumulation, written to out[0] (dtype). */
 int psr_isovalue(int32_t dtype, const void* values, const void* weights, int64_t n, void* out, void* stream);
 
+/* psr_isovalue without any device allocation: no counterpart in the reference.  For callers
+ * that cannot allocate device memory while they run (code embedded in a framework whose own
+ * pool already holds the device memory, real-time loops that must not allocate).  Its
+ * scratch is a fixed 64 KiB array in the library's device image, held by every GPU that
+ * loads the library until the process exits; n is limited to 4,194,304 values (PSR_EINVAL
+ * beyond).  The first call on a device looks up that array's address (no allocation); make
+ * it before any stream capture.  All calls share the array, so calls that overlap on the
+ * GPU (e.g. on different streams) race; results are stream-ordered, no synchronisation. */
+int psr_isovalue_static(int32_t dtype, const void* values, const void* weights, int64_t n, void* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

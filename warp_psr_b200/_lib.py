@@ -53,7 +53,7 @@ class FieldHandle(ctypes.Structure):
 
 EXPORTS = ("psr_reconstruct", "psr_result_info", "psr_result_arrays", "psr_evaluate", "psr_device_field",
            "psr_free", "psr_last_error", "psr_relax_sliced", "psr_isovalue", "psr_result_stage",
-           "psr_kernel_launches")
+           "psr_kernel_launches", "psr_isovalue_static")
 
 _lib = None
 
@@ -84,6 +84,7 @@ def load():
     L.psr_isovalue.argtypes = [i32, vp, vp, i64, vp, vp]
     L.psr_result_stage.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(vp), ctypes.POINTER(i64), ctypes.POINTER(i32)]
     L.psr_kernel_launches.argtypes = [ctypes.POINTER(i64)]
+    L.psr_isovalue_static.argtypes = [i32, vp, vp, i64, vp, vp]
     for name in EXPORTS:
         getattr(L, name).restype = i32
     _lib = L

@@ -16,6 +16,8 @@ static thread_local std::string g_error;
 namespace psr {
 std::atomic<long long> g_kernel_launches{0};
 
+void set_last_error(const std::string& message) { g_error = message; }
+
 __global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, int64_t* keys, int32_t* vals,
                                    uint64_t mask, int32_t value_offset) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;

@@ -1,6 +1,9 @@
 // A11/A12: cumulative coefficients, field evaluation, isovalue and evaluation transforms
 // (warp-psr field.py:187-421, reconstruction.py:18-116, transforms.py:211-280).
+#include "../../include/psr_b200.h"
 #include "psr_internal.cuh"
+
+#include <mutex>
 
 namespace psr {
 
@@ -257,6 +260,48 @@ void evaluation_transforms(const T* normalization, T* transforms, cudaStream_t s
   PSR_LAUNCH_CHECK();
 }
 
+// ------------------------------------------------------------------ allocation-free isovalue
+// Some callers cannot allocate device memory while they run: code embedded in a host
+// framework that has already claimed the device memory through its own pool (a renderer, a
+// deep-learning framework's caching allocator), or a real-time loop that must not take the
+// implicit synchronisation or failure modes of an allocation.  psr_isovalue_static serves
+// them: the per-block partial sums live in this file-scope array instead of a buffer from
+// the stream-ordered allocator.  Every GPU that loads the library keeps the array (64 KiB)
+// until the process exits.
+constexpr int64_t kStaticIsoBlocks = 4096;  // at most 4096 * 1024 = 4,194,304 values per call
+static __device__ __align__(256) double g_iso_scratch[2 * kStaticIsoBlocks];
+
+// Device address of g_iso_scratch for the current device, looked up once per device (the
+// host-side name is only a stand-in for the device array and must not be passed to kernels).
+static double* static_iso_scratch() {
+  static std::mutex lock;
+  static double* ptrs[64] = {nullptr};
+  int dev = 0;
+  PSR_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw Error(1, "device ordinal out of range for the static isovalue scratch");
+  std::lock_guard<std::mutex> guard(lock);
+  if (!ptrs[dev]) {
+    void* p = nullptr;
+    PSR_CUDA(cudaGetSymbolAddress(&p, g_iso_scratch));
+    ptrs[dev] = static_cast<double*>(p);
+  }
+  return ptrs[dev];
+}
+
+template <class T>
+static void isovalue_static(const T* values, const T* weights, int64_t n, T* out, cudaStream_t s) {
+  const int64_t blocks = (n + 1023) / 1024;
+  if (blocks > kStaticIsoBlocks)
+    throw Error(1, "psr_isovalue_static: at most 4,194,304 values per call (use psr_isovalue beyond that)");
+  double* partial = static_iso_scratch();
+  // Each block writes its own two partial sums before the finishing kernel reads exactly
+  // `blocks` of them, so no slot has to start at zero.
+  isovalue_blocks_kernel<T><<<unsigned(blocks), 256, 0, s>>>(values, weights, n, partial);
+  PSR_LAUNCH_CHECK();
+  isovalue_finish_kernel<T><<<1, 32, 0, s>>>(partial, blocks, out);
+  PSR_LAUNCH_CHECK();
+}
+
 #define INSTANTIATE(T)                                                                                               \
   template void cumulative_coefficients<T>(const int64_t*, const std::vector<int64_t>&, const HashView&, const T*,  \
                                            T*, int, cudaStream_t);                                                   \
@@ -269,3 +314,20 @@ INSTANTIATE(float)
 INSTANTIATE(double)
 
 }  // namespace psr
+
+extern "C" int psr_isovalue_static(int32_t dtype, const void* values, const void* weights, int64_t n, void* out,
+                                   void* stream) {
+  try {
+    if (dtype != PSR_FLOAT32 && dtype != PSR_FLOAT64) throw psr::Error(PSR_EINVAL, "dtype must be float32 or float64");
+    if (n <= 0 || !values || !weights || !out) throw psr::Error(PSR_EINVAL, "nonempty values and weights are required");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == PSR_FLOAT64)
+      psr::isovalue_static<double>((const double*)values, (const double*)weights, n, (double*)out, s);
+    else
+      psr::isovalue_static<float>((const float*)values, (const float*)weights, n, (float*)out, s);
+    return PSR_OK;
+  } catch (const psr::Error& e) {
+    psr::set_last_error(e.what());
+    return e.code;
+  }
+}

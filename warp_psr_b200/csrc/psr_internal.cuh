@@ -35,6 +35,9 @@ struct StageSink {
   }
 };
 
+// Sets the message psr_last_error returns on this thread.
+void set_last_error(const std::string& message);
+
 // ---------------------------------------------------------------- A1 samples.py
 template <class T>
 struct SampleGroups {
