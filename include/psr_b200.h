@@ -71,6 +71,8 @@ typedef struct psr_info {
   double relax_ms;          /* device time of the ordered sliced relaxation kernels (CUDA events) */
   int64_t relax_row_visits; /* rows x sweeps relaxed by those kernels */
   int64_t relax_launches;
+  double relax_finest_ms;            /* the finest level's launch alone (the dominant one) */
+  int64_t relax_finest_row_visits;
 } psr_info;
 
 /* Device arrays owned by the result (valid until psr_free). */

@@ -32,6 +32,7 @@ class Info(ctypes.Structure):
         ("iso_value", ctypes.c_double), ("cube_to_model", ctypes.c_double * 16),
         ("model_to_cube", ctypes.c_double * 16), ("stage_ms", ctypes.c_double * 8),
         ("relax_ms", ctypes.c_double), ("relax_row_visits", ctypes.c_int64), ("relax_launches", ctypes.c_int64),
+        ("relax_finest_ms", ctypes.c_double), ("relax_finest_row_visits", ctypes.c_int64),
     ]
 
 

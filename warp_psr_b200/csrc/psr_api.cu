@@ -54,6 +54,21 @@ __global__ void column_insert_kernel(const int64_t* __restrict__ keys, int64_t n
     h = (h + 1) & mask;
   }
 }
+
+__global__ void dense_column_kernel(const int64_t* __restrict__ keys, int64_t n, int32_t* dense, int32_t* error) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int64_t k = keys[i];
+  if (i > 0 && (keys[i - 1] >> 16) == (k >> 16)) return;
+  int c[3];
+  key_coords(k, c);
+  const int d = int(k >> 48), side = (1 << d) + 1;
+  if (d > kDenseColumnDepth || unsigned(c[0]) >= unsigned(side) || unsigned(c[1]) >= unsigned(side)) {
+    atomicExch(error, 1);
+    return;
+  }
+  dense[dense_column_base(d) + int64_t(c[0]) * side + c[1]] = int32_t(i);
+}
 }  // namespace psr
 
 struct psr_result {
@@ -263,6 +278,8 @@ int psr_result_info(const psr_result* R, psr_info* info) {
   info->relax_ms = R->stats.relax_ms;
   info->relax_row_visits = R->stats.row_visits;
   info->relax_launches = R->stats.launches;
+  info->relax_finest_ms = R->stats.level_relax_ms.empty() ? 0.0 : R->stats.level_relax_ms.back();
+  info->relax_finest_row_visits = R->stats.finest_row_visits;
   return PSR_OK;
 }
 

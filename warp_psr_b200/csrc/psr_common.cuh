@@ -211,14 +211,34 @@ struct HashMap {
 // Keys sorted by (depth, x, y, z) form contiguous z-runs per (depth, x, y) column.  The
 // column index maps a column to the position of its first key, so a box of neighbours costs
 // one probe per (x, y) column plus a short scan in z instead of one probe per key.
+// Column index of sorted basis keys: (d, x, y) -> index of the first key of that z-run.
+// Up to kDenseColumnDepth it is a dense table per depth ((2^d + 1)^2 int32 entries, 1.4 MB
+// through depth 9, so it stays in L2 and a probe is one load); deeper trees use a hash.
+constexpr int kDenseColumnDepth = 12;
+
+__host__ __device__ __forceinline__ int64_t dense_column_base(int d) {
+  // sum over e < d of (2^e + 1)^2
+  return ((int64_t(1) << (2 * d)) - 1) / 3 + 2 * ((int64_t(1) << d) - 1) + d;
+}
+
 struct ColumnView {
   HashView h;
+  const int32_t* dense = nullptr;
   const int64_t* keys = nullptr;
   int64_t n = 0;
   __host__ __device__ static __forceinline__ int64_t column_key(int d, int x, int y) { return basis_key(d, x, y, 0); }
+  // Index of the first key of column (d, x, y), or -1.
+  __device__ __forceinline__ int32_t column(int d, int x, int y) const {
+    if (dense) {
+      const int side = (1 << d) + 1;
+      if (unsigned(x) >= unsigned(side) || unsigned(y) >= unsigned(side)) return -1;
+      return __ldg(dense + dense_column_base(d) + int64_t(x) * side + y);
+    }
+    return h.find(column_key(d, x, y));
+  }
   // Index of the key (d, x, y, z), or -1.
   __device__ __forceinline__ int32_t find(int d, int x, int y, int z) const {
-    int32_t j = h.find(column_key(d, x, y));
+    int32_t j = column(d, x, y);
     if (j < 0) return -1;
     int64_t want = basis_key(d, x, y, z), col = column_key(d, x, y) >> 16;
     for (; j < n; ++j) {
@@ -232,23 +252,41 @@ struct ColumnView {
 
 __global__ void column_insert_kernel(const int64_t* __restrict__ keys, int64_t n, int64_t* hkeys, int32_t* hvals,
                                      uint64_t mask);
+__global__ void dense_column_kernel(const int64_t* __restrict__ keys, int64_t n, int32_t* dense, int32_t* error);
 
 struct ColumnIndex {
   HashMap map;
+  DBuf<int32_t> table;
   ColumnView view_;
-  void build(const int64_t* keys, int64_t n, cudaStream_t s) {
-    map.count = n;
-    uint64_t cap = 16;
-    while (cap < uint64_t(2 * n + 1)) cap <<= 1;
-    map.mask = cap - 1;
-    map.keys.alloc(int64_t(cap), s);
-    map.vals.alloc(int64_t(cap), s);
-    PSR_CUDA(cudaMemsetAsync(map.keys.p, 0xff, cap * sizeof(int64_t), s));
-    if (n > 0) {
-      column_insert_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, map.keys.p, map.vals.p, map.mask);
-      PSR_LAUNCH_CHECK();
+  // `max_depth` bounds the depth of every key (coordinates within [0, 2^d]).
+  void build(const int64_t* keys, int64_t n, int max_depth, cudaStream_t s) {
+    view_ = ColumnView();
+    if (max_depth <= kDenseColumnDepth) {
+      const int64_t size = dense_column_base(max_depth + 1);
+      table.alloc(size, s);
+      PSR_CUDA(cudaMemsetAsync(table.p, 0xff, size * sizeof(int32_t), s));
+      if (n > 0) {
+        DBuf<int32_t> err(1, s);
+        err.zero();
+        dense_column_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, table.p, err.p);
+        PSR_LAUNCH_CHECK();
+        if (read_scalar(err.p, s)) throw std::runtime_error("column index: key outside its depth's grid");
+      }
+      view_.dense = table.p;
+    } else {
+      map.count = n;
+      uint64_t cap = 16;
+      while (cap < uint64_t(2 * n + 1)) cap <<= 1;
+      map.mask = cap - 1;
+      map.keys.alloc(int64_t(cap), s);
+      map.vals.alloc(int64_t(cap), s);
+      PSR_CUDA(cudaMemsetAsync(map.keys.p, 0xff, cap * sizeof(int64_t), s));
+      if (n > 0) {
+        column_insert_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, map.keys.p, map.vals.p, map.mask);
+        PSR_LAUNCH_CHECK();
+      }
+      view_.h = map.view();
     }
-    view_.h = map.view();
     view_.keys = keys;
     view_.n = n;
   }

@@ -93,6 +93,7 @@ struct SolveStats {
   int64_t row_visits = 0;    // rows x sweeps relaxed by the sliced kernels
   int64_t launches = 0;
   std::vector<double> level_relax_ms;
+  int64_t finest_row_visits = 0;  // rows x sweeps of the last (finest) sliced level
 };
 template <class T>
 void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalData<T>& N,

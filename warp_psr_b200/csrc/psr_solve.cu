@@ -116,7 +116,7 @@ __device__ __forceinline__ uint32_t neighbours27(const ColumnView& cv, int d, co
     for (int dy = 0; dy < 3; ++dy) {
       int qy = ctr[1] + dy - 1;
       if (qy < 0 || qy > lim) continue;
-      int32_t j = cv.h.find(ColumnView::column_key(d, qx, qy));
+      int32_t j = cv.column(d, qx, qy);
       if (j < 0) continue;
       int64_t colk = ColumnView::column_key(d, qx, qy) >> 16;
       int z0 = ctr[2] - 1;
@@ -158,7 +158,7 @@ __global__ void normal_stencil_kernel(const int64_t* keys, int64_t n, int test_d
     for (int y = 0; y < width; ++y) {
       int ny = ctr[1] + y + first;
       if (ny < 0 || ny >= lim) continue;
-      int32_t j = cv.h.find(ColumnView::column_key(normal_depth, nx, ny));
+      int32_t j = cv.column(normal_depth, nx, ny);
       if (j < 0) continue;
       const double* iy = table + (c[1] * width + y) * 2;
       int64_t colk = ColumnView::column_key(normal_depth, nx, ny) >> 16;
@@ -983,8 +983,8 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
   nhash.build(N.keys.p, N.count, s);
   HashView nh = nhash.view();
   ColumnIndex ncols, bcols;
-  ncols.build(N.keys.p, N.count, s);
-  bcols.build(all_keys, level_offsets.back(), s);
+  ncols.build(N.keys.p, N.count, finest, s);
+  bcols.build(all_keys, level_offsets.back(), finest, s);
   const ColumnView ncv = ncols.view(), bcv = bcols.view();
 
   // ---- A6 normal loads through the finest depth (normal_loads.py:66-190)
@@ -1240,6 +1240,7 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
         stats->relax_ms += ms;
         stats->row_visits += n * p.iters;
         stats->level_relax_ms.push_back(ms);
+        stats->finest_row_visits = n * p.iters;
         stats->launches += 1;
       }
       DBuf<T> next(n, s);

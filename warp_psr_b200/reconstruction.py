@@ -47,10 +47,11 @@ class _Handle:
 
     def __init__(self, ptr):
         self.ptr = ptr
+        self._free = _lib.load().psr_free  # held so interpreter shutdown can still free
 
     def __del__(self):
-        if self.ptr:
-            _lib.load().psr_free(self.ptr)
+        if self.ptr and self._free is not None:
+            self._free(self.ptr)
             self.ptr = None
 
 
@@ -243,5 +244,7 @@ def reconstruct(positions, normals, *, depth=6, full_depth=3, base_depth=None, s
                    "level_offsets": [int(arrays.level_offsets[d]) for d in range(depth + 2)],
                    "total_seconds": info.stage_ms[7] / 1000.0,
                    "relax_seconds": info.relax_ms / 1000.0, "relax_row_visits": int(info.relax_row_visits),
-                   "relax_launches": int(info.relax_launches)}
+                   "relax_launches": int(info.relax_launches),
+                   "relax_finest_seconds": info.relax_finest_ms / 1000.0,
+                   "relax_finest_row_visits": int(info.relax_finest_row_visits)}
     return Reconstruction(field, metadata, diagnostics)
