@@ -18,6 +18,8 @@
  *   psr_free              <- (Python garbage collection of the Reconstruction)
  *   psr_relax_sliced      <- relaxation.relax_sliced         src/warp_psr/relaxation.py:189-210
  *   psr_isovalue          <- reconstruction._compute_isovalue src/warp_psr/reconstruction.py:101-116
+ *   psr_backward          <- reconstruct_differentiable backward  src/warp_psr/reconstruction_adjoint.py:99-172
+ *   psr_evaluate_backward <- DifferentiableField.evaluate VJP  field_adjoint.py:34-45,246-288; field.py:214-284
  */
 #ifndef PSR_B200_H
 #define PSR_B200_H
@@ -52,6 +54,7 @@ typedef struct psr_params {
   int32_t exact_interpolation, iters, base_v_cycles;
   int32_t precision;
   int32_t keep_stages; /* nonzero: keep intermediate stage arrays for psr_result_stage (tests) */
+  int32_t differentiable; /* nonzero: keep the reverse-pass tape for psr_backward */
 } psr_params;
 
 typedef struct psr_result psr_result;
@@ -73,6 +76,7 @@ typedef struct psr_info {
   int64_t relax_launches;
   double relax_finest_ms;            /* the finest level's launch alone (the dominant one) */
   int64_t relax_finest_row_visits;
+  double normalization[5];  /* sample transform [1/width, t0, t1, t2, normal scale] (samples.py:54-88) */
 } psr_info;
 
 /* Device arrays owned by the result (valid until psr_free). */
@@ -135,6 +139,26 @@ int psr_isovalue(int32_t dtype, const void* values, const void* weights, int64_t
  * it before any stream capture.  All calls share the array, so calls that overlap on the
  * GPU (e.g. on different streams) race; results are stream-ordered, no synchronisation. */
 int psr_isovalue_static(int32_t dtype, const void* values, const void* weights, int64_t n, void* out, void* stream);
+
+/* Reverse pass of a reconstruction made with params.differentiable (warp-psr
+ * reconstruction_adjoint.py:99-172): the vector-Jacobian product of the finite algorithm
+ * the forward ran, with its discrete choices fixed (groups, tree, bins, schedules, CG
+ * stopping points).  Seeds (result dtype; NULL = zero): g_coefficients and g_cumulative
+ * (total values each), g_iso, g_normalization (5, the adjoint of psr_info.normalization).
+ * positions/normals are the forward's inputs (unchanged since), n points of input dtype
+ * `dtype`; g_positions and g_normals (n x 3, input dtype) are written.  The tape stays, so
+ * the pass can be repeated with other seeds. */
+int psr_backward(psr_result* result, const void* positions, const void* normals, int64_t n, int32_t dtype,
+                 const void* g_coefficients, const void* g_cumulative, double g_iso, const void* g_normalization,
+                 void* g_positions, void* g_normals, void* stream);
+
+/* psr_evaluate reversed: seeds g_values (nq) and g_gradients (nq x 3, NULL = zero), result
+ * dtype.  g_coefficients and g_cumulative (total values) accumulate; g_queries (nq x 3, may
+ * be NULL) is written; g_normalization (5, may be NULL) accumulates the adjoint of the model
+ * to cube transform, expressed on psr_info.normalization. */
+int psr_evaluate_backward(const psr_result* result, const void* queries, int64_t nq, const void* g_values,
+                          const void* g_gradients, void* g_coefficients, void* g_cumulative, void* g_queries,
+                          void* g_normalization, void* stream);
 
 #ifdef __cplusplus
 }

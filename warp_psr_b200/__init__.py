@@ -4,7 +4,9 @@
 sample grouping, density and normal splats, tree, cascadic solve, field and isovalue —
 as hand-written sm_100a CUDA kernels in ``libpsr_b200.so`` behind a C ABI.
 """
-from .reconstruction import reconstruct, Reconstruction, LevelField, DeviceField
+from .reconstruction import (reconstruct, reconstruct_differentiable, Reconstruction, DifferentiableReconstruction,
+                             LevelField, DeviceField)
 from . import ops
 
-__all__ = ["reconstruct", "Reconstruction", "LevelField", "DeviceField", "ops"]
+__all__ = ["reconstruct", "reconstruct_differentiable", "Reconstruction", "DifferentiableReconstruction",
+           "LevelField", "DeviceField", "ops"]

@@ -21,7 +21,7 @@ class Params(ctypes.Structure):
         ("samples_per_node", ctypes.c_double), ("scale", ctypes.c_double),
         ("point_weight", ctypes.c_double), ("cg_accuracy", ctypes.c_double),
         ("exact_interpolation", ctypes.c_int32), ("iters", ctypes.c_int32), ("base_v_cycles", ctypes.c_int32),
-        ("precision", ctypes.c_int32), ("keep_stages", ctypes.c_int32),
+        ("precision", ctypes.c_int32), ("keep_stages", ctypes.c_int32), ("differentiable", ctypes.c_int32),
     ]
 
 
@@ -33,6 +33,7 @@ class Info(ctypes.Structure):
         ("model_to_cube", ctypes.c_double * 16), ("stage_ms", ctypes.c_double * 8),
         ("relax_ms", ctypes.c_double), ("relax_row_visits", ctypes.c_int64), ("relax_launches", ctypes.c_int64),
         ("relax_finest_ms", ctypes.c_double), ("relax_finest_row_visits", ctypes.c_int64),
+        ("normalization", ctypes.c_double * 5),
     ]
 
 
@@ -54,7 +55,7 @@ class FieldHandle(ctypes.Structure):
 
 EXPORTS = ("psr_reconstruct", "psr_result_info", "psr_result_arrays", "psr_evaluate", "psr_device_field",
            "psr_free", "psr_last_error", "psr_relax_sliced", "psr_isovalue", "psr_result_stage",
-           "psr_kernel_launches", "psr_isovalue_static")
+           "psr_kernel_launches", "psr_isovalue_static", "psr_backward", "psr_evaluate_backward")
 
 _lib = None
 
@@ -86,6 +87,8 @@ def load():
     L.psr_result_stage.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(vp), ctypes.POINTER(i64), ctypes.POINTER(i32)]
     L.psr_kernel_launches.argtypes = [ctypes.POINTER(i64)]
     L.psr_isovalue_static.argtypes = [i32, vp, vp, i64, vp, vp]
+    L.psr_backward.argtypes = [vp, vp, vp, i64, i32, vp, vp, ctypes.c_double, vp, vp, vp, vp]
+    L.psr_evaluate_backward.argtypes = [vp, vp, i64, vp, vp, vp, vp, vp, vp, vp]
     for name in EXPORTS:
         getattr(L, name).restype = i32
     _lib = L

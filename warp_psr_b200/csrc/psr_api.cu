@@ -84,10 +84,25 @@ struct psr_result {
   HashMap hash;
   double iso = 0;
   double host_transforms[32] = {0};
+  double normalization[5] = {0};
+  std::shared_ptr<void> tape;  // psr::Tape<T> of a differentiable reconstruction
   double stage_ms[8] = {0};
   SolveStats stats;
   StageSink sink;
 };
+
+namespace psr {
+// Everything the reverse pass needs, kept by a differentiable reconstruction.
+template <class T>
+struct Tape {
+  SampleGroups<T> G;
+  DensityData<T> D;
+  NormalData<T> N;
+  TreeData tree;
+  std::shared_ptr<void> solve;
+  int64_t n_input = 0;
+};
+}  // namespace psr
 
 namespace {
 
@@ -137,11 +152,12 @@ void run(const T* pos, const T* nrm, int64_t n, const Params& prm, cudaStream_t 
   cudaEvent_t ev[8];
   for (auto& e : ev) PSR_CUDA(cudaEventCreate(&e));
   PSR_CUDA(cudaEventRecord(ev[0], s));
-  SampleGroups<T> G = prepare_samples<T>(pos, nrm, n, prm.depth, prm.scale, s);
+  const bool keep = prm.differentiable != 0;
+  SampleGroups<T> G = prepare_samples<T>(pos, nrm, n, prm.depth, prm.scale, s, keep);
   PSR_CUDA(cudaEventRecord(ev[1], s));
-  DensityData<T> D = build_density<T>(G, prm.depth, prm.kernel_depth, prm.samples_per_node, s);
+  DensityData<T> D = build_density<T>(G, prm.depth, prm.kernel_depth, prm.samples_per_node, s, keep);
   PSR_CUDA(cudaEventRecord(ev[2], s));
-  NormalData<T> N = build_normals<T>(G, D, prm.base_depth, prm.depth, s);
+  NormalData<T> N = build_normals<T>(G, D, prm.base_depth, prm.depth, s, keep);
   StageSink& sink = R->sink;
   sink.put("group_keys", G.keys.p, G.count, s);
   sink.put("group_sums", G.sums.p, 3 * G.count, s);
@@ -169,7 +185,9 @@ void run(const T* pos, const T* nrm, int64_t n, const Params& prm, cudaStream_t 
   R->coefficients.alloc(total * int64_t(sizeof(T)), s);
   R->coefficients.zero();
   T* coeff = reinterpret_cast<T*>(R->coefficients.p);
-  solve_levels<T>(tree, D, N, R->level_offsets, R->keys.p, R->hash, prm, coeff, s, &R->stats, &sink);
+  std::shared_ptr<void> solve_tape;
+  solve_levels<T>(tree, D, N, R->level_offsets, R->keys.p, R->hash, prm, coeff, s, &R->stats, &sink,
+                  keep ? &solve_tape : nullptr);
   PSR_CUDA(cudaEventRecord(ev[5], s));
   R->cumulative.alloc(total * int64_t(sizeof(T)), s);
   T* cum = reinterpret_cast<T*>(R->cumulative.p);
@@ -187,11 +205,14 @@ void run(const T* pos, const T* nrm, int64_t n, const Params& prm, cudaStream_t 
   PSR_CUDA(cudaEventRecord(ev[7], s));
   T host_iso;
   T host_tr[32];
+  T host_norm[5];
   PSR_CUDA(cudaMemcpyAsync(&host_iso, iso.p, sizeof(T), cudaMemcpyDeviceToHost, s));
   PSR_CUDA(cudaMemcpyAsync(host_tr, R->transforms.p, 32 * sizeof(T), cudaMemcpyDeviceToHost, s));
+  PSR_CUDA(cudaMemcpyAsync(host_norm, G.transform.p, 5 * sizeof(T), cudaMemcpyDeviceToHost, s));
   PSR_CUDA(cudaStreamSynchronize(s));
   R->iso = double(host_iso);
   for (int i = 0; i < 32; ++i) R->host_transforms[i] = double(host_tr[i]);
+  for (int i = 0; i < 5; ++i) R->normalization[i] = double(host_norm[i]);
   for (int i = 0; i < 7; ++i) {
     float ms = 0;
     PSR_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
@@ -204,6 +225,92 @@ void run(const T* pos, const T* nrm, int64_t n, const Params& prm, cudaStream_t 
   R->groups = G.count;
   R->support_count = tree.support_count;
   R->support = std::move(tree.support);
+  if (keep) {
+    auto tape = std::make_shared<Tape<T>>();
+    tape->G = std::move(G);
+    tape->D = std::move(D);
+    tape->N = std::move(N);
+    tape->tree = std::move(tree);
+    tape->solve = std::move(solve_tape);
+    tape->n_input = n;
+    R->tape = tape;
+  }
+}
+
+template <class T>
+__global__ void cast_kernel_t(const void* in, int in_double, int64_t n, T* out) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  out[i] = in_double ? T(static_cast<const double*>(in)[i]) : T(static_cast<const float*>(in)[i]);
+}
+
+// Reverse pass: field (isovalue, cumulative) -> solve -> splats, density -> inputs.
+template <class T>
+void backward(psr_result* R, const T* pos, const T* nrm, int64_t n, const T* g_coef_in, const T* g_cum_in,
+              double g_iso, const T* g_norm, T* g_pos, T* g_nrm, cudaStream_t s) {
+  Tape<T>& tp = *static_cast<Tape<T>*>(R->tape.get());
+  const Params& prm = R->params;
+  const int64_t total = R->level_offsets.back();
+  DBuf<T> g_coef(total, s), g_cum(total, s), g_sums(3 * tp.G.count, s);
+  if (g_coef_in)
+    PSR_CUDA(cudaMemcpyAsync(g_coef.p, g_coef_in, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
+  else
+    g_coef.zero();
+  if (g_cum_in)
+    PSR_CUDA(cudaMemcpyAsync(g_cum.p, g_cum_in, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
+  else
+    g_cum.zero();
+  g_sums.zero();
+  HashView hv = R->hash.view();
+  field_backward<T>(R->keys.p, R->level_offsets, hv, reinterpret_cast<const T*>(R->coefficients.p),
+                    reinterpret_cast<const T*>(R->cumulative.p), prm.depth, tp.G.sums.p, tp.G.weights.p, tp.G.count,
+                    g_iso, g_coef.p, g_cum.p, g_sums.p, s);
+  std::vector<DBuf<T>> g_agg(prm.depth + 1);
+  for (int d = 0; d <= prm.depth; ++d) {
+    g_agg[d].alloc(4 * tp.D.agg_count[d], s);
+    g_agg[d].zero();
+  }
+  DBuf<T> g_avg(3, s), g_nvals(4 * tp.N.count, s);
+  g_avg.zero();
+  g_nvals.zero();
+  solve_backward<T>(tp.solve.get(), tp.tree, tp.D, tp.N, R->level_offsets, R->keys.p, R->hash, prm, g_coef.p, g_agg,
+                    g_avg.p, g_nvals.p, s);
+  samples_backward<T>(tp.G, tp.D, tp.N, prm.depth, prm.kernel_depth, prm.base_depth, prm.samples_per_node, prm.scale,
+                      g_agg, g_avg.p, g_nvals.p, g_sums.p, g_norm, pos, nrm, n, g_pos, g_nrm, s);
+}
+
+
+}  // namespace
+
+namespace {
+template <class T>
+__global__ void ltr_to_normalization_kernel(const double* g_ltr, T* g_norm) {
+  if (threadIdx.x != 0) return;
+  // model -> cube is [[0,s,0,t0],[0,0,s,t1],[s,0,0,t2]] (transforms.py:55-70)
+  g_norm[0] = g_norm[0] + T(g_ltr[1] + g_ltr[5] + g_ltr[6]);
+  for (int a = 0; a < 3; ++a) g_norm[1 + a] = g_norm[1 + a] + T(g_ltr[9 + a]);
+}
+
+template <class T>
+static void evaluate_backward_typed(const psr_result* R, const T* q, int64_t nq, const T* gv, const T* gg, T* gc,
+                                    T* gcum, T* gq, T* gnorm, cudaStream_t s) {
+  DBuf<T> lt(12, s);
+  T h[12];
+  for (int r = 0; r < 3; ++r) {
+    for (int c = 0; c < 3; ++c) h[3 * r + c] = T(R->host_transforms[16 + 4 * r + c]);
+    h[9 + r] = T(R->host_transforms[16 + 4 * r + 3]);
+  }
+  PSR_CUDA(cudaMemcpyAsync(lt.p, h, sizeof(h), cudaMemcpyHostToDevice, s));
+  DBuf<double> ltr(12, s);
+  ltr.zero();
+  evaluate_backward<T>(R->hash.view(), reinterpret_cast<const T*>(R->coefficients.p),
+                       reinterpret_cast<const T*>(R->cumulative.p), q, nq, lt.p, lt.p + 9, R->depth, gv, gg, gc, gcum,
+                       gq, gnorm ? ltr.p : nullptr, s);
+  if (gnorm) {
+    ltr_to_normalization_kernel<T><<<1, 32, 0, s>>>(ltr.p, gnorm);
+    PSR_LAUNCH_CHECK();
+  }
+  PSR_CUDA(cudaStreamSynchronize(s));
 }
 
 }  // namespace
@@ -225,6 +332,7 @@ int psr_reconstruct(const void* positions, const void* normals, int64_t n, int32
     Params prm{params->depth, params->full_depth, params->base_depth, params->solve_depth, params->kernel_depth,
                params->samples_per_node, params->scale, params->point_weight, params->cg_accuracy,
                params->exact_interpolation, params->iters, params->base_v_cycles, params->precision};
+    prm.differentiable = params->differentiable != 0;
     std::unique_ptr<psr_result> R(new psr_result());
     R->sink.on = params->keep_stages != 0;
     R->depth = prm.depth;
@@ -280,6 +388,7 @@ int psr_result_info(const psr_result* R, psr_info* info) {
   info->relax_launches = R->stats.launches;
   info->relax_finest_ms = R->stats.level_relax_ms.empty() ? 0.0 : R->stats.level_relax_ms.back();
   info->relax_finest_row_visits = R->stats.finest_row_visits;
+  for (int i = 0; i < 5; ++i) info->normalization[i] = R->normalization[i];
   return PSR_OK;
 }
 
@@ -328,6 +437,74 @@ int psr_evaluate(const psr_result* R, const void* queries, int64_t nq, void* val
                               valid, false, nullptr, nullptr, s);
     }
     PSR_CUDA(cudaStreamSynchronize(s));
+    return PSR_OK;
+  } catch (const Error& e) {
+    return fail(e);
+  }
+}
+
+int psr_backward(psr_result* R, const void* positions, const void* normals, int64_t n, int32_t dtype,
+                 const void* g_coefficients, const void* g_cumulative, double g_iso, const void* g_normalization,
+                 void* g_positions, void* g_normals, void* stream) {
+  try {
+    if (!R) throw Error(PSR_EINVAL, "result must not be NULL");
+    if (!R->tape) throw Error(PSR_EINVAL, "the reconstruction was not made differentiable (params.differentiable)");
+    if (dtype != PSR_FLOAT32 && dtype != PSR_FLOAT64) throw Error(PSR_EINVAL, "dtype must be float32 or float64");
+    if (!positions || !normals || !g_positions || !g_normals) throw Error(PSR_EINVAL, "inputs and outputs are required");
+    if (!std::isfinite(g_iso)) throw Error(PSR_EINVAL, "g_iso must be finite");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (R->dtype == PSR_FLOAT64) {
+      const int64_t want = static_cast<Tape<double>*>(R->tape.get())->n_input;
+      if (n != want) throw Error(PSR_EINVAL, "n differs from the forward's point count");
+      if (dtype == PSR_FLOAT64) {
+        backward<double>(R, (const double*)positions, (const double*)normals, n, (const double*)g_coefficients,
+                         (const double*)g_cumulative, g_iso, (const double*)g_normalization, (double*)g_positions,
+                         (double*)g_normals, s);
+      } else {
+        DBuf<double> p64(3 * n, s), n64(3 * n, s), gp(3 * n, s), gn(3 * n, s);
+        cast_kernel_t<double><<<blocks_for(3 * n), kThreads, 0, s>>>(positions, 0, 3 * n, p64.p);
+        PSR_LAUNCH_CHECK();
+        cast_kernel_t<double><<<blocks_for(3 * n), kThreads, 0, s>>>(normals, 0, 3 * n, n64.p);
+        PSR_LAUNCH_CHECK();
+        backward<double>(R, p64.p, n64.p, n, (const double*)g_coefficients, (const double*)g_cumulative, g_iso,
+                         (const double*)g_normalization, gp.p, gn.p, s);
+        cast_kernel_t<float><<<blocks_for(3 * n), kThreads, 0, s>>>(gp.p, 1, 3 * n, (float*)g_positions);
+        PSR_LAUNCH_CHECK();
+        cast_kernel_t<float><<<blocks_for(3 * n), kThreads, 0, s>>>(gn.p, 1, 3 * n, (float*)g_normals);
+        PSR_LAUNCH_CHECK();
+      }
+    } else {
+      if (dtype != PSR_FLOAT32) throw Error(PSR_EINVAL, "inputs must have the forward's dtype");
+      const int64_t want = static_cast<Tape<float>*>(R->tape.get())->n_input;
+      if (n != want) throw Error(PSR_EINVAL, "n differs from the forward's point count");
+      backward<float>(R, (const float*)positions, (const float*)normals, n, (const float*)g_coefficients,
+                      (const float*)g_cumulative, g_iso, (const float*)g_normalization, (float*)g_positions,
+                      (float*)g_normals, s);
+    }
+    PSR_CUDA(cudaStreamSynchronize(s));
+    return PSR_OK;
+  } catch (const Error& e) {
+    return fail(e);
+  }
+}
+
+int psr_evaluate_backward(const psr_result* R, const void* queries, int64_t nq, const void* g_values,
+                          const void* g_gradients, void* g_coefficients, void* g_cumulative, void* g_queries,
+                          void* g_normalization, void* stream) {
+  try {
+    if (!R) throw Error(PSR_EINVAL, "result must not be NULL");
+    if (nq < 0 || (nq > 0 && !queries)) throw Error(PSR_EINVAL, "queries are required");
+    if (!g_coefficients || !g_cumulative) throw Error(PSR_EINVAL, "coefficient adjoints are required");
+    if (nq == 0) return PSR_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (R->dtype == PSR_FLOAT64)
+      evaluate_backward_typed<double>(R, (const double*)queries, nq, (const double*)g_values,
+                                      (const double*)g_gradients, (double*)g_coefficients, (double*)g_cumulative,
+                                      (double*)g_queries, (double*)g_normalization, s);
+    else
+      evaluate_backward_typed<float>(R, (const float*)queries, nq, (const float*)g_values, (const float*)g_gradients,
+                                     (float*)g_coefficients, (float*)g_cumulative, (float*)g_queries,
+                                     (float*)g_normalization, s);
     return PSR_OK;
   } catch (const Error& e) {
     return fail(e);

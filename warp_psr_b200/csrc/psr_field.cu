@@ -302,7 +302,225 @@ static void isovalue_static(const T* values, const T* weights, int64_t n, T* out
   PSR_LAUNCH_CHECK();
 }
 
+// ------------------------------------------------------------------ A13 field reverse (field_adjoint.py, field.py:214-284)
+// One level of evaluate_kernel reversed: coefficient adjoints (atomic) and the cube-frame
+// position adjoint.  gv seeds the value, gg (cube frame) the spatial gradient r[1..3].
+template <class T>
+__device__ __forceinline__ void add_level_reverse(const HashView& h, const T* coeff, const T p[3], int d, T gv,
+                                                  const T gg[3], T* g_coeff, T qp[3]) {
+  int n = 1 << d;
+  T t[3], f[3];
+  int cell[3], base[3];
+  for (int a = 0; a < 3; ++a) {
+    t[a] = p[a] * T(n);
+    cell[a] = min(max(int(ceil(t[a])) - 1, 0), n - 1);
+    base[a] = int(floor(t[a]));
+    f[a] = t[a] - T(base[a]);
+  }
+  for (int corner = 0; corner < 8; ++corner) {
+    int node[3] = {cell[0] + corner / 4, cell[1] + (corner / 2) % 2, cell[2] + corner % 2};
+    if (min(node[0] - base[0], min(node[1] - base[1], node[2] - base[2])) < 0) continue;
+    int32_t idx = h.find(basis_key(d, node[0], node[1], node[2]));
+    if (idx < 0) continue;
+    T hh[3], sg[3];
+    for (int a = 0; a < 3; ++a) {
+      hh[a] = T(1) - f[a];
+      sg[a] = T(-1);
+      if (node[a] > base[a]) {
+        hh[a] = f[a];
+        sg[a] = T(1);
+      }
+    }
+    const T nn = T(n);
+    const T bgrad[3] = {nn * sg[0] * hh[1] * hh[2], nn * hh[0] * sg[1] * hh[2], nn * hh[0] * hh[1] * sg[2]};
+    const T gc = gv * hh[0] * hh[1] * hh[2] + gg[0] * bgrad[0] + gg[1] * bgrad[1] + gg[2] * bgrad[2];
+    if (gc != T(0)) atomicAdd(g_coeff + idx, gc);
+    const T c = coeff[idx];
+    const T xy = c * nn * nn * sg[0] * sg[1] * hh[2];
+    const T xz = c * nn * nn * sg[0] * hh[1] * sg[2];
+    const T yz = c * nn * nn * hh[0] * sg[1] * sg[2];
+    qp[0] = qp[0] + gv * c * bgrad[0] + gg[1] * xy + gg[2] * xz;
+    qp[1] = qp[1] + gv * c * bgrad[1] + gg[0] * xy + gg[2] * yz;
+    qp[2] = qp[2] + gv * c * bgrad[2] + gg[0] * xz + gg[1] * yz;
+  }
+}
+
+// evaluate_kernel reversed.  Model frame: p = L q + tr, model gradient = L^T r[1..3]; the
+// adjoints of q (g_q, written), of L and tr (g_ltr: 12 float64 sums, atomic) are produced.
+// Cube frame (isovalue centroids q = sums / w): g_q is the adjoint of the group sums.
+template <class T>
+__global__ void evaluate_reverse_kernel(const HashView h, const T* coeff, const T* cumulative, const T* queries,
+                                        int64_t nq, const T* linear, const T* translation, int depth, const T* g_values,
+                                        const T* g_gradients, T* g_coeff, T* g_cum, T* g_q, double* g_ltr,
+                                        int cube_frame, const T* gsums, const T* gweights) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nq) return;
+  T L[9], tr[3], q[3];
+  if (cube_frame) {
+    for (int a = 0; a < 9; ++a) L[a] = (a % 4 == 0) ? T(1) : T(0);
+    tr[0] = tr[1] = tr[2] = T(0);
+    T w = gweights[i];
+    for (int a = 0; a < 3; ++a) q[a] = gsums[3 * i + a] / w;
+  } else {
+    for (int a = 0; a < 9; ++a) L[a] = linear[a];
+    for (int a = 0; a < 3; ++a) tr[a] = translation[a];
+    for (int a = 0; a < 3; ++a) q[a] = queries[3 * i + a];
+  }
+  const T gv = g_values ? g_values[i] : T(0);
+  T gm[3] = {T(0), T(0), T(0)};
+  if (g_gradients)
+    for (int a = 0; a < 3; ++a) gm[a] = g_gradients[3 * i + a];
+  T gq[3] = {T(0), T(0), T(0)};
+  T p[3];
+  for (int r = 0; r < 3; ++r) p[r] = L[3 * r] * q[0] + L[3 * r + 1] * q[1] + L[3 * r + 2] * q[2] + tr[r];
+  bool ok = isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]) && dmin(p[0], dmin(p[1], p[2])) >= T(0) &&
+            dmax(p[0], dmax(p[1], p[2])) <= T(1);
+  if (ok && (gv != T(0) || gm[0] != T(0) || gm[1] != T(0) || gm[2] != T(0))) {
+    const T orig[3] = {p[0], p[1], p[2]};
+    int leaf = 0;
+    for (int d = depth; d >= 0; --d) {
+      int n = 1 << d;
+      int c[3];
+      for (int a = 0; a < 3; ++a) c[a] = min(max(int(ceil(p[a] * T(n))) - 1, 0), n - 1);
+      if (h.find(basis_key(d, c[0], c[1], c[2])) >= 0) {
+        leaf = d;
+        break;
+      }
+    }
+    for (int a = 0; a < 3; ++a) {
+      if (p[a] == T(0))
+        p[a] = T(1e-6);
+      else if (p[a] == T(1))
+        p[a] = T(1.0 - 1e-6);
+    }
+    // cube-frame spatial seed: model gradient = L^T r  =>  g_r = L g_model
+    const T gg[3] = {L[0] * gm[0] + L[1] * gm[1] + L[2] * gm[2], L[3] * gm[0] + L[4] * gm[1] + L[5] * gm[2],
+                     L[6] * gm[0] + L[7] * gm[1] + L[8] * gm[2]};
+    T qp[3] = {T(0), T(0), T(0)};
+    add_level_reverse(h, coeff, p, leaf, gv, gg, g_coeff, qp);
+    if (leaf > 0) add_level_reverse(h, cumulative, p, leaf - 1, gv, gg, g_cum, qp);
+    if (leaf < depth) add_level_reverse(h, coeff, p, leaf + 1, gv, gg, g_coeff, qp);
+    for (int a = 0; a < 3; ++a)
+      if (orig[a] == T(0) || orig[a] == T(1)) qp[a] = T(0);
+    for (int c = 0; c < 3; ++c) gq[c] = L[c] * qp[0] + L[3 + c] * qp[1] + L[6 + c] * qp[2];
+    if (g_ltr && !cube_frame) {
+      // r[1..3] of the forward, needed for the adjoint of L through the model gradient
+      T r[4] = {T(0), T(0), T(0), T(0)};
+      add_level(h, coeff, p, leaf, r);
+      if (leaf > 0) {
+        T sl[4] = {T(0), T(0), T(0), T(0)};
+        add_level(h, cumulative, p, leaf - 1, sl);
+        for (int a = 0; a < 4; ++a) r[a] = r[a] + sl[a];
+      }
+      if (leaf < depth) {
+        T sl[4] = {T(0), T(0), T(0), T(0)};
+        add_level(h, coeff, p, leaf + 1, sl);
+        for (int a = 0; a < 4; ++a) r[a] = r[a] + sl[a];
+      }
+      for (int rr = 0; rr < 3; ++rr)
+        for (int c = 0; c < 3; ++c) {
+          const double g = double(qp[rr]) * double(q[c]) + double(r[1 + rr]) * double(gm[c]);
+          if (g != 0.0) atomicAdd(g_ltr + 3 * rr + c, g);
+        }
+      for (int rr = 0; rr < 3; ++rr)
+        if (qp[rr] != T(0)) atomicAdd(g_ltr + 9 + rr, double(qp[rr]));
+    }
+  }
+  if (g_q) {
+    if (cube_frame) {
+      const T w = gweights[i];
+      for (int a = 0; a < 3; ++a) g_q[3 * i + a] = g_q[3 * i + a] + gq[a] / w;
+    } else {
+      for (int a = 0; a < 3; ++a) g_q[3 * i + a] = gq[a];
+    }
+  }
+}
+
+// Isovalue reversed (field_adjoint.py:144-152): each centroid value's adjoint is
+// T(g_iso / total weight) * w.
+template <class T>
+__global__ void isovalue_reverse_kernel(const T* weights, int64_t n, double g_iso, const double* mass, T* g_values) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i < n) g_values[i] = T(g_iso / mass[0]) * weights[i];
+}
+
+template <class T>
+__global__ void mass_kernel(const T* weights, int64_t n, double* mass) {
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) acc += double(weights[i]);
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) mass[0] = red[0];
+}
+
+// cumulative_kernel reversed for one depth: g_coeff += g_cum; parents receive h * g_cum.
+template <class T>
+__global__ void cumulative_reverse_kernel(const int64_t* keys, int64_t begin, int64_t end, int d, HashView h, T* g_cum,
+                                          T* g_coeff) {
+  int64_t i = begin + blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= end) return;
+  const T g = g_cum[i];
+  g_coeff[i] = g_coeff[i] + g;
+  if (d == 0 || g == T(0)) return;
+  int c[3];
+  key_coords(keys[i], c);
+  for (int corner = 0; corner < 8; ++corner) {
+    int p[3] = {c[0] / 2 + corner / 4, c[1] / 2 + (corner / 2) % 2, c[2] / 2 + corner % 2};
+    T hw = (T(1) - fabs(T(c[0]) * T(.5) - T(p[0]))) * (T(1) - fabs(T(c[1]) * T(.5) - T(p[1]))) *
+           (T(1) - fabs(T(c[2]) * T(.5) - T(p[2])));
+    if (hw > T(0)) {
+      int32_t idx = h.find(basis_key(d - 1, p[0], p[1], p[2]));
+      if (idx >= 0) atomicAdd(g_cum + idx, g * hw);
+    }
+  }
+}
+
+template <class T>
+void field_backward(const int64_t* keys, const std::vector<int64_t>& offsets, const HashView& h, const T* coeff,
+                    const T* cumulative, int depth, const T* gsums, const T* gweights, int64_t groups, double g_iso,
+                    T* g_coeff, T* g_cum, T* g_sums, cudaStream_t s) {
+  if (g_iso != 0.0 && groups > 0) {
+    DBuf<double> mass(1, s);
+    mass_kernel<T><<<1, 256, 0, s>>>(gweights, groups, mass.p);
+    PSR_LAUNCH_CHECK();
+    DBuf<T> gv(groups, s);
+    isovalue_reverse_kernel<T><<<blocks_for(groups), kThreads, 0, s>>>(gweights, groups, g_iso, mass.p, gv.p);
+    PSR_LAUNCH_CHECK();
+    evaluate_reverse_kernel<T><<<blocks_for(groups, 128), 128, 0, s>>>(h, coeff, cumulative, nullptr, groups, nullptr,
+                                                                       nullptr, depth, gv.p, nullptr, g_coeff, g_cum,
+                                                                       g_sums, nullptr, 1, gsums, gweights);
+    PSR_LAUNCH_CHECK();
+  }
+  for (int d = depth; d >= 0; --d) {
+    int64_t n = offsets[d + 1] - offsets[d];
+    if (!n) continue;
+    cumulative_reverse_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(keys, offsets[d], offsets[d + 1], d, h, g_cum,
+                                                                    g_coeff);
+    PSR_LAUNCH_CHECK();
+  }
+}
+
+template <class T>
+void evaluate_backward(const HashView& h, const T* coeff, const T* cumulative, const T* queries, int64_t nq,
+                       const T* linear, const T* translation, int depth, const T* g_values, const T* g_gradients,
+                       T* g_coeff, T* g_cum, T* g_queries, double* g_ltr, cudaStream_t s) {
+  if (nq <= 0) return;
+  evaluate_reverse_kernel<T><<<blocks_for(nq, 128), 128, 0, s>>>(h, coeff, cumulative, queries, nq, linear,
+                                                                 translation, depth, g_values, g_gradients, g_coeff,
+                                                                 g_cum, g_queries, g_ltr, 0, nullptr, nullptr);
+  PSR_LAUNCH_CHECK();
+}
+
 #define INSTANTIATE(T)                                                                                               \
+  template void field_backward<T>(const int64_t*, const std::vector<int64_t>&, const HashView&, const T*, const T*, \
+                                  int, const T*, const T*, int64_t, double, T*, T*, T*, cudaStream_t);               \
+  template void evaluate_backward<T>(const HashView&, const T*, const T*, const T*, int64_t, const T*, const T*,     \
+                                     int, const T*, const T*, T*, T*, T*, double*, cudaStream_t);                    \
   template void cumulative_coefficients<T>(const int64_t*, const std::vector<int64_t>&, const HashView&, const T*,  \
                                            T*, int, cudaStream_t);                                                   \
   template void evaluate_queries<T>(const int64_t*, const HashView&, const T*, const T*, const T*, int64_t,         \

@@ -4,6 +4,7 @@
 #include "psr_common.cuh"
 
 #include <map>
+#include <memory>
 #include <string>
 
 namespace psr {
@@ -12,6 +13,7 @@ struct Params {
   int depth, full_depth, base_depth, solve_depth, kernel_depth;
   double samples_per_node, scale, point_weight, cg_accuracy;
   int exact, iters, base_v_cycles, precision;
+  int differentiable = 0;
 };
 
 // Optional copies of intermediate arrays, kept for stage-by-stage parity checks.
@@ -47,9 +49,15 @@ struct SampleGroups {
   DBuf<T> weights;            // sample count per group
   DBuf<int32_t> first;        // smallest input index of the group
   DBuf<T> transform;          // [inv, t0, t1, t2, normal_scale]
+  // Kept for the adjoint only (`keep`): group of every input point (-1 when rejected), the
+  // bounding box [lo xyz, hi xyz] and, per bound, the lowest input index attaining it.
+  DBuf<int32_t> input_group;
+  DBuf<T> bounds;
+  DBuf<int32_t> bound_owner;
 };
 template <class T>
-SampleGroups<T> prepare_samples(const T* pos, const T* nrm, int64_t n, int depth, double scale, cudaStream_t s);
+SampleGroups<T> prepare_samples(const T* pos, const T* nrm, int64_t n, int depth, double scale, cudaStream_t s,
+                                bool keep = false);
 
 // ---------------------------------------------------------------- A2 density.py
 template <class T>
@@ -59,9 +67,17 @@ struct DensityData {
   std::vector<int64_t> agg_count;
   DBuf<T> dw;                           // 2 per group: raw splat depth, splat weight
   T scale;
+  // Kept for the adjoint only (`keep`):
+  std::vector<DBuf<int32_t>> parent_of;   // [d]: aggregate index at d-1 of each record at d
+  std::vector<DBuf<int32_t>> splat_order; // [d]: morton order of the depth-d aggregates
+  std::vector<DBuf<int32_t>> splat_slot;  // [d]: unique level value of splat record 27*i+k, or -1
+  std::vector<DBuf<T>> level_values;      // [d]: reduced density splat values
+  std::vector<HashMap> level_hash;        // [d]: their keys
+  DBuf<T> densities;                      // G x (kernel_depth+1) density at each group centroid
 };
 template <class T>
-DensityData<T> build_density(const SampleGroups<T>& g, int depth, int kernel_depth, double spn, cudaStream_t s);
+DensityData<T> build_density(const SampleGroups<T>& g, int depth, int kernel_depth, double spn, cudaStream_t s,
+                             bool keep = false);
 template <class T>
 T density_scale();
 
@@ -73,10 +89,14 @@ struct NormalData {
   DBuf<T> values;                   // 4 per record (negated normal coefficients, 4th = -0)
   std::vector<int64_t> offsets;     // per depth, depth+2 entries
   DBuf<T> average;                  // [mean depth, mean weight, total weight]
+  // Kept for the adjoint only (`keep`): groups in first-index order and the unique record
+  // of every splat record 54*i+k (-1 when the record was not emitted).
+  DBuf<int32_t> group_order;
+  DBuf<int32_t> record_slot;
 };
 template <class T>
 NormalData<T> build_normals(const SampleGroups<T>& g, const DensityData<T>& D, int minimum, int maximum,
-                            cudaStream_t s);
+                            cudaStream_t s, bool keep = false);
 
 // ---------------------------------------------------------------- A4 tree.py
 struct TreeData {
@@ -95,10 +115,22 @@ struct SolveStats {
   std::vector<double> level_relax_ms;
   int64_t finest_row_visits = 0;  // rows x sweeps of the last (finest) sliced level
 };
+// With `tape_out` the solve keeps what its adjoint needs (an opaque SolveTape<T>).
 template <class T>
 void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalData<T>& N,
                   const std::vector<int64_t>& level_offsets, const int64_t* all_keys, const HashMap& all_hash,
-                  const Params& p, T* coefficients, cudaStream_t s, SolveStats* stats, StageSink* sink);
+                  const Params& p, T* coefficients, cudaStream_t s, SolveStats* stats, StageSink* sink,
+                  std::shared_ptr<void>* tape_out = nullptr);
+
+// Reverse pass of solve_levels over its tape: from the adjoint of the per-level coefficients
+// (all levels, key order) to the adjoints of the density aggregates (g_agg[d], 4 per record,
+// accumulated), of the normal average (3, accumulated) and of the normal coefficients
+// (4 per record, accumulated).
+template <class T>
+void solve_backward(void* tape, const TreeData& tree, const DensityData<T>& D, const NormalData<T>& N,
+                    const std::vector<int64_t>& level_offsets, const int64_t* all_keys, const HashMap& all_hash,
+                    const Params& p, const T* g_coef, std::vector<DBuf<T>>& g_agg, T* g_average, T* g_nvals,
+                    cudaStream_t s);
 
 // Ordered sliced relaxation on an ELL level (28 slots per row; slot k < 27 is the k-th
 // lexicographic neighbour, -1 absent).  Rows are referenced through `rows` grouped by
@@ -121,9 +153,15 @@ void build_strip_schedule(const int64_t* keys, int64_t rows, int depth, StripSch
 // Strip-scheduled relaxation of operator rows already in schedule order: values T[28] and
 // group-relative neighbour indices I[32] per row, b with 16 bytes of slack; x in key order
 // holds the initial guess and receives the result.
+//
+// `hist` (optional, iters x rows in schedule order) receives per visit the new x of every row,
+// or with `record_increment` the update r / A_ii.  `rev` runs the colours of a slice in the
+// order 3, 2, 1, 0: on the z-mirrored schedule this is the exact reverse of the forward
+// sequential order (used by the adjoint).
 template <class T, class V, class I>
 void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sidx, const V* sb, V* x, int iters,
-                            cudaStream_t s, float* ms);
+                            cudaStream_t s, float* ms, V* hist = nullptr, bool rev = false,
+                            bool record_increment = false);
 
 // Strip-scheduled ordered relaxation (psr_relax.cu): slot-ELL rows in key order, x in key
 // order holds the initial guess and receives the result.
@@ -143,5 +181,27 @@ template <class T>
 void isovalue(const T* values, const T* weights, int64_t n, T* out, cudaStream_t s);
 template <class T>
 void evaluation_transforms(const T* normalization, T* transforms /* 32 */, cudaStream_t s);
+
+// ---------------------------------------------------------------- A13 reverse passes
+// Isovalue (seed g_iso) through the centroid evaluation, then the cumulative coefficients:
+// g_coeff and g_cum (in/out) end as the adjoint of the per-level coefficients; g_sums (3 per
+// group, accumulated) receives the centroids' share.
+template <class T>
+void field_backward(const int64_t* keys, const std::vector<int64_t>& offsets, const HashView& h, const T* coeff,
+                    const T* cumulative, int depth, const T* gsums, const T* gweights, int64_t groups, double g_iso,
+                    T* g_coeff, T* g_cum, T* g_sums, cudaStream_t s);
+// Model-frame query evaluation reversed: g_coeff, g_cum accumulate; g_queries is written;
+// g_ltr (12 float64: L row-major, then tr) accumulates.
+template <class T>
+void evaluate_backward(const HashView& h, const T* coeff, const T* cumulative, const T* queries, int64_t nq,
+                       const T* linear, const T* translation, int depth, const T* g_values, const T* g_gradients,
+                       T* g_coeff, T* g_cum, T* g_queries, double* g_ltr, cudaStream_t s);
+// Normal splat, splat depths, density and sample preparation reversed onto the inputs.
+template <class T>
+void samples_backward(const SampleGroups<T>& G, const DensityData<T>& D, const NormalData<T>& N, int depth,
+                      int kernel_depth, int base_depth, double samples_per_node, double scale,
+                      std::vector<DBuf<T>>& g_agg, const T* g_average, const T* g_nvals, T* g_sums,
+                      const T* g_transform, const T* pos, const T* nrm, int64_t n, T* g_pos, T* g_nrm,
+                      cudaStream_t s);
 
 }  // namespace psr

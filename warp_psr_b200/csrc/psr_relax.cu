@@ -61,6 +61,10 @@ struct StripLevel {
   int* counter;
   int* error;
   long long* trace;          // optional: 8 timestamps per task
+  void* hist;                // optional V[nvisits_per_slice * rows]: per visit t, what each row recorded
+  int64_t rows;              // rows of the level (stride of `hist`)
+  int record_increment;      // hist holds the update r / A_ii (else the new x)
+  int rev;                   // colours in the order 3, 2, 1, 0 (the mirrored adjoint sweep)
 };
 
 __device__ __forceinline__ long long globaltimer() {
@@ -142,7 +146,7 @@ __device__ __forceinline__ void load_idx(const I* src, I out[kIdxSlots]) {
 // k is not the k-th neighbour) is reported through `error` and not accessed.
 template <int C, class T, class V, class I>
 __device__ __forceinline__ void update_row(const I* nrow, const T* arow, V bv, V* foot, const int* delta,
-                                           unsigned total, int* error) {
+                                           unsigned total, int* error, V* rec, bool record_increment) {
   __align__(16) I n[kIdxSlots];  // filled with 16-byte vector loads
   load_idx(nrow, n);
   __align__(16) T a[kSlotsR];
@@ -166,23 +170,33 @@ __device__ __forceinline__ void update_row(const I* nrow, const T* arow, V bv, V
     atomicExch(error, 3);
     return;
   }
-  if (n[13] >= 0 && a[13] != T(0)) foot[self] = xs[13] + r * (V(1.0) / V(a[13]));
+  V inc = V(0);
+  if (n[13] >= 0 && a[13] != T(0)) {
+    inc = r * (V(1.0) / V(a[13]));
+    foot[self] = xs[13] + inc;
+  }
+  if (rec) *rec = record_increment ? inc : foot[self];
 }
 
+// `hist` (optional) is this visit's record row; only the strip's own rows [o0, o1) write it
+// (halo rows are recomputed by the neighbouring strip, which owns them).
 template <int C, class T, class V, class I>
 __device__ __forceinline__ void phase(const StripLevel& L, bool staged, int p0, int p1, int rbase, int bshift,
                                       const I* s_idx, const T* s_vals, const V* s_b, V* foot, const int* delta,
-                                      unsigned total) {
+                                      unsigned total, V* hist, int o0, int o1) {
   const I* gidx = reinterpret_cast<const I*>(L.nidx);
   const T* gvals = reinterpret_cast<const T*>(L.vals);
   const V* gb = reinterpret_cast<const V*>(L.b);
+  const bool inc = L.record_increment != 0;
   for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+    V* rec = (hist && p >= o0 && p < o1) ? hist + p : nullptr;
     if (staged) {
       int i = rbase + (p - p0);
       update_row<C>(s_idx + int64_t(i) * kIdxSlots, s_vals + int64_t(i) * kSlotsR, s_b[bshift + (p - p0)], foot,
-                    delta, total, L.error);
+                    delta, total, L.error, rec, inc);
     } else {
-      update_row<C>(gidx + int64_t(p) * kIdxSlots, gvals + int64_t(p) * kSlotsR, gb[p], foot, delta, total, L.error);
+      update_row<C>(gidx + int64_t(p) * kIdxSlots, gvals + int64_t(p) * kSlotsR, gb[p], foot, delta, total, L.error,
+                    rec, inc);
     }
   }
 }
@@ -245,7 +259,7 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
         else
           s_lo[r] = v;
       } else {
-        int k = i - 24, c = (k >> 1) & 3, own = k >= 8, h = own ? 0 : 3 - c;
+        int k = i - 24, c = (k >> 1) & 3, own = k >= 8, h = own ? 0 : (L.rev ? c : 3 - c);
         int X = (k & 1) ? min(x1 + h, L.n + 1) : max(min(x0 - h, L.n + 1), 0);
         int v = L.xstart[int64_t(z * 4 + c) * nx + X];
         if (own) {
@@ -359,18 +373,19 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
     if (staged) parity ^= 1;
     __syncthreads();
     if (tr) tr[4] = globaltimer();
-    phase<0, T, V, I>(L, staged, s_p0[0], s_p1[0], s_rbase[0], s_bshift[0], s_idx, s_vals, s_b, foot, s_delta,
-                        unsigned(s_total));
-    __syncthreads();
-    phase<1, T, V, I>(L, staged, s_p0[1], s_p1[1], s_rbase[1], s_bshift[1], s_idx, s_vals, s_b, foot, s_delta,
-                        unsigned(s_total));
-    __syncthreads();
-    phase<2, T, V, I>(L, staged, s_p0[2], s_p1[2], s_rbase[2], s_bshift[2], s_idx, s_vals, s_b, foot, s_delta,
-                        unsigned(s_total));
-    __syncthreads();
-    phase<3, T, V, I>(L, staged, s_p0[3], s_p1[3], s_rbase[3], s_bshift[3], s_idx, s_vals, s_b, foot, s_delta,
-                        unsigned(s_total));
-    __syncthreads();
+    {
+      V* hv = L.hist ? reinterpret_cast<V*>(L.hist) + int64_t(t) * L.rows : nullptr;
+#define PSR_PHASE(C)                                                                                             \
+  phase<C, T, V, I>(L, staged, s_p0[C], s_p1[C], s_rbase[C], s_bshift[C], s_idx, s_vals, s_b, foot, s_delta,   \
+                    unsigned(s_total), hv, s_o0[C], s_o1[C]);                                                  \
+  __syncthreads();
+      if (!L.rev) {
+        PSR_PHASE(0) PSR_PHASE(1) PSR_PHASE(2) PSR_PHASE(3)
+      } else {
+        PSR_PHASE(3) PSR_PHASE(2) PSR_PHASE(1) PSR_PHASE(0)
+      }
+#undef PSR_PHASE
+    }
     if (tr) tr[5] = globaltimer();
     // Publish the strip's own rows (x in [x0, x1)) as visit t.
     {
@@ -431,7 +446,7 @@ __global__ void strip_bounds_kernel(const int32_t* xstart, int n, int strips, in
 }
 
 // Largest footprint, update-row count and staged right-hand-side span over all tasks.
-__global__ void footprint_kernel(const int32_t* xstart, const int32_t* bounds, int n, int strips, int per16,
+__global__ void footprint_kernel(const int32_t* xstart, const int32_t* bounds, int n, int strips, int per16, int rev,
                                  int* caps) {
   int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (n + 1) * strips) return;
@@ -440,7 +455,7 @@ __global__ void footprint_kernel(const int32_t* xstart, const int32_t* bounds, i
   int rows = 0, bspan = 0;
   for (int c = 0; c < 4; ++c) {
     const int32_t* xs = xstart + int64_t(z * 4 + c) * nx;
-    int h = 3 - c;
+    int h = rev ? c : 3 - c;
     int p0 = xs[max(min(x0 - h, n + 1), 0)], p1 = xs[min(x1 + h, n + 1)];
     rows += p1 - p0;
     if (p1 > p0) bspan += (p1 + per16 - 1) / per16 * per16 - (p0 - p0 % per16);
@@ -558,7 +573,7 @@ __global__ void gather_x_kernel(const int32_t* perm, int64_t n, const V* x, V* s
 
 template <class T, class V, class I>
 void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sidx, const V* sb, V* x, int iters,
-                            cudaStream_t s, float* ms) {
+                            cudaStream_t s, float* ms, V* hist, bool rev, bool record_increment) {
   const int64_t rows = S.rows;
   if (iters <= 0 || rows <= 0) return;
   const int depth = S.depth;
@@ -588,7 +603,8 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
   int* counter = flags.p + pad_end;
   int* error = flags.p + pad_end + kPad;
   int* caps_dev = flags.p + pad_end + 2 * kPad;
-  footprint_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, bounds.p, n, strips, per16, caps_dev);
+  footprint_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, bounds.p, n, strips, per16, rev ? 1 : 0,
+                                                                      caps_dev);
   PSR_LAUNCH_CHECK();
   std::vector<int> caps = read_vector(caps_dev, 3, s);
   const int maxfp = caps[0], maxrows = caps[1], maxb = caps[2];
@@ -618,6 +634,10 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
   L.done = flags.p;
   L.counter = counter;
   L.error = error;
+  L.hist = hist;
+  L.rows = rows;
+  L.record_increment = record_increment ? 1 : 0;
+  L.rev = rev ? 1 : 0;
   // Shared memory: the footprint, plus the staged rows of tasks that fit.
   const int64_t budget = std::min<int64_t>(device_smem_optin() - 4096, 220 * 1024);
   const int64_t fp_bytes = (int64_t(std::max(maxfp, 1)) * int64_t(sizeof(V)) + 15) & ~int64_t(15);
@@ -746,7 +766,7 @@ template void relax_sliced_strips<float, double>(const int64_t*, int64_t, int, c
 namespace psr {
 #define PSR_SCHED(T, V, I)                                                                                       \
   template void relax_strips_scheduled<T, V, I>(const StripSchedule&, const T*, const I*, const V*, V*, int,  \
-                                                cudaStream_t, float*);
+                                                cudaStream_t, float*, V*, bool, bool);
 PSR_SCHED(float, float, int16_t)
 PSR_SCHED(float, float, int32_t)
 PSR_SCHED(double, double, int16_t)

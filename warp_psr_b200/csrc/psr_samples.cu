@@ -142,6 +142,42 @@ __global__ void groups_kernel(const uint64_t* __restrict__ keys, const int32_t* 
   first[g] = order[i];
 }
 
+// Adjoint bookkeeping: bounding box and the lowest input index attaining each bound.
+template <class T>
+__global__ void bounds_final_kernel(const T* partial, int blocks, T* bounds) {
+  if (threadIdx.x != 0) return;
+  T lo[3] = {T(INFINITY), T(INFINITY), T(INFINITY)}, hi[3] = {T(-INFINITY), T(-INFINITY), T(-INFINITY)};
+  for (int b = 0; b < blocks; ++b)
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = dmin(lo[a], partial[6 * b + a]);
+      hi[a] = dmax(hi[a], partial[6 * b + 3 + a]);
+    }
+  for (int a = 0; a < 3; ++a) {
+    bounds[a] = lo[a];
+    bounds[3 + a] = hi[a];
+  }
+}
+
+template <class T>
+__global__ void bound_owner_kernel(const T* __restrict__ pos, int64_t n, const T* bounds, int32_t* owner) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  T p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+  if (!(isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]))) return;
+  for (int a = 0; a < 3; ++a) {
+    if (p[a] == bounds[a]) atomicMin(owner + a, int32_t(i));
+    if (p[a] == bounds[3 + a]) atomicMin(owner + 3 + a, int32_t(i));
+  }
+}
+
+// Group of every input point (-1 for points rejected by the classification).
+__global__ void input_group_kernel(const uint64_t* __restrict__ keys, const int32_t* __restrict__ order,
+                                   const int32_t* __restrict__ prefix, int64_t n, uint64_t sentinel, int32_t* group) {
+  int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (j >= n) return;
+  group[order[j]] = keys[j] < sentinel ? prefix[j] - 1 : -1;
+}
+
 // Marks segment heads of sorted keys and returns the number of segments.
 static int64_t segment_heads(const uint64_t* keys, int64_t n, uint64_t sentinel, int shift, DBuf<int32_t>& heads,
                              DBuf<int32_t>& prefix, cudaStream_t s) {
@@ -155,7 +191,8 @@ static int64_t segment_heads(const uint64_t* keys, int64_t n, uint64_t sentinel,
 }
 
 template <class T>
-SampleGroups<T> prepare_samples(const T* pos, const T* nrm, int64_t n, int depth, double scale, cudaStream_t s) {
+SampleGroups<T> prepare_samples(const T* pos, const T* nrm, int64_t n, int depth, double scale, cudaStream_t s,
+                                bool keep) {
   SampleGroups<T> G;
   int blocks = int(blocks_for(n) < 592 ? blocks_for(n) : 592);
   DBuf<T> partial(6 * blocks, s);
@@ -168,6 +205,15 @@ SampleGroups<T> prepare_samples(const T* pos, const T* nrm, int64_t n, int depth
   transform_kernel<T><<<1, 32, 0, s>>>(partial.p, blocks, T(scale), G.transform.p, status.p);
   PSR_LAUNCH_CHECK();
   if (read_scalar(status.p, s)) throw Error(3, "Nonfinite positions or degenerate/overflowing bounding cube");
+  if (keep) {
+    G.bounds.alloc(6, s);
+    bounds_final_kernel<T><<<1, 32, 0, s>>>(partial.p, blocks, G.bounds.p);
+    PSR_LAUNCH_CHECK();
+    G.bound_owner.alloc(6, s);
+    PSR_CUDA(cudaMemsetAsync(G.bound_owner.p, 0x7f, 6 * sizeof(int32_t), s));
+    bound_owner_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(pos, n, G.bounds.p, G.bound_owner.p);
+    PSR_LAUNCH_CHECK();
+  }
   DBuf<T> q(3 * n, s), un(3 * n, s);
   DBuf<uint64_t> keys(n, s), skeys(n, s);
   DBuf<int32_t> ids(n, s), order(n, s);
@@ -187,6 +233,11 @@ SampleGroups<T> prepare_samples(const T* pos, const T* nrm, int64_t n, int depth
   groups_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(skeys.p, order.p, heads.p, prefix.p, n, q.p, un.p, depth,
                                                       G.keys.p, G.sums.p, G.normal_sums.p, G.weights.p, G.first.p);
   PSR_LAUNCH_CHECK();
+  if (keep) {
+    G.input_group.alloc(n, s);
+    input_group_kernel<<<blocks_for(n), kThreads, 0, s>>>(skeys.p, order.p, prefix.p, n, sentinel, G.input_group.p);
+    PSR_LAUNCH_CHECK();
+  }
   return G;
 }
 
@@ -355,9 +406,25 @@ __global__ void depths_kernel(const T* dens, int64_t G, int kernel_depth, T targ
   dw[2 * i + 1] = h * h / density;
 }
 
+// Adjoint bookkeeping: map every sorted record to its segment (unique key) index.
+__global__ void segment_slot_kernel(const int32_t* order, const int32_t* prefix, const uint64_t* skeys, int64_t n,
+                                    uint64_t sentinel, int shift, int32_t* slot) {
+  int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (j >= n) return;
+  slot[order[j]] = (skeys[j] >> shift) < (sentinel >> shift) ? prefix[j] - 1 : -1;
+}
+
 template <class T>
-DensityData<T> build_density(const SampleGroups<T>& g, int depth, int kernel_depth, double spn, cudaStream_t s) {
+DensityData<T> build_density(const SampleGroups<T>& g, int depth, int kernel_depth, double spn, cudaStream_t s,
+                             bool keep) {
   DensityData<T> D;
+  if (keep) {
+    D.parent_of.resize(depth + 1);
+    D.splat_order.resize(kernel_depth + 1);
+    D.splat_slot.resize(kernel_depth + 1);
+    D.level_values.resize(kernel_depth + 1);
+    D.level_hash.resize(kernel_depth + 1);
+  }
   int64_t G = g.count;
   D.agg_keys.resize(depth + 1);
   D.agg_values.resize(depth + 1);
@@ -384,6 +451,12 @@ DensityData<T> build_density(const SampleGroups<T>& g, int depth, int kernel_dep
                                                                D.agg_values[d].p, d, D.agg_keys[d - 1].p,
                                                                D.agg_values[d - 1].p);
     PSR_LAUNCH_CHECK();
+    if (keep) {
+      D.parent_of[d].alloc(n, s);
+      segment_slot_kernel<<<blocks_for(n), kThreads, 0, s>>>(order.p, prefix.p, scomp.p, n, ~uint64_t(0), 0,
+                                                             D.parent_of[d].p);
+      PSR_LAUNCH_CHECK();
+    }
   }
   D.scale = density_scale<T>();
   DBuf<T> dens(G * (kernel_depth + 1), s);
@@ -415,10 +488,20 @@ DensityData<T> build_density(const SampleGroups<T>& g, int depth, int kernel_dep
     density_eval_kernel<T><<<blocks_for(G), kThreads, 0, s>>>(hm.view(), lvals.p, g.sums.p, g.weights.p, G, d,
                                                               kernel_depth + 1, dens.p);
     PSR_LAUNCH_CHECK();
+    if (keep) {
+      D.splat_slot[d].alloc(r, s);
+      segment_slot_kernel<<<blocks_for(r), kThreads, 0, s>>>(rorder.p, prefix.p, skeys.p, r, uint64_t(1) << (3 * Db),
+                                                             0, D.splat_slot[d].p);
+      PSR_LAUNCH_CHECK();
+      D.splat_order[d] = std::move(order);
+      D.level_values[d] = std::move(lvals);
+      D.level_hash[d] = std::move(hm);
+    }
   }
   D.dw.alloc(2 * G, s);
   depths_kernel<T><<<blocks_for(G), kThreads, 0, s>>>(dens.p, G, kernel_depth, T(spn), D.dw.p);
   PSR_LAUNCH_CHECK();
+  if (keep) D.densities = std::move(dens);
   return D;
 }
 
@@ -568,7 +651,7 @@ __global__ void depth_offsets_kernel(const int64_t* keys, int64_t n, int levels,
 
 template <class T>
 NormalData<T> build_normals(const SampleGroups<T>& g, const DensityData<T>& D, int minimum, int maximum,
-                            cudaStream_t s) {
+                            cudaStream_t s, bool keep) {
   NormalData<T> N;
   int64_t n = g.count;
   DBuf<uint32_t> fk(n, s), sfk(n, s);
@@ -594,6 +677,12 @@ NormalData<T> build_normals(const SampleGroups<T>& g, const DensityData<T>& D, i
     normal_reduce_kernel<T><<<blocks_for(r), kThreads, 0, s>>>(skeys.p, rorder.p, heads.p, prefix.p, r, rvals.p, Db,
                                                                N.keys.p, N.values.p);
     PSR_LAUNCH_CHECK();
+    if (keep) {
+      N.record_slot.alloc(r, s);
+      segment_slot_kernel<<<blocks_for(r), kThreads, 0, s>>>(rorder.p, prefix.p, skeys.p, r,
+                                                             uint64_t(1) << (3 * Db + 4), 0, N.record_slot.p);
+      PSR_LAUNCH_CHECK();
+    }
   }
   int64_t chunks = (n + 1023) / 1024;
   DBuf<T> partial(3 * chunks, s), contrib(3 * n, s);
@@ -609,18 +698,23 @@ NormalData<T> build_normals(const SampleGroups<T>& g, const DensityData<T>& D, i
   depth_offsets_kernel<<<1, 32, 0, s>>>(N.keys.p, N.count, maximum + 2, off.p);
   PSR_LAUNCH_CHECK();
   N.offsets = read_vector(off.p, maximum + 2, s);
+  if (keep) N.group_order = std::move(order);
   return N;
 }
 
-template SampleGroups<float> prepare_samples<float>(const float*, const float*, int64_t, int, double, cudaStream_t);
-template SampleGroups<double> prepare_samples<double>(const double*, const double*, int64_t, int, double, cudaStream_t);
-template DensityData<float> build_density<float>(const SampleGroups<float>&, int, int, double, cudaStream_t);
-template DensityData<double> build_density<double>(const SampleGroups<double>&, int, int, double, cudaStream_t);
+template SampleGroups<float> prepare_samples<float>(const float*, const float*, int64_t, int, double, cudaStream_t,
+                                                   bool);
+template SampleGroups<double> prepare_samples<double>(const double*, const double*, int64_t, int, double,
+                                                     cudaStream_t, bool);
+template DensityData<float> build_density<float>(const SampleGroups<float>&, int, int, double, cudaStream_t, bool);
+template DensityData<double> build_density<double>(const SampleGroups<double>&, int, int, double, cudaStream_t, bool);
 template NormalData<float> build_normals<float>(const SampleGroups<float>&, const DensityData<float>&, int, int,
-                                                cudaStream_t);
+                                                cudaStream_t, bool);
 template NormalData<double> build_normals<double>(const SampleGroups<double>&, const DensityData<double>&, int, int,
-                                                  cudaStream_t);
+                                                  cudaStream_t, bool);
 template float density_scale<float>();
 template double density_scale<double>();
+
+#include "psr_samples_adjoint.cuh"
 
 }  // namespace psr

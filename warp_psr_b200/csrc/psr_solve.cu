@@ -531,9 +531,10 @@ template <class V>
 __device__ __forceinline__ void st_x(V* x, int64_t i, V v) { __stcg(x + i, v); }
 
 // relaxation.py:51-62, one row: r = b_i - sum_k x[c_k] A_k (slot order); x_i += r / A_ii.
+// With `rec` (adjoint tape) the row's old x and residual r are stored at rec[0], rec[1].
 template <class T, class V>
 __device__ __forceinline__ void gs_row(const int32_t* __restrict__ cols, const T* __restrict__ vals,
-                                       const V* __restrict__ b, V* x, int32_t row) {
+                                       const V* __restrict__ b, V* x, int32_t row, V* rec = nullptr) {
   const int4* cr = reinterpret_cast<const int4*>(cols + int64_t(row) * kSlots);
   int cc[kSlots];
 #pragma unroll
@@ -562,6 +563,10 @@ __device__ __forceinline__ void gs_row(const int32_t* __restrict__ cols, const T
       diagonal = aa[k];
       xi = xs[k];
     }
+  }
+  if (rec) {
+    rec[0] = xi;
+    rec[1] = r;
   }
   if (diagonal != T(0)) st_x(x, row, xi + r * (V(1.0) / V(diagonal)));
 }
@@ -634,15 +639,17 @@ __global__ void __launch_bounds__(512) sliced_gs_kernel(const int32_t* __restric
   }
 }
 
-// Eight-colour relaxation of a small level by one CTA (relaxation.py:261-271).
+// Eight-colour relaxation of a small level by one CTA (relaxation.py:261-271).  With `hist`
+// (adjoint tape) visit `it` of row i stores (old x, r) at hist[2 * (it * n + i)].
 template <class T>
 __global__ void __launch_bounds__(512) relax_colors_kernel(const int32_t* cols, const T* vals, const T* b, T* x,
                                                             const int32_t* rows, const int32_t* group_off, int iters,
-                                                            int forward) {
+                                                            int forward, T* hist = nullptr, int64_t n = 0) {
   for (int it = 0; it < iters; ++it)
     for (int cc = 0; cc < 8; ++cc) {
       int g = forward ? cc : 7 - cc;
-      for (int j = group_off[g] + threadIdx.x; j < group_off[g + 1]; j += blockDim.x) gs_row(cols, vals, b, x, rows[j]);
+      for (int j = group_off[g] + threadIdx.x; j < group_off[g + 1]; j += blockDim.x)
+        gs_row(cols, vals, b, x, rows[j], hist ? hist + 2 * (int64_t(it) * n + rows[j]) : nullptr);
       __syncthreads();
     }
 }
@@ -926,6 +933,37 @@ __global__ void narrow_kernel(const T* in, int64_t n, float* out) {
   if (i < n) out[i] = float(in[i]);
 }
 
+// ------------------------------------------------------------------ adjoint tape of the solve
+// What the reverse pass needs from the forward solve, kept only when a reconstruction is
+// differentiable.  Everything is in the forward's own layout.
+template <class T>
+struct SlicedTape {
+  bool on = false;
+  StripSchedule sched;
+  DBuf<char> svals, sidx;  // schedule-order operator rows (float32 values in the mixed precision)
+  DBuf<T> b;               // schedule-order right-hand side after the cross term
+  DBuf<T> hist;            // iters x n (schedule order): x after each visit
+};
+
+template <class T>
+struct SolveTape {
+  int base = 0, top = -1;  // solved depths base..top
+  bool screened = false, mixed = false, dc = false;
+  std::vector<PointsData<T>> points;        // per depth (screened levels)
+  std::vector<DBuf<int32_t>> pcol;          // per depth: prolongation from d-1 (8 slots per fine row)
+  std::vector<DBuf<T>> pval;
+  std::vector<DBuf<T>> cum;                 // cumulative solution after solving depth d (key order)
+  std::vector<SlicedTape<T>> sliced;        // per depth > base
+  // base multigrid: level operators (index base = the assembled level, below = Galerkin)
+  std::vector<DBuf<int32_t>> mcols;
+  std::vector<DBuf<T>> mvals;
+  std::vector<Schedule> msched;
+  DBuf<T> base_b;
+  std::vector<DBuf<T>> relax_hist;          // per colour-relaxation call, in call order
+  std::vector<DBuf<T>> resid_x;             // per residual call: x of that level at the time
+  std::vector<DBuf<T>> root_x0, root_b;     // per cycle: root CG starting point (64) and right-hand side
+};
+
 // ------------------------------------------------------------------ orchestration
 struct LevelOp {
   DBuf<int32_t> cols;
@@ -974,8 +1012,22 @@ static PointsData<T> make_points(const DensityData<T>& D, const NormalData<T>& N
 template <class T>
 void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalData<T>& N,
                   const std::vector<int64_t>& level_offsets, const int64_t* all_keys, const HashMap& all_hash,
-                  const Params& p, T* coefficients, cudaStream_t s, SolveStats* stats, StageSink* sink) {
+                  const Params& p, T* coefficients, cudaStream_t s, SolveStats* stats, StageSink* sink,
+                  std::shared_ptr<void>* tape_out) {
   const int finest = p.depth, base = p.base_depth;
+  std::shared_ptr<SolveTape<T>> tape_holder;
+  SolveTape<T>* tp = nullptr;
+  if (tape_out) {
+    tape_holder = std::make_shared<SolveTape<T>>();
+    tp = tape_holder.get();
+    *tape_out = tape_holder;
+    tp->base = base;
+    tp->points.resize(finest + 1);
+    tp->cum.resize(finest + 1);
+    tp->sliced.resize(finest + 1);
+    tp->mcols.resize(base + 1);
+    tp->mvals.resize(base + 1);
+  }
   HashView bh = all_hash.view();
   auto keys_at = [&](int d) { return all_keys + level_offsets[d]; };
   auto count_at = [&](int d) { return level_offsets[d + 1] - level_offsets[d]; };
@@ -1070,10 +1122,15 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
   }
 
   const bool screened = p.point_weight > 0 && !p.exact;
+  if (tp) {
+    tp->screened = screened;
+    tp->mixed = sizeof(T) == 8 && p.precision == 1;
+  }
   DBuf<T> cumulative;
   for (int d = base; d <= p.solve_depth; ++d) {
     int64_t n = count_at(d);
     if (!n) break;
+    if (tp) tp->top = d;
     PointsData<T> P;
     if (screened) P = make_points(D, N, tree, d, p.point_weight, bool(p.exact), s);
     PointsView<T> pv = screened ? P.view() : PointsView<T>();
@@ -1170,12 +1227,24 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
       bool dc = base == 0 && p.point_weight == 0;
       DBuf<T> root_state(64, s);
       root_state.zero();
+      // Adjoint tape: (old x, r) of every colour-relaxation visit, x at every residual, and
+      // the root solve's inputs.
+      auto relax_hist = [&](int l) -> T* {
+        if (!tp) return nullptr;
+        tp->relax_hist.emplace_back(2 * int64_t(p.iters) * count_at(l), s);
+        return tp->relax_hist.back().p;
+      };
       for (int cycle = 0; cycle < p.base_v_cycles; ++cycle) {
         for (int l = base; l > 0; --l) {
           int64_t nl = count_at(l);
+          T* rh = relax_hist(l);
           relax_colors_kernel<T><<<1, 512, 0, s>>>(Cl(l), Vl(l), Rl(l), Xl(l), sched[l].rows.p, sched[l].off.p,
-                                                    p.iters, 1);
+                                                    p.iters, 1, rh, nl);
           PSR_LAUNCH_CHECK();
+          if (tp) {
+            tp->resid_x.emplace_back(nl, s);
+            PSR_CUDA(cudaMemcpyAsync(tp->resid_x.back().p, Xl(l), nl * sizeof(T), cudaMemcpyDeviceToDevice, s));
+          }
           DBuf<T> r(nl, s);
           residual_kernel<T><<<blocks_for(nl), kThreads, 0, s>>>(Cl(l), Vl(l), Rl(l), Xl(l), nl, r.p);
           PSR_LAUNCH_CHECK();
@@ -1185,6 +1254,17 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
           PSR_LAUNCH_CHECK();
           PSR_CUDA(cudaMemsetAsync(xs[l - 1].p, 0, nc * sizeof(T), s));
         }
+        if (tp) {
+          const int64_t n0 = count_at(0);
+          tp->root_b.emplace_back(n0, s);
+          PSR_CUDA(cudaMemcpyAsync(tp->root_b.back().p, Rl(0), n0 * sizeof(T), cudaMemcpyDeviceToDevice, s));
+          tp->root_x0.emplace_back(64, s);
+          tp->root_x0.back().zero();
+          if (dc)
+            PSR_CUDA(cudaMemcpyAsync(tp->root_x0.back().p, root_state.p, 64 * sizeof(T), cudaMemcpyDeviceToDevice, s));
+          else
+            PSR_CUDA(cudaMemcpyAsync(tp->root_x0.back().p, Xl(0), n0 * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        }
         root_solve_kernel<T><<<1, 32, 0, s>>>(keys_at(0), int(count_at(0)), Cl(0), Vl(0), Rl(0), Xl(0), root_state.p,
                                               dc, p.cg_accuracy, base, cycle);
         PSR_LAUNCH_CHECK();
@@ -1193,14 +1273,26 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
           prolong_add_kernel<T><<<blocks_for(nl), kThreads, 0, s>>>(pcol[l].p, pval[l].p, nl, Xl(l - 1), Xl(l));
           PSR_LAUNCH_CHECK();
           PSR_CUDA(cudaMemsetAsync(xs[l - 1].p, 0, count_at(l - 1) * sizeof(T), s));
+          T* rh = relax_hist(l);
           relax_colors_kernel<T><<<1, 512, 0, s>>>(Cl(l), Vl(l), Rl(l), Xl(l), sched[l].rows.p, sched[l].off.p,
-                                                    p.iters, 0);
+                                                    p.iters, 0, rh, nl);
           PSR_LAUNCH_CHECK();
         }
       }
+      if (tp) {
+        tp->dc = dc;
+        tp->mcols[base] = std::move(cols);
+        tp->mvals[base] = std::move(vals);
+        tp->base_b = std::move(b);
+        for (int l = 0; l < base; ++l) {
+          tp->mcols[l] = std::move(mc[l]);
+          tp->mvals[l] = std::move(mv[l]);
+        }
+        tp->msched = std::move(sched);
+      }
       cumulative.alloc(n, s);
       PSR_CUDA(cudaMemcpyAsync(cumulative.p, x, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
-      if (sink) sink->put("rhs_" + std::to_string(d), b.p, n, s);
+      if (sink) sink->put("rhs_" + std::to_string(d), tp ? tp->base_b.p : b.p, n, s);
     } else {
       DBuf<double> ctable(int64_t(res + 1) * 6, s);
       stiffness_table_kernel<<<blocks_for(res + 1), kThreads, 0, s>>>(d, d - 1, ctable.p);
@@ -1221,20 +1313,26 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
       }
       float ms = 0;
       float* msp = stats ? &ms : nullptr;
+      DBuf<T> hist;
+      if (tp) hist.alloc(int64_t(p.iters) * n, s);
       if (mixed) {
         if (sched.wide)
           relax_strips_scheduled<float, T, int32_t>(sched, reinterpret_cast<const float*>(svals.p),
-                                                    reinterpret_cast<const int32_t*>(sidx.p), b.p, x, p.iters, s, msp);
+                                                    reinterpret_cast<const int32_t*>(sidx.p), b.p, x, p.iters, s, msp,
+                                                    hist.p);
         else
           relax_strips_scheduled<float, T, int16_t>(sched, reinterpret_cast<const float*>(svals.p),
-                                                    reinterpret_cast<const int16_t*>(sidx.p), b.p, x, p.iters, s, msp);
+                                                    reinterpret_cast<const int16_t*>(sidx.p), b.p, x, p.iters, s, msp,
+                                                    hist.p);
       } else {
         if (sched.wide)
           relax_strips_scheduled<T, T, int32_t>(sched, reinterpret_cast<const T*>(svals.p),
-                                                reinterpret_cast<const int32_t*>(sidx.p), b.p, x, p.iters, s, msp);
+                                                reinterpret_cast<const int32_t*>(sidx.p), b.p, x, p.iters, s, msp,
+                                                hist.p);
         else
           relax_strips_scheduled<T, T, int16_t>(sched, reinterpret_cast<const T*>(svals.p),
-                                                reinterpret_cast<const int16_t*>(sidx.p), b.p, x, p.iters, s, msp);
+                                                reinterpret_cast<const int16_t*>(sidx.p), b.p, x, p.iters, s, msp,
+                                                hist.p);
       }
       if (stats) {
         stats->relax_ms += ms;
@@ -1248,16 +1346,36 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
       prolong_add_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(pcol[d].p, pval[d].p, n, cumulative.p, next.p);
       PSR_LAUNCH_CHECK();
       cumulative = std::move(next);
+      if (tp) {
+        SlicedTape<T>& st = tp->sliced[d];
+        st.on = true;
+        st.sched = std::move(sched);
+        st.svals = std::move(svals);
+        st.sidx = std::move(sidx);
+        st.b = std::move(b);
+        st.hist = std::move(hist);
+      }
     }
+    if (tp) {
+      tp->cum[d].alloc(n, s);
+      PSR_CUDA(cudaMemcpyAsync(tp->cum[d].p, cumulative.p, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+      if (screened) tp->points[d] = std::move(P);
+    }
+  }
+  if (tp) {
+    tp->pcol = std::move(pcol);
+    tp->pval = std::move(pval);
   }
 }
 
 template void solve_levels<float>(const TreeData&, const DensityData<float>&, const NormalData<float>&,
                                   const std::vector<int64_t>&, const int64_t*, const HashMap&, const Params&, float*,
-                                  cudaStream_t, SolveStats*, StageSink*);
+                                  cudaStream_t, SolveStats*, StageSink*, std::shared_ptr<void>*);
 template void solve_levels<double>(const TreeData&, const DensityData<double>&, const NormalData<double>&,
                                    const std::vector<int64_t>&, const int64_t*, const HashMap&, const Params&, double*,
-                                   cudaStream_t, SolveStats*, StageSink*);
+                                   cudaStream_t, SolveStats*, StageSink*, std::shared_ptr<void>*);
+#include "psr_solve_adjoint.cuh"
+
 template void relax_sliced_ell<float, float>(const int32_t*, const float*, const float*, float*, const int32_t*,
                                              const int32_t*, int, int, cudaStream_t, float*);
 template void relax_sliced_ell<double, double>(const int32_t*, const double*, const double*, double*, const int32_t*,

@@ -151,7 +151,7 @@ STAGES = ("samples", "density", "normal_field", "tree", "assembly_and_solve", "f
 
 def reconstruct(positions, normals, *, depth=6, full_depth=3, base_depth=None, solve_depth=None, kernel_depth=None,
                 samples_per_node=1.5, scale=1.1, point_weight=2.0, exact_interpolation=False, iters=8,
-                base_v_cycles=1, cg_accuracy=1e-3, precision="input", keep_stages=False):
+                base_v_cycles=1, cg_accuracy=1e-3, precision="input", keep_stages=False, _differentiable=False):
     """Reconstruct oriented CUDA float32/float64 vectors; point_weight=0 selects PSR.
 
     Degree one, Neumann boundaries, confidence disabled.  The return value evaluates the
@@ -182,7 +182,7 @@ def reconstruct(positions, normals, *, depth=6, full_depth=3, base_depth=None, s
     params = _lib.Params(depth, full_depth, base_depth, solve_depth, kernel_depth, float(samples_per_node),
                          float(scale), float(point_weight), float(cg_accuracy), int(bool(exact_interpolation)), iters,
                          base_v_cycles, _lib.PSR_PRECISION_MIXED if precision == "mixed" else _lib.PSR_PRECISION_INPUT,
-                         int(bool(keep_stages)))
+                         int(bool(keep_stages)), int(bool(_differentiable)))
     L = _lib.load()
     out = ctypes.c_void_p()
     dtype_code = _lib.PSR_FLOAT64 if p.dtype == torch.float64 else _lib.PSR_FLOAT32
@@ -246,5 +246,136 @@ def reconstruct(positions, normals, *, depth=6, full_depth=3, base_depth=None, s
                    "relax_seconds": info.relax_ms / 1000.0, "relax_row_visits": int(info.relax_row_visits),
                    "relax_launches": int(info.relax_launches),
                    "relax_finest_seconds": info.relax_finest_ms / 1000.0,
-                   "relax_finest_row_visits": int(info.relax_finest_row_visits)}
+                   "relax_finest_row_visits": int(info.relax_finest_row_visits),
+                   "normalization": tuple(info.normalization)}
     return Reconstruction(field, metadata, diagnostics)
+
+
+# ---------------------------------------------------------------- differentiable reconstruction
+class _ReconstructFunction(torch.autograd.Function):
+    """Forward: a differentiable reconstruction.  Outputs the per-level coefficients, the
+    cumulative coefficients, the isovalue and the 5-value sample normalisation; backward is
+    the library's reverse pass (psr_backward) onto positions and normals."""
+
+    @staticmethod
+    def forward(ctx, positions, normals, box, options):
+        result = reconstruct(positions.detach(), normals.detach(), _differentiable=True, **options)
+        field = result.field
+        dtype, device = field.coefficients.dtype, field.coefficients.device
+        box["result"] = result
+        ctx.box = box
+        ctx.save_for_backward(positions, normals)
+        iso = torch.tensor(field.iso_value, dtype=dtype, device=device)
+        normalization = torch.tensor(result.diagnostics["normalization"], dtype=dtype, device=device)
+        return field.coefficients.clone(), field.cumulative.clone(), iso, normalization
+
+    @staticmethod
+    def backward(ctx, g_coef, g_cum, g_iso, g_norm):
+        positions, normals = ctx.saved_tensors
+        result = ctx.box["result"]
+        p = positions.detach().contiguous()
+        n = normals.detach().contiguous()
+        dtype = result.field.coefficients.dtype
+        g_p = torch.empty_like(p)
+        g_n = torch.empty_like(n)
+
+        def ptr(t):
+            return 0 if t is None else t.to(dtype).contiguous().data_ptr()
+
+        keep = [t.to(dtype).contiguous() if t is not None else None for t in (g_coef, g_cum, g_norm)]
+        dtype_code = _lib.PSR_FLOAT64 if p.dtype == torch.float64 else _lib.PSR_FLOAT32
+        with torch.cuda.device(p.device):
+            _lib.check(_lib.load().psr_backward(
+                result.field._handle.ptr, p.data_ptr(), n.data_ptr(), p.shape[0], dtype_code,
+                ptr(keep[0]), ptr(keep[1]), float(g_iso) if g_iso is not None else 0.0, ptr(keep[2]),
+                g_p.data_ptr(), g_n.data_ptr(), _stream(p.device)))
+        return (g_p if ctx.needs_input_grad[0] else None), (g_n if ctx.needs_input_grad[1] else None), None, None
+
+
+class _EvaluateFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, coefficients, cumulative, iso, normalization, queries, result, centered):
+        values, gradients, valid = result.field.evaluate(queries.detach())
+        ctx.result = result
+        ctx.centered = centered
+        ctx.save_for_backward(queries)
+        ctx.mark_non_differentiable(valid)
+        if centered:
+            values = values - iso.detach()
+        return values, gradients, valid
+
+    @staticmethod
+    def backward(ctx, g_values, g_gradients, _g_valid):
+        (queries,) = ctx.saved_tensors
+        result = ctx.result
+        field = result.field
+        dtype = field.coefficients.dtype
+        q = queries.detach().contiguous()
+        g_coef = torch.zeros_like(field.coefficients)
+        g_cum = torch.zeros_like(field.cumulative)
+        g_q = torch.zeros_like(q)
+        g_norm = torch.zeros(5, dtype=dtype, device=q.device)
+        gv = g_values.to(dtype).contiguous() if g_values is not None else None
+        gg = g_gradients.to(dtype).contiguous() if g_gradients is not None else None
+        with torch.cuda.device(q.device):
+            _lib.check(_lib.load().psr_evaluate_backward(
+                field._handle.ptr, q.data_ptr(), q.shape[0], gv.data_ptr() if gv is not None else 0,
+                gg.data_ptr() if gg is not None else 0, g_coef.data_ptr(), g_cum.data_ptr(), g_q.data_ptr(),
+                g_norm.data_ptr(), _stream(q.device)))
+        g_iso = None
+        if ctx.centered and gv is not None:
+            valid = torch.isfinite(gv)
+            g_iso = -gv[valid].sum()
+        return g_coef, g_cum, g_iso, g_norm, g_q, None, None
+
+
+class DifferentiableReconstruction:
+    """Result of reconstruct_differentiable (warp-psr reconstruction_adjoint.py:45-58).
+
+    ``evaluate(queries, centered=False)`` returns (values, model-space gradients, valid) as
+    torch tensors connected to the autograd graph of the input positions and normals;
+    ``iso_value`` is a 0-d tensor on the same graph.
+    """
+
+    def __init__(self, coefficients, cumulative, iso, normalization, result):
+        self.coefficients = coefficients
+        self.cumulative = cumulative
+        self.iso_value = iso
+        self.normalization = normalization
+        self.result = result
+        self.metadata = dict(result.metadata)
+        self.metadata["differentiability"] = {
+            "mode": "finite_algorithm_fixed_assignments", "inputs": ["positions", "normals"],
+            "constant_options": ["point_weight", "scale", "samples_per_node", "cg_accuracy", "depths", "iterations"],
+            "first_order_only": True}
+        self.diagnostics = result.diagnostics
+
+    def evaluate(self, queries, *, centered=False):
+        q = _as_vec3(queries, "queries")
+        dtype = self.result.field.coefficients.dtype
+        if q.dtype != dtype or q.device != self.coefficients.device:
+            raise ValueError("queries must match field precision and device")
+        return _EvaluateFunction.apply(self.coefficients, self.cumulative, self.iso_value, self.normalization, q,
+                                       self.result, bool(centered))
+
+
+def reconstruct_differentiable(positions, normals, **options):
+    """Differentiable reconstruction (warp-psr reconstruction_adjoint.py:61-185).
+
+    Same options as ``reconstruct``.  Positions and/or normals must require gradients; the
+    VJP is that of the finite algorithm with its discrete choices (groups, tree, bins,
+    schedules, CG stopping points) fixed, first order.  Inputs must stay unchanged until
+    backward has run.
+    """
+    if not isinstance(positions, torch.Tensor) or not isinstance(normals, torch.Tensor):
+        raise TypeError("positions and normals must be torch tensors")
+    if not positions.requires_grad and not normals.requires_grad:
+        raise ValueError("track positions and/or normals with requires_grad=True")
+    for name, value in options.items():
+        if isinstance(value, torch.Tensor):
+            raise ValueError(f"{name} must be a constant scalar; only positions and normals support gradients")
+    if options.get("keep_stages"):
+        raise ValueError("keep_stages is not available for differentiable reconstructions")
+    box = {}
+    coefficients, cumulative, iso, normalization = _ReconstructFunction.apply(positions, normals, box, options)
+    return DifferentiableReconstruction(coefficients, cumulative, iso, normalization, box["result"])
