@@ -1,10 +1,11 @@
 #!/usr/bin/env python
 """Depth-9 screened-Poisson benchmark (synthetic stand-in for the eagle scan, 800k points).
 
-One step = one full reconstruction (sample grouping, density and normal splats, tree,
-operator assembly, cascadic ordered Gauss-Seidel solve, field and isovalue) of an 800k-point
-bumpy sphere at depth 9, full depth 4, point weight 2, in the mixed precision the metric names
-(float64 solve, float32 relaxation operators).  Multi-GPU runs are independent replicas
+One step = one solve+adjoint: a differentiable reconstruction (sample grouping, density and
+normal splats, tree, operator assembly, cascadic ordered Gauss-Seidel solve, field and
+isovalue) of an 800k-point bumpy sphere at depth 9, full depth 4, point weight 2, a loss on
+32 isovalue-centred field values, and the reverse pass onto positions and normals; in the
+mixed precision the metric names (float64 solve, float32 relaxation operators).  Multi-GPU runs are independent replicas
 (weak scaling): the ordered solve does not shard.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -120,7 +121,7 @@ def field_error(result, reference, queries):
 def run_ours(args, rank, world):
     import torch
     import torch.distributed as dist
-    from warp_psr_b200 import reconstruct, _lib
+    from warp_psr_b200 import reconstruct, reconstruct_differentiable, _lib
 
     device = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(device)
@@ -133,11 +134,39 @@ def run_ours(args, rank, world):
     stream = torch.cuda.current_stream(device)
 
     finest = []  # (seconds, row visits) of the finest level's relaxation launch, per timed step
+    split = []   # (forward ms, backward ms) per timed step
+    # The loss of the adjoint: sum of seeded, isovalue-centred field values at 32 queries.
+    rng = np.random.default_rng(2027)
+    lo, hi = p_host.min(0), p_host.max(0)
+    q_host = lo + (hi - lo) * rng.uniform(size=(32, 3))
+    seed_host = rng.normal(size=32)
 
-    def step(**kw):
-        r = reconstruct(p_dev, n_dev, precision=args.precision, **CONFIG, **kw)
+    def step(p_in=None, n_in=None):
+        """One solve+adjoint: differentiable reconstruction, loss, reverse pass onto the inputs."""
+        P = (p_dev if p_in is None else p_in).detach().requires_grad_(True)
+        N = (n_dev if n_in is None else n_in).detach().requires_grad_(True)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        res = reconstruct_differentiable(P, N, precision=args.precision, **CONFIG)
+        dtype = res.result.field.coefficients.dtype
+        q = torch.as_tensor(q_host, dtype=dtype, device=device)
+        seed = torch.as_tensor(seed_host, dtype=dtype, device=device)
+        v, _, _ = res.evaluate(q, centered=True)
+        loss = (torch.nan_to_num(v) * seed).sum()
+        e[1].record(stream)
+        loss.backward()
+        e[2].record(stream)
+        e[2].synchronize()
+        split.append((e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])))
+        r = res.result
         finest.append((r.diagnostics["relax_finest_seconds"], r.diagnostics["relax_finest_row_visits"]))
-        return r
+        # Keep only a summary: the tape (several GB at depth 9) is released with the result
+        # before the next step, as a training loop would.
+        summary = {"dtype": dtype, "coefficients": int(r.field.keys.numel()),
+                   "basis_counts": r.metadata["basis_counts"], "timings": r.metadata["timings_seconds"],
+                   "relax_seconds": r.diagnostics["relax_seconds"], "relax_launches": r.diagnostics["relax_launches"],
+                   "relax_row_visits": r.diagnostics["relax_row_visits"]}
+        return summary, P.grad, N.grad
 
     for _ in range(args.warmup):
         step()
@@ -162,9 +191,12 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     launches0 = _lib.kernel_launches()
     finest.clear()
+    split.clear()
     with Clocks(device.index) as clocks:
-        ms, result = timed(step, args.steps)
+        ms, (result, _, _) = timed(step, args.steps)
     launches = _lib.kernel_launches() - launches0
+    fwd_ms = statistics.mean(x[0] for x in split)
+    bwd_ms = statistics.mean(x[1] for x in split)
     torch.cuda.synchronize()
     if world > 1:
         t = torch.tensor([ms], device=device)
@@ -172,21 +204,28 @@ def run_ours(args, rank, world):
         ms = t.item()
         dist.barrier()
 
-    # End to end through the public API with host buffers: pinned H2D copy of the cloud,
-    # reconstruction, and the device-to-host read of the isovalue and transforms.
+    # End to end through the public API with host buffers: pinned H2D copy of the cloud, the
+    # solve+adjoint step, and the device-to-host read of the position and normal gradients.
+    g_host = [torch.empty(p_pin.shape, dtype=p_pin.dtype).pin_memory() for _ in range(2)]
+
     def e2e_step():
         p = p_pin.to(device, non_blocking=True)
         n = n_pin.to(device, non_blocking=True)
-        return reconstruct(p, n, precision=args.precision, **CONFIG)
+        r, gp, gn = step(p, n)
+        g_host[0].copy_(gp, non_blocking=True)
+        g_host[1].copy_(gn, non_blocking=True)
+        return None
 
     e2e_ms, _ = timed(e2e_step, args.steps)
     if world > 1:
         t = torch.tensor([e2e_ms], device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = t.item()
+    # the forward alone, not differentiable (what reconstruct() costs)
+    plain_ms, _ = timed(lambda: reconstruct(p_dev, n_dev, precision=args.precision, **CONFIG), max(1, args.steps // 2))
 
-    out_dtype = "f64" if result.field.coefficients.dtype == torch.float64 else "f32"
-    info = result.diagnostics
+    out_dtype = "f64" if result["dtype"] == torch.float64 else "f32"
+    info = result
     # Roofline of the dominant kernel: the finest level's ordered-relaxation launch
     # (strip_gs_kernel).  Algorithmic bytes per row visit: 27 operator entries (float32 in the
     # mixed path, else the input precision), b read, x read, x write in the vector precision,
@@ -214,9 +253,10 @@ def run_ours(args, rank, world):
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": out_dtype, "data": "synthetic",
         "config": {"workload": "bumpy sphere 800k points (SH l<=8, 10x density variation), depth 9, full depth 4, "
-                               "SPSR point weight 2, 8 GS iterations; forward reconstruction (adjoint not included)",
-                   "points": POINTS, "coefficients": int(result.field.keys.numel()),
-                   "basis_counts": result.metadata["basis_counts"], "precision": args.precision,
+                               "SPSR point weight 2, 8 GS iterations; step = differentiable reconstruction + "
+                               "32-query centred-value loss + reverse pass onto positions and normals",
+                   "points": POINTS, "coefficients": result["coefficients"],
+                   "basis_counts": result["basis_counts"], "precision": args.precision,
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "kernel": "strip_gs_kernel, finest level (ordered relaxation, depth 9)",
                      "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
@@ -228,9 +268,11 @@ def run_ours(args, rank, world):
                                     "ms": round(all_s * 1e3, 3),
                                     "achieved": round(all_visits * per_visit / all_s / 1e9, 1) if all_s > 0 else None}},
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(p_pin.numel() * 4 * 2),
-                "d2h_bytes_per_step": (1 + 32) * (8 if out_dtype == "f64" else 4)},
+                "d2h_bytes_per_step": int(p_pin.numel() * 4 * 2)},
+        "split_ms": {"forward_differentiable": round(fwd_ms, 3), "backward": round(bwd_ms, 3),
+                     "adjoint_over_forward": round(bwd_ms / fwd_ms, 3), "forward_plain": round(plain_ms, 3)},
         "gpu_launches": int(launches),
-        "stage_ms": {k: round(v * 1e3, 3) for k, v in result.metadata["timings_seconds"].items()},
+        "stage_ms": {k: round(v * 1e3, 3) for k, v in result["timings"].items()},
         "clocks": clocks.summary(),
     }
     if rank == 0 and not args.no_accuracy:
@@ -239,7 +281,8 @@ def run_ours(args, rank, world):
         lo, hi = p_host.min(0), p_host.max(0)
         q = np.concatenate([p_host[rng.choice(len(p_host), 20000, replace=False)],
                             lo + (hi - lo) * rng.uniform(size=(20000, 3))])
-        line["error_vs_fp64"] = field_error(result, fp64, q)
+        mixed = reconstruct(p_dev, n_dev, precision=args.precision, **CONFIG)
+        line["error_vs_fp64"] = field_error(mixed, fp64, q)
         if args.precision != "input":
             f32 = reconstruct(p_dev, n_dev, **CONFIG)
             line["fp32_error_vs_fp64"] = field_error(f32, fp64, q)
@@ -260,7 +303,8 @@ def cpu_baseline(p, n, steps):
         times.append((time.perf_counter() - t) * 1e3)
     return {"value": round(statistics.mean(times), 1), "unit": "ms", "cores": oracle.threads(), "kind": "port",
             "sample": f"{len(times)} full forward reconstruction(s) of the benchmark workload by the C++ oracle "
-                      f"(OpenMP, {oracle.threads()} threads)"}
+                      f"(OpenMP, {oracle.threads()} threads); the CPU restatement has no reverse pass, so this "
+                      f"times the forward part of the step only"}
 
 
 def run_reference(args):
@@ -286,7 +330,8 @@ def run_reference(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": {"workload": "bumpy sphere 800k points, depth 9, full depth 4, SPSR point weight 2; forward "
                                    "reconstruction by the C++ CPU restatement of warp-psr (PoissonRecon 262b0f5 "
-                                   "and Warp are not installable offline)", "points": POINTS},
+                                   "and Warp are not installable offline; the restatement has no reverse pass)",
+                       "points": POINTS},
             "cpu_baseline": {"value": round(ms, 1), "unit": "ms", "cores": oracle.threads(), "kind": "port",
                              "sample": f"{len(times)} full reconstruction(s), warm-up on {small}-point prefixes"},
             "e2e": {"value": round(ms, 1), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
