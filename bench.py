@@ -135,6 +135,7 @@ def run_ours(args, rank, world):
 
     finest = []  # (seconds, row visits) of the finest level's relaxation launch, per timed step
     split = []   # (forward ms, backward ms) per timed step
+    bw_stages = []  # device ms per reverse-pass stage, per timed step
     # The loss of the adjoint: sum of seeded, isovalue-centred field values at 32 queries.
     rng = np.random.default_rng(2027)
     lo, hi = p_host.min(0), p_host.max(0)
@@ -158,6 +159,7 @@ def run_ours(args, rank, world):
         e[2].record(stream)
         e[2].synchronize()
         split.append((e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])))
+        bw_stages.append(res.backward_stats.get("backward_ms", {}))
         r = res.result
         finest.append((r.diagnostics["relax_finest_seconds"], r.diagnostics["relax_finest_row_visits"]))
         # Keep only a summary: the tape (several GB at depth 9) is released with the result
@@ -192,9 +194,11 @@ def run_ours(args, rank, world):
     launches0 = _lib.kernel_launches()
     finest.clear()
     split.clear()
+    bw_stages.clear()
     with Clocks(device.index) as clocks:
         ms, (result, _, _) = timed(step, args.steps)
     launches = _lib.kernel_launches() - launches0
+    bw_stage_ms = {k: round(statistics.mean(b[k] for b in bw_stages), 3) for k in bw_stages[0]} if bw_stages else {}
     fwd_ms = statistics.mean(x[0] for x in split)
     bwd_ms = statistics.mean(x[1] for x in split)
     torch.cuda.synchronize()
@@ -270,7 +274,8 @@ def run_ours(args, rank, world):
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(p_pin.numel() * 4 * 2),
                 "d2h_bytes_per_step": int(p_pin.numel() * 4 * 2)},
         "split_ms": {"forward_differentiable": round(fwd_ms, 3), "backward": round(bwd_ms, 3),
-                     "adjoint_over_forward": round(bwd_ms / fwd_ms, 3), "forward_plain": round(plain_ms, 3)},
+                     "adjoint_over_forward": round(bwd_ms / fwd_ms, 3), "forward_plain": round(plain_ms, 3),
+                     "backward_stages": bw_stage_ms},
         "gpu_launches": int(launches),
         "stage_ms": {k: round(v * 1e3, 3) for k, v in result["timings"].items()},
         "clocks": clocks.summary(),
@@ -340,7 +345,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--precision", choices=("mixed", "input"), default="mixed")

@@ -77,6 +77,8 @@ typedef struct psr_info {
   double relax_finest_ms;            /* the finest level's launch alone (the dominant one) */
   int64_t relax_finest_row_visits;
   double normalization[5];  /* sample transform [1/width, t0, t1, t2, normal scale] (samples.py:54-88) */
+  double backward_ms[8];    /* last psr_backward, device ms: field, mirrored operators, reverse sweeps, operator
+                               adjoints, base multigrid, point constraints, normal loads, splats+density+samples */
 } psr_info;
 
 /* Device arrays owned by the result (valid until psr_free). */

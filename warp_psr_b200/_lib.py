@@ -33,7 +33,7 @@ class Info(ctypes.Structure):
         ("model_to_cube", ctypes.c_double * 16), ("stage_ms", ctypes.c_double * 8),
         ("relax_ms", ctypes.c_double), ("relax_row_visits", ctypes.c_int64), ("relax_launches", ctypes.c_int64),
         ("relax_finest_ms", ctypes.c_double), ("relax_finest_row_visits", ctypes.c_int64),
-        ("normalization", ctypes.c_double * 5),
+        ("normalization", ctypes.c_double * 5), ("backward_ms", ctypes.c_double * 8),
     ]
 
 

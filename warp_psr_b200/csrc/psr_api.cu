@@ -89,6 +89,7 @@ struct psr_result {
   double stage_ms[8] = {0};
   SolveStats stats;
   StageSink sink;
+  double backward_ms[8] = {0};  // last reverse pass, per stage (psr_info.backward_ms)
 };
 
 namespace psr {
@@ -262,9 +263,12 @@ void backward(psr_result* R, const T* pos, const T* nrm, int64_t n, const T* g_c
     g_cum.zero();
   g_sums.zero();
   HashView hv = R->hash.view();
+  EventMarks marks;
+  marks.begin(s);
   field_backward<T>(R->keys.p, R->level_offsets, hv, reinterpret_cast<const T*>(R->coefficients.p),
                     reinterpret_cast<const T*>(R->cumulative.p), prm.depth, tp.G.sums.p, tp.G.weights.p, tp.G.count,
                     g_iso, g_coef.p, g_cum.p, g_sums.p, s);
+  marks.mark(kBwField, s);
   std::vector<DBuf<T>> g_agg(prm.depth + 1);
   for (int d = 0; d <= prm.depth; ++d) {
     g_agg[d].alloc(4 * tp.D.agg_count[d], s);
@@ -274,9 +278,12 @@ void backward(psr_result* R, const T* pos, const T* nrm, int64_t n, const T* g_c
   g_avg.zero();
   g_nvals.zero();
   solve_backward<T>(tp.solve.get(), tp.tree, tp.D, tp.N, R->level_offsets, R->keys.p, R->hash, prm, g_coef.p, g_agg,
-                    g_avg.p, g_nvals.p, s);
+                    g_avg.p, g_nvals.p, s, &marks);
   samples_backward<T>(tp.G, tp.D, tp.N, prm.depth, prm.kernel_depth, prm.base_depth, prm.samples_per_node, prm.scale,
                       g_agg, g_avg.p, g_nvals.p, g_sums.p, g_norm, pos, nrm, n, g_pos, g_nrm, s);
+  marks.mark(kBwSamples, s);
+  PSR_CUDA(cudaStreamSynchronize(s));
+  marks.collect(R->backward_ms, kBwSlots);
 }
 
 
@@ -389,6 +396,7 @@ int psr_result_info(const psr_result* R, psr_info* info) {
   info->relax_finest_ms = R->stats.level_relax_ms.empty() ? 0.0 : R->stats.level_relax_ms.back();
   info->relax_finest_row_visits = R->stats.finest_row_visits;
   for (int i = 0; i < 5; ++i) info->normalization[i] = R->normalization[i];
+  for (int i = 0; i < 8; ++i) info->backward_ms[i] = R->backward_ms[i];
   return PSR_OK;
 }
 

@@ -6,6 +6,8 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <utility>
+#include <vector>
 
 namespace psr {
 
@@ -36,6 +38,37 @@ struct StageSink {
     entries[name] = std::move(e);
   }
 };
+
+// Stream-ordered stage timer: mark(k) closes the interval since the previous mark and adds
+// its device time to slot k (read after the stream has synchronised).
+struct EventMarks {
+  std::vector<std::pair<int, cudaEvent_t>> marks;
+  cudaEvent_t start = nullptr;
+  void begin(cudaStream_t s) {
+    PSR_CUDA(cudaEventCreate(&start));
+    PSR_CUDA(cudaEventRecord(start, s));
+  }
+  void mark(int slot, cudaStream_t s) {
+    cudaEvent_t e;
+    PSR_CUDA(cudaEventCreate(&e));
+    PSR_CUDA(cudaEventRecord(e, s));
+    marks.emplace_back(slot, e);
+  }
+  void collect(double* out, int slots) {  // after synchronisation
+    for (int i = 0; i < slots; ++i) out[i] = 0;
+    cudaEvent_t prev = start;
+    for (auto& m : marks) {
+      float ms = 0;
+      if (prev && cudaEventElapsedTime(&ms, prev, m.second) == cudaSuccess && m.first < slots) out[m.first] += ms;
+      prev = m.second;
+    }
+    for (auto& m : marks) cudaEventDestroy(m.second);
+    if (start) cudaEventDestroy(start);
+    marks.clear();
+    start = nullptr;
+  }
+};
+enum { kBwField, kBwMirror, kBwSweep, kBwOperator, kBwBase, kBwPoints, kBwNormalLoads, kBwSamples, kBwSlots };
 
 // Sets the message psr_last_error returns on this thread.
 void set_last_error(const std::string& message);
@@ -130,7 +163,7 @@ template <class T>
 void solve_backward(void* tape, const TreeData& tree, const DensityData<T>& D, const NormalData<T>& N,
                     const std::vector<int64_t>& level_offsets, const int64_t* all_keys, const HashMap& all_hash,
                     const Params& p, const T* g_coef, std::vector<DBuf<T>>& g_agg, T* g_average, T* g_nvals,
-                    cudaStream_t s);
+                    cudaStream_t s, EventMarks* marks = nullptr);
 
 // Ordered sliced relaxation on an ELL level (28 slots per row; slot k < 27 is the k-th
 // lexicographic neighbour, -1 absent).  Rows are referenced through `rows` grouped by
@@ -154,8 +187,8 @@ void build_strip_schedule(const int64_t* keys, int64_t rows, int depth, StripSch
 // group-relative neighbour indices I[32] per row, b with 16 bytes of slack; x in key order
 // holds the initial guess and receives the result.
 //
-// `hist` (optional, iters x rows in schedule order) receives per visit the new x of every row,
-// or with `record_increment` the update r / A_ii.  `rev` runs the colours of a slice in the
+// `hist` (optional, rows x iters in schedule order: row p, visit t at p * iters + t) receives
+// per visit the new x of every row, or with `record_increment` the update r / A_ii.  `rev` runs the colours of a slice in the
 // order 3, 2, 1, 0: on the z-mirrored schedule this is the exact reverse of the forward
 // sequential order (used by the adjoint).
 template <class T, class V, class I>

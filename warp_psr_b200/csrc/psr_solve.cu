@@ -448,10 +448,11 @@ __global__ void assemble_sliced_kernel(const int64_t* keys, int64_t n, int d, Co
 
 // Cross operator (rows at d, trial functions at d-1; stiffness + screening, rounded to T)
 // applied to the coarser cumulative solution: b = b - C cumulative (solver.py:428-446).
+// With ccols_out / cvals_out (adjoint tape) the row's cross operator is kept (28 slots).
 template <class T, bool SCREEN>
 __global__ void cross_apply_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t coff,
                                    const double* table, PointsView<T> P, const T* cumulative, T* b,
-                                   const int32_t* inv) {
+                                   const int32_t* inv, int32_t* ccols_out = nullptr, T* cvals_out = nullptr) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   int c[3];
@@ -474,7 +475,10 @@ __global__ void cross_apply_kernel(const int64_t* keys, int64_t n, int d, Column
     double stiff = x[1] * y[0] * z[0] + x[0] * y[1] * z[0] + x[0] * y[0] * z[1];
     T v = T(SCREEN ? stiff + acc[k] : stiff);
     s = s + v * cumulative[col[k]];
+    if (cvals_out) cvals_out[i * kSlots + k] = v;
   }
+  if (ccols_out)
+    for (int k = 0; k < kSlots; ++k) ccols_out[i * kSlots + k] = k < 27 ? col[k] : -1;
   const int64_t p = inv ? inv[i] : i;
   b[p] = -s + b[p];
 }
@@ -652,6 +656,86 @@ __global__ void __launch_bounds__(512) relax_colors_kernel(const int32_t* cols, 
         gs_row(cols, vals, b, x, rows[j], hist ? hist + 2 * (int64_t(it) * n + rows[j]) : nullptr);
       __syncthreads();
     }
+}
+
+// The same relaxation with x held in shared memory for the whole call (levels whose x fits):
+// identical arithmetic and order, without a round trip to L2 per neighbour read.
+template <class T>
+__device__ __forceinline__ void gs_row_shared(const int32_t* __restrict__ cols, const T* __restrict__ vals,
+                                              const T* __restrict__ b, T* xs_sh, int32_t row, T* rec) {
+  const int4* cr = reinterpret_cast<const int4*>(cols + int64_t(row) * kSlots);
+  int cc[kSlots];
+#pragma unroll
+  for (int q = 0; q < kSlots / 4; ++q) {
+    int4 v = __ldg(cr + q);
+    cc[4 * q] = v.x;
+    cc[4 * q + 1] = v.y;
+    cc[4 * q + 2] = v.z;
+    cc[4 * q + 3] = v.w;
+  }
+  T aa[kSlots];
+  const T* vr = vals + int64_t(row) * kSlots;
+#pragma unroll
+  for (int q = 0; q < kSlots; ++q) aa[q] = __ldg(vr + q);
+  T xs[27];
+#pragma unroll
+  for (int k = 0; k < 27; ++k) xs[k] = cc[k] >= 0 ? xs_sh[cc[k]] : T(0);
+  T r = b[row];
+  T diagonal = T(0);
+  T xi = T(0);
+#pragma unroll
+  for (int k = 0; k < 27; ++k) {
+    if (cc[k] < 0) continue;
+    r = r - xs[k] * T(aa[k]);
+    if (cc[k] == row) {
+      diagonal = aa[k];
+      xi = xs[k];
+    }
+  }
+  if (rec) {
+    rec[0] = xi;
+    rec[1] = r;
+  }
+  if (diagonal != T(0)) xs_sh[row] = xi + r * (T(1.0) / T(diagonal));
+}
+
+template <class T>
+__global__ void __launch_bounds__(512) relax_colors_shared_kernel(const int32_t* cols, const T* vals, const T* b, T* x,
+                                                                   const int32_t* rows, const int32_t* group_off,
+                                                                   int iters, int forward, T* hist, int64_t n) {
+  extern __shared__ __align__(16) unsigned char relax_smem[];
+  T* xs = reinterpret_cast<T*>(relax_smem);
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) xs[i] = x[i];
+  __syncthreads();
+  for (int it = 0; it < iters; ++it)
+    for (int cc = 0; cc < 8; ++cc) {
+      int g = forward ? cc : 7 - cc;
+      for (int j = group_off[g] + threadIdx.x; j < group_off[g + 1]; j += blockDim.x)
+        gs_row_shared(cols, vals, b, xs, rows[j], hist ? hist + 2 * (int64_t(it) * n + rows[j]) : nullptr);
+      __syncthreads();
+    }
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) x[i] = xs[i];
+}
+
+constexpr size_t kRelaxSharedBytes = 200 * 1024;
+
+// One colour-relaxation call on a small level: shared-memory x when it fits.
+template <class T>
+static void relax_colors(const int32_t* cols, const T* vals, const T* b, T* x, const int32_t* rows,
+                         const int32_t* group_off, int iters, int forward, T* hist, int64_t n, cudaStream_t s) {
+  const size_t bytes = size_t(n) * sizeof(T);
+  if (n > 0 && bytes <= kRelaxSharedBytes) {
+    static bool configured = false;
+    if (!configured) {
+      PSR_CUDA(cudaFuncSetAttribute(relax_colors_shared_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(kRelaxSharedBytes)));
+      configured = true;
+    }
+    relax_colors_shared_kernel<T><<<1, 512, bytes, s>>>(cols, vals, b, x, rows, group_off, iters, forward, hist, n);
+  } else {
+    relax_colors_kernel<T><<<1, 512, 0, s>>>(cols, vals, b, x, rows, group_off, iters, forward, hist, n);
+  }
+  PSR_LAUNCH_CHECK();
 }
 
 // r = rhs - A x  (bsr_mv alpha=-1, beta=1)
@@ -942,7 +1026,9 @@ struct SlicedTape {
   StripSchedule sched;
   DBuf<char> svals, sidx;  // schedule-order operator rows (float32 values in the mixed precision)
   DBuf<T> b;               // schedule-order right-hand side after the cross term
-  DBuf<T> hist;            // iters x n (schedule order): x after each visit
+  DBuf<T> hist;            // n x iters (schedule order): x after each visit
+  DBuf<int32_t> ccols;     // cross operator (rows at d, columns at d-1), key order, 28 slots
+  DBuf<T> cvals;
 };
 
 template <class T>
@@ -1238,9 +1324,7 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
         for (int l = base; l > 0; --l) {
           int64_t nl = count_at(l);
           T* rh = relax_hist(l);
-          relax_colors_kernel<T><<<1, 512, 0, s>>>(Cl(l), Vl(l), Rl(l), Xl(l), sched[l].rows.p, sched[l].off.p,
-                                                    p.iters, 1, rh, nl);
-          PSR_LAUNCH_CHECK();
+          relax_colors<T>(Cl(l), Vl(l), Rl(l), Xl(l), sched[l].rows.p, sched[l].off.p, p.iters, 1, rh, nl, s);
           if (tp) {
             tp->resid_x.emplace_back(nl, s);
             PSR_CUDA(cudaMemcpyAsync(tp->resid_x.back().p, Xl(l), nl * sizeof(T), cudaMemcpyDeviceToDevice, s));
@@ -1274,9 +1358,7 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
           PSR_LAUNCH_CHECK();
           PSR_CUDA(cudaMemsetAsync(xs[l - 1].p, 0, count_at(l - 1) * sizeof(T), s));
           T* rh = relax_hist(l);
-          relax_colors_kernel<T><<<1, 512, 0, s>>>(Cl(l), Vl(l), Rl(l), Xl(l), sched[l].rows.p, sched[l].off.p,
-                                                    p.iters, 0, rh, nl);
-          PSR_LAUNCH_CHECK();
+          relax_colors<T>(Cl(l), Vl(l), Rl(l), Xl(l), sched[l].rows.p, sched[l].off.p, p.iters, 0, rh, nl, s);
         }
       }
       if (tp) {
@@ -1297,13 +1379,25 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
       DBuf<double> ctable(int64_t(res + 1) * 6, s);
       stiffness_table_kernel<<<blocks_for(res + 1), kThreads, 0, s>>>(d, d - 1, ctable.p);
       PSR_LAUNCH_CHECK();
+      DBuf<int32_t> ccols;
+      DBuf<T> cvals;
+      if (tp) {
+        ccols.alloc(kSlots * n, s);
+        cvals.alloc(kSlots * n, s);
+        cvals.zero();
+      }
       if (screened)
         cross_apply_kernel<T, true><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d - 1],
-                                                                        ctable.p, pv, cumulative.p, b.p, sched.inv.p);
+                                                                        ctable.p, pv, cumulative.p, b.p, sched.inv.p,
+                                                                        ccols.p, cvals.p);
       else
         cross_apply_kernel<T, false><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d - 1],
                                                                          ctable.p, pv, cumulative.p, b.p,
-                                                                         sched.inv.p);
+                                                                         sched.inv.p, ccols.p, cvals.p);
+      if (tp) {
+        tp->sliced[d].ccols = std::move(ccols);
+        tp->sliced[d].cvals = std::move(cvals);
+      }
       PSR_LAUNCH_CHECK();
       if (sink && sink->on) {  // kept in key order, like every other stage
         DBuf<T> kb(n, s);

@@ -56,23 +56,33 @@ __device__ __forceinline__ T hat3_grad(const T p[3], const int c[3], int depth, 
 __device__ __forceinline__ int sched_group(const int c[3]) { return 4 * c[2] + (c[0] & 1) + 2 * (c[1] & 1); }
 
 // ------------------------------------------------------------------ mirrored, transposed operator
-__global__ void mirror_keys_kernel(const int64_t* keys, int64_t n, int depth, int64_t* out, int32_t* ids) {
-  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i >= n) return;
+// Mirrored schedule straight from the forward one: group (z, c) becomes group (2^d - z, c)
+// and keeps its rows and their order, so no sort is needed.
+__global__ void mirror_offsets_kernel(const int32_t* off, int groups, int nz, int32_t* off2) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int32_t acc = 0;
+  for (int g2 = 0; g2 < groups; ++g2) {
+    off2[g2] = acc;
+    const int g = 4 * (nz - g2 / 4) + g2 % 4;
+    acc += off[g + 1] - off[g];
+  }
+  off2[groups] = acc;
+}
+
+__global__ void mirror_positions_kernel(const int32_t* perm, const int32_t* off, const int64_t* skeys,
+                                        const int32_t* off2, int64_t n, int depth, int32_t* perm2, int32_t* inv2,
+                                        int64_t* skeys2) {
+  int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (p >= n) return;
   int c[3];
-  key_coords(keys[i], c);
-  out[i] = basis_key(depth, c[0], c[1], (1 << depth) - c[2]);
-  ids[i] = int32_t(i);
-}
-
-__global__ void inverse_map_kernel(const int32_t* map, int64_t n, int32_t* inv) {
-  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i < n) inv[map[i]] = int32_t(i);
-}
-
-__global__ void compose_kernel(const int32_t* a, const int32_t* b, int64_t n, int32_t* out) {  // out = a[b[i]]
-  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i < n) out[i] = a[b[i]];
+  key_coords(skeys[p], c);
+  const int nz = 1 << depth;
+  const int g = 4 * c[2] + (c[0] & 1) + 2 * (c[1] & 1);
+  const int g2 = 4 * (nz - c[2]) + (c[0] & 1) + 2 * (c[1] & 1);
+  const int64_t p2 = off2[g2] + (p - off[g]);
+  perm2[p2] = perm[p];
+  inv2[perm[p]] = int32_t(p2);
+  skeys2[p2] = basis_key(depth, c[0], c[1], nz - c[2]);
 }
 
 // Row p2 of the mirrored schedule: slot k2 (mirrored dz) holds A_{nbr, row} of the forward
@@ -84,7 +94,7 @@ __global__ void mirror_operator_kernel(int64_t n, int depth, const int32_t* perm
                                        const int64_t* skeys2, const S* svals, const I* sidx, S* tvals, I* tidx) {
   int64_t p2 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (p2 >= n) return;
-  const int64_t i = orig_of[perm2[p2]];
+  const int64_t i = orig_of ? orig_of[perm2[p2]] : perm2[p2];
   const int64_t p = inv[i];
   int m[3];
   key_coords(skeys2[p2], m);
@@ -111,13 +121,7 @@ __global__ void mirror_operator_kernel(int64_t n, int depth, const int32_t* perm
 template <class T>
 __global__ void gather_seed_kernel(const int32_t* perm2, const int32_t* orig_of, int64_t n, const T* seed, T* b2) {
   int64_t p2 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (p2 < n) b2[p2] = seed[orig_of[perm2[p2]]];
-}
-
-template <class T>
-__global__ void scatter_mirrored_kernel(const int32_t* orig_of, int64_t n, const T* in, T* out) {
-  int64_t i2 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i2 < n) out[orig_of[i2]] = in[i2];
+  if (p2 < n) b2[p2] = seed[orig_of ? orig_of[perm2[p2]] : perm2[p2]];
 }
 
 // ------------------------------------------------------------------ fused level reverse kernel
@@ -138,13 +142,15 @@ struct LevelReverse {
   const int32_t* inv = nullptr;
   const int32_t* off = nullptr;
   const I* sidx = nullptr;
-  const T* xhist = nullptr;    // iters x n forward x after each visit (schedule order)
-  const T* mu = nullptr;       // iters x n increments of the reversed sweep (mirrored schedule order)
+  const T* xhist = nullptr;    // n x iters forward x after each visit (schedule order)
+  const T* mu = nullptr;       // n x iters increments of the reversed sweep (mirrored schedule order)
   const int32_t* inv2 = nullptr;  // key index -> mirrored schedule position
   // base level: explicit operator adjoint (28 slots, key order)
   const T* g_A = nullptr;
   // cross
   bool cross = false;
+  const int32_t* ccols = nullptr;  // forward's cross operator (28 slots, key order); else recomputed
+  const T* cvals = nullptr;
   const double* ctable = nullptr;
   const T* cum_prev = nullptr;
   T* g_cum_prev = nullptr;
@@ -178,10 +184,12 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
       // 0: the neighbour's value after this visit, 1: after the previous visit
       const int delay = k == 13 ? 0 : (q[2] > c[2] || (q[2] == c[2] && qc < own)) ? 0 : 1;
       T acc = T(0);
+      const T* mrow = L.mu + p2 * L.iters;
+      const T* xrow = L.xhist + pk * L.iters;
       for (int t = 0; t < L.iters; ++t) {
-        const T m = L.mu[int64_t(L.iters - 1 - t) * L.n + p2];
+        const T m = mrow[L.iters - 1 - t];
         const int tv = t - delay;
-        const T xv = tv >= 0 ? L.xhist[int64_t(tv) * L.n + pk] : T(0);
+        const T xv = tv >= 0 ? xrow[tv] : T(0);
         acc = acc - m * xv;
       }
       gA[k] = acc;
@@ -195,7 +203,19 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
   T gC[27];
   double cacc[27];
   int q0c[3] = {0, 0, 0};
-  if (L.cross) {
+  if (L.cross && L.ccols) {
+    int ctr[3] = {c[0] >> 1, c[1] >> 1, c[2] >> 1};
+    for (int a = 0; a < 3; ++a) q0c[a] = ctr[a] - 1;
+    for (int k = 0; k < 27; ++k) {
+      gC[k] = T(0);
+      const int32_t col = L.ccols[i * kSlots + k];
+      if (col < 0) continue;
+      cpresent |= 1u << k;
+      const T v = L.cvals[i * kSlots + k];
+      if (gb != T(0)) atomicAdd(L.g_cum_prev + col, -(v * gb));
+      gC[k] = -(gb * L.cum_prev[col]);
+    }
+  } else if (L.cross) {
     int ctr[3] = {c[0] >> 1, c[1] >> 1, c[2] >> 1};
     cpresent = neighbours27(L.cv, L.d - 1, ctr, L.coff, ccol);
     for (int k = 0; k < 27; ++k) cacc[k] = 0.0;
@@ -300,51 +320,97 @@ __global__ void prolong_apply_kernel(const int32_t* pcol, const T* pval, int64_t
 }
 
 // ------------------------------------------------------------------ base multigrid reverse
-// Reverse of one colour relaxation call (relaxation_adjoint.py:50-78) by one CTA: the visit
-// records (old x, r) rewind x; lambda (in/out), the rhs adjoint and the operator adjoint
-// accumulate.  x is rebuilt from the last visit's record first.
+// ---- colour relaxation reversed as a Gauss-Seidel sweep on A^T (no atomics)
+// Transposed operator in the same 28-slot layout: slot k of row i holds A_{col, i}, the
+// neighbour's entry at the opposite offset (slot 26 - k).
 template <class T>
-__global__ void __launch_bounds__(512) relax_colors_reverse_kernel(const int32_t* cols, const T* vals,
-                                                                    const int32_t* rows, const int32_t* group_off,
-                                                                    int iters, int forward, const T* hist, int64_t n,
-                                                                    T* x, T* lambda, T* g_b, T* g_A) {
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
-    const T* rec = hist + 2 * (int64_t(iters - 1) * n + i);
-    T diag = T(0);
-    for (int k = 0; k < 27; ++k)
-      if (cols[i * kSlots + k] == int32_t(i)) diag = vals[i * kSlots + k];
-    x[i] = diag != T(0) ? rec[0] + rec[1] * (T(1.0) / diag) : rec[0];
+__global__ void transpose_slots_kernel(const int32_t* cols, const T* vals, int64_t n, T* vals_t) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  for (int k = 0; k < kSlots; ++k) {
+    const int32_t c = k < 27 ? cols[i * kSlots + k] : -1;
+    vals_t[i * kSlots + k] = c >= 0 ? vals[int64_t(c) * kSlots + (26 - k)] : T(0);
   }
-  __syncthreads();
-  for (int it = iters - 1; it >= 0; --it)
-    for (int cc = 7; cc >= 0; --cc) {
-      const int g = forward ? cc : 7 - cc;
-      for (int j = group_off[g] + threadIdx.x; j < group_off[g + 1]; j += blockDim.x) {
-        const int32_t i = rows[j];
-        const T* rec = hist + 2 * (int64_t(it) * n + i);
-        x[i] = rec[0];
-        T diag = T(0);
-        int dk = -1;
-        for (int k = 0; k < 27; ++k)
-          if (cols[int64_t(i) * kSlots + k] == i) {
-            diag = vals[int64_t(i) * kSlots + k];
-            dk = k;
-          }
-        if (diag == T(0)) continue;
-        const T seed = lambda[i];
-        const T mu = seed * (T(1.0) / diag);
-        if (mu == T(0) && seed == T(0)) continue;
-        g_b[i] = g_b[i] + mu;
-        atomicAdd(g_A + int64_t(i) * kSlots + dk, -(seed * rec[1]) / (diag * diag));
-        for (int k = 0; k < 27; ++k) {
-          const int32_t col = cols[int64_t(i) * kSlots + k];
-          if (col < 0) continue;
-          atomicAdd(g_A + int64_t(i) * kSlots + k, -(mu * x[col]));
-          atomicAdd(lambda + col, -(mu * vals[int64_t(i) * kSlots + k]));
-        }
+}
+
+// lambda -= A^T M  (the adjoint leaving the call), and g_b += M.
+template <class T>
+__global__ void adjoint_out_kernel(const int32_t* cols, const T* vals_t, const T* M, int64_t n, T* lambda, T* g_b) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  T s = T(0);
+  for (int k = 0; k < 27; ++k) {
+    const int32_t c = cols[i * kSlots + k];
+    if (c < 0) continue;
+    s = s + vals_t[i * kSlots + k] * M[c];
+  }
+  lambda[i] = lambda[i] - s;
+  g_b[i] = g_b[i] + M[i];
+}
+
+__device__ __forceinline__ int colour8(const int c[3]) { return (c[0] & 1) + 2 * (c[1] & 1) + 4 * (c[2] & 1); }
+
+// Operator adjoint of one colour-relaxation call: g_A_ik -= sum_t mu_i(t) x_k(seen at visit t),
+// mu from the transposed sweep's records, x from the forward call's records.
+template <class T>
+__global__ void relax_operator_adjoint_kernel(const int64_t* keys, const int32_t* cols, const T* vals, int64_t n,
+                                              int iters, int forward, const T* hist_fwd, const T* hist_rev, T* g_A) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int ci[3];
+  key_coords(keys[i], ci);
+  const int pos_i = forward ? colour8(ci) : 7 - colour8(ci);
+  T diag_i = T(0);
+  for (int k = 0; k < 27; ++k)
+    if (cols[i * kSlots + k] == int32_t(i)) diag_i = vals[i * kSlots + k];
+  if (diag_i == T(0)) return;
+  const T inv_i = T(1.0) / diag_i;
+  for (int k = 0; k < 27; ++k) {
+    const int32_t c = cols[i * kSlots + k];
+    if (c < 0) continue;
+    int ck[3];
+    key_coords(keys[c], ck);
+    const int pos_k = forward ? colour8(ck) : 7 - colour8(ck);
+    T diag_k = T(0);
+    if (c == int32_t(i) || pos_k < pos_i)
+      for (int q = 0; q < 27; ++q)
+        if (cols[int64_t(c) * kSlots + q] == c) diag_k = vals[int64_t(c) * kSlots + q];
+    T acc = T(0);
+    for (int t = 0; t < iters; ++t) {
+      const T mu = hist_rev[2 * (int64_t(iters - 1 - t) * n + i) + 1] * inv_i;
+      T xv;
+      if (c == int32_t(i) || pos_k < pos_i) {  // seen after its own visit t
+        const T* rec = hist_fwd + 2 * (int64_t(t) * n + c);
+        xv = diag_k != T(0) ? rec[0] + rec[1] * (T(1.0) / diag_k) : rec[0];
+      } else {  // seen before its visit t
+        xv = hist_fwd[2 * (int64_t(t) * n + c)];
       }
-      __syncthreads();
+      acc = acc - mu * xv;
     }
+    g_A[i * kSlots + k] = g_A[i * kSlots + k] + acc;
+  }
+}
+
+template <class T>
+struct BaseTranspose {
+  std::vector<DBuf<T>> vals_t;
+};
+
+// Reverse of one relax_colors call (forward flag `forward`): lambda (in/out) is the adjoint
+// of x, g_b and g_A accumulate.
+template <class T>
+static void relax_colors_adjoint(const int64_t* keys, const int32_t* cols, const T* vals, const T* vals_t,
+                                 const int32_t* rows, const int32_t* group_off, int iters, int forward,
+                                 const T* hist_fwd, int64_t n, T* lambda, T* g_b, T* g_A, cudaStream_t s) {
+  if (n <= 0) return;
+  DBuf<T> M(n, s), hist_rev(2 * int64_t(iters) * n, s);
+  M.zero();
+  relax_colors<T>(cols, vals_t, lambda, M.p, rows, group_off, iters, forward ? 0 : 1, hist_rev.p, n, s);
+  relax_operator_adjoint_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(keys, cols, vals, n, iters, forward, hist_fwd,
+                                                                       hist_rev.p, g_A);
+  PSR_LAUNCH_CHECK();
+  adjoint_out_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(cols, vals_t, M.p, n, lambda, g_b);
+  PSR_LAUNCH_CHECK();
 }
 
 // r = rhs - A x reversed: g_rhs += g_r, g_x -= A^T g_r, g_A_ik -= g_r_i x_k.
@@ -732,8 +798,11 @@ template <class T>
 void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& D, const NormalData<T>& N,
                     const std::vector<int64_t>& level_offsets, const int64_t* all_keys, const HashMap& all_hash,
                     const Params& p, const T* g_coef, std::vector<DBuf<T>>& g_agg, T* g_average, T* g_nvals,
-                    cudaStream_t s) {
+                    cudaStream_t s, EventMarks* marks) {
   SolveTape<T>& tp = *static_cast<SolveTape<T>*>(tape_ptr);
+  auto mark = [&](int slot) {
+    if (marks) marks->mark(slot, s);
+  };
   const int finest = p.depth, base = p.base_depth;
   HashView bh = all_hash.view();
   auto keys_at = [&](int d) { return all_keys + level_offsets[d]; };
@@ -770,54 +839,54 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
     DBuf<T> seed(n, s);
     axpy_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(g_coef + level_offsets[d], g_cum[d].p, n, seed.p);
     PSR_LAUNCH_CHECK();
-    // mirrored schedule
-    DBuf<int64_t> mk(n, s), mks(n, s);
-    DBuf<int32_t> ids(n, s), orig_of(n, s), inv2(n, s);
-    mirror_keys_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys_at(d), n, d, mk.p, ids.p);
-    PSR_LAUNCH_CHECK();
-    sort_pairs(reinterpret_cast<const uint64_t*>(mk.p), reinterpret_cast<uint64_t*>(mks.p), ids.p, orig_of.p, n, 48,
-               s);
+    // mirrored schedule (its "key order" is the forward key order: perm2 maps to forward rows)
+    const int nz = 1 << d, groups = 4 * (nz + 1);
     StripSchedule S2;
-    build_strip_schedule(mks.p, n, d, S2, s);
-    // key index -> mirrored schedule position
-    {
-      DBuf<int32_t> i2_of(n, s);
-      inverse_map_kernel<<<blocks_for(n), kThreads, 0, s>>>(orig_of.p, n, i2_of.p);
-      PSR_LAUNCH_CHECK();
-      compose_kernel<<<blocks_for(n), kThreads, 0, s>>>(S2.inv.p, i2_of.p, n, inv2.p);
-      PSR_LAUNCH_CHECK();
-    }
+    S2.rows = n;
+    S2.depth = d;
+    S2.wide = st.sched.wide;
+    S2.perm.alloc(n, s);
+    S2.inv.alloc(n, s);
+    S2.off.alloc(groups + 1, s);
+    S2.skeys.alloc(n, s);
+    mirror_offsets_kernel<<<1, 32, 0, s>>>(st.sched.off.p, groups, nz, S2.off.p);
+    PSR_LAUNCH_CHECK();
+    mirror_positions_kernel<<<blocks_for(n), kThreads, 0, s>>>(st.sched.perm.p, st.sched.off.p, st.sched.skeys.p,
+                                                               S2.off.p, n, d, S2.perm.p, S2.inv.p, S2.skeys.p);
+    PSR_LAUNCH_CHECK();
+    const int32_t* inv2 = S2.inv.p;
     DBuf<T> b2(n + 4, s), M(n, s), mu(int64_t(p.iters) * n, s);
     b2.zero();
     M.zero();
-    gather_seed_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(S2.perm.p, orig_of.p, n, seed.p, b2.p);
+    gather_seed_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(S2.perm.p, nullptr, n, seed.p, b2.p);
     PSR_LAUNCH_CHECK();
+    mark(kBwMirror);
     auto reverse_sweep = [&](auto s_tag, auto i_tag) {
       using S = decltype(s_tag);
       using I = decltype(i_tag);
       DBuf<S> tv(kSlots * n, s);
       DBuf<I> ti(kIdxSlots * n, s);
       mirror_operator_kernel<S, I><<<blocks_for(n), kThreads, 0, s>>>(
-          n, d, S2.perm.p, orig_of.p, st.sched.inv.p, st.sched.off.p, S2.off.p, S2.skeys.p,
+          n, d, S2.perm.p, nullptr, st.sched.inv.p, st.sched.off.p, S2.off.p, S2.skeys.p,
           reinterpret_cast<const S*>(st.svals.p), reinterpret_cast<const I*>(st.sidx.p), tv.p, ti.p);
       PSR_LAUNCH_CHECK();
+      mark(kBwMirror);
       relax_strips_scheduled<S, T, I>(S2, tv.p, ti.p, b2.p, M.p, p.iters, s, nullptr, mu.p, true, true);
+      mark(kBwSweep);
     };
     if (tp.mixed) {
-      if (st.sched.wide || S2.wide)
+      if (st.sched.wide)
         reverse_sweep(float(), int32_t());
       else
         reverse_sweep(float(), int16_t());
     } else {
-      if (st.sched.wide || S2.wide)
+      if (st.sched.wide)
         reverse_sweep(T(), int32_t());
       else
         reverse_sweep(T(), int16_t());
     }
-    // M (mirrored key order) -> rhs adjoint (key order)
-    DBuf<T> g_b(n, s);
-    scatter_mirrored_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(orig_of.p, n, M.p, g_b.p);
-    PSR_LAUNCH_CHECK();
+    // M (forward key order): the rhs adjoint
+    DBuf<T>& g_b = M;
     // operator, cross and screening adjoints
     const int res = 1 << d;
     DBuf<double> ctable(int64_t(res + 1) * 6, s);
@@ -839,8 +908,10 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
       L.sidx = reinterpret_cast<const I*>(st.sidx.p);
       L.xhist = st.hist.p;
       L.mu = mu.p;
-      L.inv2 = inv2.p;
+      L.inv2 = inv2;
       L.cross = true;
+      L.ccols = st.ccols.p;
+      L.cvals = st.cvals.p;
       L.ctable = ctable.p;
       L.cum_prev = tp.cum[d - 1].p;
       L.g_cum_prev = g_cum[d - 1].p;
@@ -863,13 +934,14 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
     PSR_LAUNCH_CHECK();
     to_double_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(g_b.p, n, g_load[d].p);
     PSR_LAUNCH_CHECK();
+    mark(kBwOperator);
   }
 
   // ---- base multigrid
   {
     const int64_t nb = count_at(base);
     point_grads(base);
-    std::vector<DBuf<T>> gx(base + 1), grhs(base + 1), gA(base + 1), work(base + 1);
+    std::vector<DBuf<T>> gx(base + 1), grhs(base + 1), gA(base + 1);
     for (int l = 0; l <= base; ++l) {
       const int64_t nl = count_at(l);
       gx[l].alloc(nl, s);
@@ -878,10 +950,18 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
       grhs[l].zero();
       gA[l].alloc(kSlots * nl, s);
       gA[l].zero();
-      work[l].alloc(nl, s);
     }
     axpy_kernel<T><<<blocks_for(nb), kThreads, 0, s>>>(g_coef + level_offsets[base], g_cum[base].p, nb, gx[base].p);
     PSR_LAUNCH_CHECK();
+    std::vector<DBuf<T>> vt(base + 1);  // transposed level operators
+    for (int l = 1; l <= base; ++l) {
+      const int64_t nl = count_at(l);
+      vt[l].alloc(kSlots * nl, s);
+      if (nl) {
+        transpose_slots_kernel<T><<<blocks_for(nl), kThreads, 0, s>>>(tp.mcols[l].p, tp.mvals[l].p, nl, vt[l].p);
+        PSR_LAUNCH_CHECK();
+      }
+    }
     auto Rl = [&](int l) { return l == base ? tp.base_b.p : nullptr; };
     (void)Rl;
     const int cycles = p.base_v_cycles;
@@ -895,10 +975,9 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
     for (int cycle = cycles - 1; cycle >= 0; --cycle) {
       for (int l = base; l >= 1; --l) {  // reverse of the upward pass
         const int64_t nl = count_at(l);
-        relax_colors_reverse_kernel<T><<<1, 512, 0, s>>>(tp.mcols[l].p, tp.mvals[l].p, tp.msched[l].rows.p,
-                                                          tp.msched[l].off.p, p.iters, 0, tp.relax_hist[h--].p, nl,
-                                                          work[l].p, gx[l].p, grhs[l].p, gA[l].p);
-        PSR_LAUNCH_CHECK();
+        relax_colors_adjoint<T>(keys_at(l), tp.mcols[l].p, tp.mvals[l].p, vt[l].p, tp.msched[l].rows.p,
+                                tp.msched[l].off.p, p.iters, 0, tp.relax_hist[h--].p, nl, gx[l].p, grhs[l].p,
+                                gA[l].p, s);
         // x_l += P x_{l-1}, then x_{l-1} = 0
         gx[l - 1].zero();
         prolong_transpose_kernel<T><<<blocks_for(nl), kThreads, 0, s>>>(tp.pcol[l].p, tp.pval[l].p, nl, gx[l].p,
@@ -936,10 +1015,9 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
                                                                        tp.resid_x[rx--].p, g_r.p, nl, grhs[l].p,
                                                                        gx[l].p, gA[l].p);
         PSR_LAUNCH_CHECK();
-        relax_colors_reverse_kernel<T><<<1, 512, 0, s>>>(tp.mcols[l].p, tp.mvals[l].p, tp.msched[l].rows.p,
-                                                          tp.msched[l].off.p, p.iters, 1, tp.relax_hist[h--].p, nl,
-                                                          work[l].p, gx[l].p, grhs[l].p, gA[l].p);
-        PSR_LAUNCH_CHECK();
+        relax_colors_adjoint<T>(keys_at(l), tp.mcols[l].p, tp.mvals[l].p, vt[l].p, tp.msched[l].rows.p,
+                                tp.msched[l].off.p, p.iters, 1, tp.relax_hist[h--].p, nl, gx[l].p, grhs[l].p,
+                                gA[l].p, s);
       }
     }
     // Galerkin products, coarsest first
@@ -974,6 +1052,7 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
     }
   }
 
+  mark(kBwBase);
   // ---- point constraints -> density aggregates and the mean splat weight
   if (tp.screened) {
     for (int d = base; d <= top; ++d) {
@@ -987,6 +1066,7 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
     }
   }
 
+  mark(kBwPoints);
   // ---- normal loads (normal_load_adjoint.py:123-161)
   {
     HashMap nhash;
@@ -1065,11 +1145,14 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
       PSR_LAUNCH_CHECK();
     }
   }
+  mark(kBwNormalLoads);
 }
 
 template void solve_backward<float>(void*, const TreeData&, const DensityData<float>&, const NormalData<float>&,
                                     const std::vector<int64_t>&, const int64_t*, const HashMap&, const Params&,
-                                    const float*, std::vector<DBuf<float>>&, float*, float*, cudaStream_t);
+                                    const float*, std::vector<DBuf<float>>&, float*, float*, cudaStream_t,
+                                    EventMarks*);
 template void solve_backward<double>(void*, const TreeData&, const DensityData<double>&, const NormalData<double>&,
                                      const std::vector<int64_t>&, const int64_t*, const HashMap&, const Params&,
-                                     const double*, std::vector<DBuf<double>>&, double*, double*, cudaStream_t);
+                                     const double*, std::vector<DBuf<double>>&, double*, double*, cudaStream_t,
+                                     EventMarks*);

@@ -252,6 +252,9 @@ def reconstruct(positions, normals, *, depth=6, full_depth=3, base_depth=None, s
 
 
 # ---------------------------------------------------------------- differentiable reconstruction
+BACKWARD_STAGES = ("field", "mirrored_operators", "reverse_sweeps", "operator_adjoints", "base_multigrid",
+                   "point_constraints", "normal_loads", "splats_density_samples")
+
 class _ReconstructFunction(torch.autograd.Function):
     """Forward: a differentiable reconstruction.  Outputs the per-level coefficients, the
     cumulative coefficients, the isovalue and the 5-value sample normalisation; backward is
@@ -289,6 +292,9 @@ class _ReconstructFunction(torch.autograd.Function):
                 result.field._handle.ptr, p.data_ptr(), n.data_ptr(), p.shape[0], dtype_code,
                 ptr(keep[0]), ptr(keep[1]), float(g_iso) if g_iso is not None else 0.0, ptr(keep[2]),
                 g_p.data_ptr(), g_n.data_ptr(), _stream(p.device)))
+        info = _lib.Info()
+        _lib.check(_lib.load().psr_result_info(result.field._handle.ptr, ctypes.byref(info)))
+        ctx.box["backward_ms"] = dict(zip(BACKWARD_STAGES, (float(v) for v in info.backward_ms)))
         return (g_p if ctx.needs_input_grad[0] else None), (g_n if ctx.needs_input_grad[1] else None), None, None
 
 
@@ -378,4 +384,6 @@ def reconstruct_differentiable(positions, normals, **options):
         raise ValueError("keep_stages is not available for differentiable reconstructions")
     box = {}
     coefficients, cumulative, iso, normalization = _ReconstructFunction.apply(positions, normals, box, options)
-    return DifferentiableReconstruction(coefficients, cumulative, iso, normalization, box["result"])
+    out = DifferentiableReconstruction(coefficients, cumulative, iso, normalization, box["result"])
+    out.backward_stats = box  # box["backward_ms"]: device ms per stage of the last reverse pass
+    return out
