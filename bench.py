@@ -256,7 +256,7 @@ def run_ours(args, rank, world):
         "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": out_dtype, "data": "synthetic",
-        "config": {"workload": "bumpy sphere 800k points (SH l<=8, 10x density variation), depth 9, full depth 4, "
+        "config": {"workload": f"bumpy sphere {POINTS} points (SH l<=8, 10x density variation), depth {CONFIG['depth']}, full depth 4, "
                                "SPSR point weight 2, 8 GS iterations; step = differentiable reconstruction + "
                                "32-query centred-value loss + reverse pass onto positions and normals",
                    "points": POINTS, "coefficients": result["coefficients"],
@@ -351,7 +351,12 @@ def main():
     ap.add_argument("--precision", choices=("mixed", "input"), default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--depth", type=int, default=CONFIG["depth"],
+                    help="smaller cases for profiling only; the metric is quoted at depth 9")
+    ap.add_argument("--points", type=int, default=POINTS, help="points of the cloud (profiling cases)")
     args = ap.parse_args()
+    CONFIG["depth"] = args.depth
+    globals()["POINTS"] = args.points
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     if args.impl == "reference":

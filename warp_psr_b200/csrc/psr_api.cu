@@ -55,7 +55,7 @@ __global__ void column_insert_kernel(const int64_t* __restrict__ keys, int64_t n
   }
 }
 
-__global__ void dense_column_kernel(const int64_t* __restrict__ keys, int64_t n, int32_t* dense, int32_t* error) {
+__global__ void dense_column_kernel(const int64_t* __restrict__ keys, int64_t n, int2* dense, int32_t* error) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   int64_t k = keys[i];
@@ -67,7 +67,21 @@ __global__ void dense_column_kernel(const int64_t* __restrict__ keys, int64_t n,
     atomicExch(error, 1);
     return;
   }
-  dense[dense_column_base(d) + int64_t(c[0]) * side + c[1]] = int32_t(i);
+  dense[dense_column_base(d) + int64_t(c[0]) * side + c[1]] = make_int2(int32_t(i), 0);
+}
+
+// Second pass: the last key of each column stores the column's length.
+__global__ void dense_count_kernel(const int64_t* __restrict__ keys, int64_t n, int2* dense) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int64_t k = keys[i];
+  if (i + 1 < n && (keys[i + 1] >> 16) == (k >> 16)) return;
+  int c[3];
+  key_coords(k, c);
+  const int d = int(k >> 48), side = (1 << d) + 1;
+  if (d > kDenseColumnDepth || unsigned(c[0]) >= unsigned(side) || unsigned(c[1]) >= unsigned(side)) return;
+  int2* e = dense + dense_column_base(d) + int64_t(c[0]) * side + c[1];
+  e->y = int32_t(i + 1) - e->x;
 }
 }  // namespace psr
 

@@ -223,18 +223,49 @@ __host__ __device__ __forceinline__ int64_t dense_column_base(int d) {
 
 struct ColumnView {
   HashView h;
-  const int32_t* dense = nullptr;
+  const int2* dense = nullptr;  // {first index, length} per column, start -1 when empty
   const int64_t* keys = nullptr;
   int64_t n = 0;
   __host__ __device__ static __forceinline__ int64_t column_key(int d, int x, int y) { return basis_key(d, x, y, 0); }
   // Index of the first key of column (d, x, y), or -1.
   __device__ __forceinline__ int32_t column(int d, int x, int y) const {
+    int32_t count;
+    return column_range(d, x, y, count);
+  }
+  // First index and length of column (d, x, y) (-1 when absent).  Without the dense table
+  // the length is unknown and reported as INT32_MAX: the caller stops at the column's end.
+  __device__ __forceinline__ int32_t column_range(int d, int x, int y, int32_t& count) const {
     if (dense) {
       const int side = (1 << d) + 1;
+      count = 0;
       if (unsigned(x) >= unsigned(side) || unsigned(y) >= unsigned(side)) return -1;
-      return __ldg(dense + dense_column_base(d) + int64_t(x) * side + y);
+      const int2 e = __ldg(dense + dense_column_base(d) + int64_t(x) * side + y);
+      count = e.y;
+      return e.x;
     }
+    count = INT32_MAX;
     return h.find(column_key(d, x, y));
+  }
+  // First index in [start, start + count) of column `colk` (= key >> 16) whose z >= z0.
+  __device__ __forceinline__ int32_t lower_z(int32_t start, int32_t count, int64_t colk, int z0) const {
+    if (count != INT32_MAX) {
+      int32_t lo = start, hi = start + count;
+      while (lo < hi) {
+        const int32_t mid = (lo + hi) >> 1;
+        if (int(__ldg(keys + mid) & 65535) < z0)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      return lo;
+    }
+    int32_t j = start;
+    while (j < n) {
+      const int64_t k = __ldg(keys + j);
+      if ((k >> 16) != colk || int(k & 65535) >= z0) break;
+      ++j;
+    }
+    return j;
   }
   // Index of the key (d, x, y, z), or -1.
   __device__ __forceinline__ int32_t find(int d, int x, int y, int z) const {
@@ -252,11 +283,12 @@ struct ColumnView {
 
 __global__ void column_insert_kernel(const int64_t* __restrict__ keys, int64_t n, int64_t* hkeys, int32_t* hvals,
                                      uint64_t mask);
-__global__ void dense_column_kernel(const int64_t* __restrict__ keys, int64_t n, int32_t* dense, int32_t* error);
+__global__ void dense_column_kernel(const int64_t* __restrict__ keys, int64_t n, int2* dense, int32_t* error);
+__global__ void dense_count_kernel(const int64_t* __restrict__ keys, int64_t n, int2* dense);
 
 struct ColumnIndex {
   HashMap map;
-  DBuf<int32_t> table;
+  DBuf<int2> table;
   ColumnView view_;
   // `max_depth` bounds the depth of every key (coordinates within [0, 2^d]).
   void build(const int64_t* keys, int64_t n, int max_depth, cudaStream_t s) {
@@ -264,11 +296,13 @@ struct ColumnIndex {
     if (max_depth <= kDenseColumnDepth) {
       const int64_t size = dense_column_base(max_depth + 1);
       table.alloc(size, s);
-      PSR_CUDA(cudaMemsetAsync(table.p, 0xff, size * sizeof(int32_t), s));
+      PSR_CUDA(cudaMemsetAsync(table.p, 0xff, size * sizeof(int2), s));
       if (n > 0) {
         DBuf<int32_t> err(1, s);
         err.zero();
         dense_column_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, table.p, err.p);
+        PSR_LAUNCH_CHECK();
+        dense_count_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, table.p);
         PSR_LAUNCH_CHECK();
         if (read_scalar(err.p, s)) throw std::runtime_error("column index: key outside its depth's grid");
       }

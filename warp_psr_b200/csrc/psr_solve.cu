@@ -116,20 +116,24 @@ __device__ __forceinline__ uint32_t neighbours27(const ColumnView& cv, int d, co
     for (int dy = 0; dy < 3; ++dy) {
       int qy = ctr[1] + dy - 1;
       if (qy < 0 || qy > lim) continue;
-      int32_t j = cv.column(d, qx, qy);
-      if (j < 0) continue;
-      int64_t colk = ColumnView::column_key(d, qx, qy) >> 16;
-      int z0 = ctr[2] - 1;
-      for (; j < cv.n; ++j) {
-        int64_t key = __ldg(cv.keys + j);
+      int32_t count;
+      const int32_t j0 = cv.column_range(d, qx, qy, count);
+      if (j0 < 0) continue;
+      const int64_t colk = ColumnView::column_key(d, qx, qy) >> 16;
+      const int z0 = ctr[2] - 1;
+      const int64_t end = count == INT32_MAX ? cv.n : int64_t(j0) + count;
+      int32_t j = cv.lower_z(j0, count, colk, z0);
+      // the keys of z0, z0 + 1, z0 + 2 (those present) follow each other from j
+#pragma unroll
+      for (int dz = 0; dz < 3; ++dz) {
+        if (j >= end) break;
+        const int64_t key = __ldg(cv.keys + j);
         if ((key >> 16) != colk) break;
-        int dz = int(key & 65535) - z0;
-        if (dz > 2) break;
-        if (dz >= 0) {
-          int k = dx * 9 + dy * 3 + dz;
-          col[k] = int32_t(j - off);
-          present |= 1u << k;
-        }
+        if (int(key & 65535) != z0 + dz) continue;
+        const int k = dx * 9 + dy * 3 + dz;
+        col[k] = int32_t(j - off);
+        present |= 1u << k;
+        ++j;
       }
     }
   }
@@ -158,18 +162,24 @@ __global__ void normal_stencil_kernel(const int64_t* keys, int64_t n, int test_d
     for (int y = 0; y < width; ++y) {
       int ny = ctr[1] + y + first;
       if (ny < 0 || ny >= lim) continue;
-      int32_t j = cv.column(normal_depth, nx, ny);
-      if (j < 0) continue;
+      int32_t count;
+      const int32_t j0 = cv.column_range(normal_depth, nx, ny, count);
+      if (j0 < 0) continue;
       const double* iy = table + (c[1] * width + y) * 2;
-      int64_t colk = ColumnView::column_key(normal_depth, nx, ny) >> 16;
-      for (; j < cv.n; ++j) {  // ascending z: the reference's innermost loop order
-        int64_t key = __ldg(cv.keys + j);
+      const int64_t colk = ColumnView::column_key(normal_depth, nx, ny) >> 16;
+      const int64_t end = count == INT32_MAX ? cv.n : int64_t(j0) + count;
+      int32_t j = cv.lower_z(j0, count, colk, z0);
+      // ascending z inside the window: the reference's innermost loop order
+      for (int z = 0; z < width; ++z) {
+        if (j >= end) break;
+        const int64_t key = __ldg(cv.keys + j);
         if ((key >> 16) != colk) break;
-        int z = int(key & 65535) - z0;
-        if (z >= width) break;
-        if (z < 0 || int(key & 65535) >= lim) continue;
+        const int kz = int(key & 65535);
+        if (kz != z0 + z) continue;
+        ++j;
+        if (kz >= lim) continue;
         const double* iz = table + (c[2] * width + z) * 2;
-        const T* v = nvals + 4 * (int64_t(j) - noff);
+        const T* v = nvals + 4 * (int64_t(j - 1) - noff);
         value += double(v[0]) * ix[1] * iy[0] * iz[0];
         value += double(v[1]) * ix[0] * iy[1] * iz[0];
         value += double(v[2]) * ix[0] * iy[0] * iz[1];

@@ -739,16 +739,17 @@ __global__ void normal_stencil_reverse_kernel(const int64_t* nkeys, int64_t m, i
       const int cy = normal_center(yi, test_depth, normal_depth);
       const int oy = a[1] - cy - first;
       if (oy < 0 || oy >= width) continue;
-      int32_t r = tcv.column(test_depth, xi, yi);
-      if (r < 0) continue;
+      int32_t count;
+      const int32_t r0 = tcv.column_range(test_depth, xi, yi, count);
+      if (r0 < 0) continue;
       const double* iy = table + (yi * width + oy) * 2;
       const int64_t colk = ColumnView::column_key(test_depth, xi, yi) >> 16;
-      for (; r < tcv.n; ++r) {
+      const int64_t end = count == INT32_MAX ? tcv.n : int64_t(r0) + count;
+      for (int32_t r = tcv.lower_z(r0, count, colk, lo[2]); r < end; ++r) {
         const int64_t key = __ldg(tcv.keys + r);
         if ((key >> 16) != colk) break;
         const int zi = int(key & 65535);
         if (zi > hi[2]) break;
-        if (zi < lo[2]) continue;
         const int cz = normal_center(zi, test_depth, normal_depth);
         const int oz = a[2] - cz - first;
         if (oz < 0 || oz >= width) continue;
