@@ -269,15 +269,13 @@ struct ColumnView {
   }
   // Index of the key (d, x, y, z), or -1.
   __device__ __forceinline__ int32_t find(int d, int x, int y, int z) const {
-    int32_t j = column(d, x, y);
-    if (j < 0) return -1;
-    int64_t want = basis_key(d, x, y, z), col = column_key(d, x, y) >> 16;
-    for (; j < n; ++j) {
-      int64_t k = __ldg(keys + j);
-      if ((k >> 16) != col || k > want) return -1;
-      if (k == want) return j;
-    }
-    return -1;
+    int32_t count;
+    const int32_t j0 = column_range(d, x, y, count);
+    if (j0 < 0) return -1;
+    const int64_t col = column_key(d, x, y) >> 16;
+    const int32_t j = lower_z(j0, count, col, z);
+    if (j >= n || (count != INT32_MAX && j >= j0 + count)) return -1;
+    return __ldg(keys + j) == basis_key(d, x, y, z) ? j : -1;
   }
 };
 

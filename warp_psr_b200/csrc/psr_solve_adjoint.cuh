@@ -159,6 +159,9 @@ struct LevelReverse {
   PointsView<T> P;
   T* g_pos = nullptr;
   T* g_w = nullptr;
+  // when set, the row's operator adjoint is written here (27 per row, key order) and the
+  // screening VJP is left to screening_points_reverse_kernel
+  T* row_gA = nullptr;
 };
 
 template <class T, class S, class I, bool SLICED>
@@ -213,7 +216,7 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
       cpresent |= 1u << k;
       const T v = L.cvals[i * kSlots + k];
       if (gb != T(0)) atomicAdd(L.g_cum_prev + col, -(v * gb));
-      gC[k] = -(gb * L.cum_prev[col]);
+      if (!L.row_gA) gC[k] = -(gb * L.cum_prev[col]);
     }
   } else if (L.cross) {
     int ctr[3] = {c[0] >> 1, c[1] >> 1, c[2] >> 1};
@@ -234,6 +237,10 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
     }
   }
   if (!L.screened) return;
+  if (L.row_gA) {
+    for (int k = 0; k < 27; ++k) L.row_gA[i * 27 + k] = gA[k];
+    return;
+  }
   // screening VJP (point load: b = T(load) + T(0.5) T(point load))
   const T gl = T(0.5) * gb;
   const int nt = 1 << L.d, ntc = 1 << (L.d > 0 ? L.d - 1 : 0);
@@ -289,6 +296,93 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
       if (gw != T(0)) atomicAdd(L.g_w + index, gw);
     }
   }
+}
+
+// Screening VJP per point (assembly_adjoint.py:69-100, gathered): a point of bin cell b
+// (floor bins at depth d) enters the rows at the eight corners b + {0,1}^3 that exist; for
+// each, the point-load term, the same-depth trial functions (the corners of b) and, with a
+// cross operator, the depth d-1 trial functions (the corners of the point's depth d-1 bin).
+// Row adjoints come from level_reverse_kernel (gA, gC: 27 per row; gA may use a 28-slot
+// stride).  One thread per point, no atomics.
+template <class T>
+__global__ void screening_points_reverse_kernel(PointsView<T> P, int64_t m, int d, ColumnView cv, int64_t row_off,
+                                                const T* g_b, const T* gA, int gA_stride, const T* cum_prev,
+                                                int64_t coff, T* g_pos, T* g_w) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= m) return;
+  const T w = P.w[i];
+  if (w == T(0)) return;
+  const T p[3] = {P.pos[3 * i], P.pos[3 * i + 1], P.pos[3 * i + 2]};
+  const int nt = 1 << d, ntc = 1 << (d > 0 ? d - 1 : 0);
+  int b[3], bc[3];
+  for (int a = 0; a < 3; ++a) {
+    b[a] = min(max(int(floor(p[a] * T(nt))), 0), nt - 1);
+    bc[a] = min(max(int(floor(p[a] * T(ntc))), 0), ntc - 1);
+  }
+  // cross trial functions: the corners of the point's depth d-1 bin, with the coarser
+  // cumulative solution there (the cross operator's adjoint is -g_b(row) * cumulative(q))
+  T cq[8];
+  if (cum_prev) {
+    for (int e = 0; e < 8; ++e) {
+      const int q[3] = {bc[0] + e / 4, bc[1] + (e / 2) % 2, bc[2] + e % 2};
+      const int32_t j = cv.find(d - 1, q[0], q[1], q[2]);
+      cq[e] = j >= 0 ? cum_prev[int64_t(j) - coff] : T(0);
+    }
+  }
+  T gp[3] = {T(0), T(0), T(0)};
+  T gw = T(0);
+  for (int ex = 0; ex < 2; ++ex)
+    for (int ey = 0; ey < 2; ++ey) {
+      int32_t count;
+      const int rx = b[0] + ex, ry = b[1] + ey;
+      const int32_t j0 = cv.column_range(d, rx, ry, count);
+      if (j0 < 0) continue;
+      const int64_t colk = ColumnView::column_key(d, rx, ry) >> 16;
+      const int64_t end = count == INT32_MAX ? cv.n : int64_t(j0) + count;
+      int32_t j = cv.lower_z(j0, count, colk, b[2]);
+      for (int ez = 0; ez < 2; ++ez) {
+        if (j >= end) break;
+        const int64_t key = __ldg(cv.keys + j);
+        if ((key >> 16) != colk) break;
+        const int rz = int(key & 65535);
+        if (rz != b[2] + ez) continue;
+        const int64_t row = int64_t(j) - row_off;
+        ++j;
+        const int r[3] = {rx, ry, rz};
+        T dphi[3];
+        const T phi = hat3_grad(p, r, d, dphi);
+        const T gl = T(0.5) * g_b[row];
+        gw = gw + gl * phi;
+        for (int a = 0; a < 3; ++a) gp[a] = gp[a] + gl * w * dphi[a];
+        const T* ga = gA + row * gA_stride;
+        for (int e = 0; e < 8; ++e) {
+          const int q[3] = {b[0] + e / 4, b[1] + (e / 2) % 2, b[2] + e % 2};
+          const int k = (q[0] - r[0] + 1) * 9 + (q[1] - r[1] + 1) * 3 + (q[2] - r[2] + 1);
+          const T g = ga[k];
+          if (g == T(0)) continue;
+          T dtr[3];
+          const T tr = hat3_grad(p, q, d, dtr);
+          const T gwp = g * w;
+          gw = gw + g * (phi * tr);
+          for (int a = 0; a < 3; ++a) gp[a] = gp[a] + (gwp * tr) * dphi[a] + (gwp * phi) * dtr[a];
+        }
+        if (cum_prev) {
+          const T gbr = g_b[row];
+          for (int e = 0; e < 8; ++e) {
+            const int q[3] = {bc[0] + e / 4, bc[1] + (e / 2) % 2, bc[2] + e % 2};
+            const T g = -(gbr * cq[e]);
+            if (g == T(0)) continue;
+            T dtr[3];
+            const T tr = hat3_grad(p, q, d - 1, dtr);
+            const T gwp = g * w;
+            gw = gw + g * (phi * tr);
+            for (int a = 0; a < 3; ++a) gp[a] = gp[a] + (gwp * tr) * dphi[a] + (gwp * phi) * dtr[a];
+          }
+        }
+      }
+    }
+  for (int a = 0; a < 3; ++a) g_pos[3 * i + a] = g_pos[3 * i + a] + gp[a];
+  g_w[i] = g_w[i] + gw;
 }
 
 // g_coarse[parent] += w * g_fine[i] over the prolongation stencil (transpose of prolong_add).
@@ -917,13 +1011,23 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
       L.cum_prev = tp.cum[d - 1].p;
       L.g_cum_prev = g_cum[d - 1].p;
       L.screened = tp.screened;
+      DBuf<T> rA;
       if (tp.screened) {
         L.P = tp.points[d].view();
         L.g_pos = g_pos[d].p;
         L.g_w = g_w[d].p;
+        rA.alloc(27 * n, s);
+        L.row_gA = rA.p;
       }
       level_reverse_kernel<T, S, I, true><<<blocks_for(n, 128), 128, 0, s>>>(L);
       PSR_LAUNCH_CHECK();
+      if (tp.screened && tp.points[d].m) {
+        const int64_t m = tp.points[d].m;
+        screening_points_reverse_kernel<T><<<blocks_for(m, 128), 128, 0, s>>>(
+            L.P, m, d, bcv, level_offsets[d], g_b.p, rA.p, 27, tp.cum[d - 1].p, level_offsets[d - 1], g_pos[d].p,
+            g_w[d].p);
+        PSR_LAUNCH_CHECK();
+      }
     };
     if (st.sched.wide)
       fused(T(), int32_t());
@@ -1046,8 +1150,13 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
       L.g_w = g_w[base].p;
     }
     if (nb) {
-      level_reverse_kernel<T, T, int32_t, false><<<blocks_for(nb, 128), 128, 0, s>>>(L);
-      PSR_LAUNCH_CHECK();
+      if (tp.screened && tp.points[base].m) {
+        const int64_t m = tp.points[base].m;
+        screening_points_reverse_kernel<T><<<blocks_for(m, 128), 128, 0, s>>>(
+            L.P, m, base, bcv, level_offsets[base], grhs[base].p, gA[base].p, kSlots, nullptr, 0, g_pos[base].p,
+            g_w[base].p);
+        PSR_LAUNCH_CHECK();
+      }
       to_double_kernel<T><<<blocks_for(nb), kThreads, 0, s>>>(grhs[base].p, nb, g_load[base].p);
       PSR_LAUNCH_CHECK();
     }
