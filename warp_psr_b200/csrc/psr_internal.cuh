@@ -3,6 +3,7 @@
 #pragma once
 #include "psr_common.cuh"
 
+#include <cstring>
 #include <map>
 #include <memory>
 #include <string>
@@ -171,6 +172,14 @@ void solve_backward(void* tape, const TreeData& tree, const DensityData<T>& D, c
 template <class T, class V>
 void relax_sliced_ell(const int32_t* cols, const T* vals, const V* b, V* x, const int32_t* rows,
                       const int32_t* group_off, int depth, int iters, cudaStream_t s, float* ms);
+
+// Index rows of the schedule-order operator: 32 slots (0..26 neighbours, 27 own index); the
+// padding slots 28..31 carry 1 / A_ii in the vector precision (write_inv_diag).
+template <class V, class I>
+__host__ __device__ __forceinline__ void write_inv_diag(I* row, V inv) {
+  static_assert(4 * sizeof(I) >= sizeof(V), "index padding too small for the reciprocal");
+  memcpy(reinterpret_cast<char*>(row + 28), &inv, sizeof(V));
+}
 
 // Schedule order of a sliced level: rows sorted by (slice, colour), key order inside a group.
 struct StripSchedule {

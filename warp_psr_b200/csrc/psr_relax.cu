@@ -37,7 +37,22 @@
 namespace psr {
 
 constexpr int kSlotsR = 28;
-constexpr int kIdxSlots = 32;  // neighbour index rows: slots 0..26, own index at 27, padding
+constexpr int kIdxSlots = 32;  // neighbour index rows: slots 0..26, own index at 27, then 1 / A_ii
+
+// The padding of an index row (slots 28..31, 8 bytes or more) carries the row's reciprocal
+// diagonal 1 / A_ii in the vector precision, computed exactly as the update would
+// (V(1) / V(A_ii)), so the sweep multiplies instead of dividing on its critical path.
+template <class V, class I>
+__host__ __device__ __forceinline__ void put_inv_diag(I* row, V inv) {
+  static_assert(4 * sizeof(I) >= sizeof(V), "index padding too small for the reciprocal");
+  memcpy(reinterpret_cast<char*>(row + 28), &inv, sizeof(V));
+}
+template <class V, class I>
+__host__ __device__ __forceinline__ V get_inv_diag(const I* row) {
+  V inv;
+  memcpy(&inv, reinterpret_cast<const char*>(row + 28), sizeof(V));
+  return inv;
+}
 constexpr int kPad = 32;       // one 128-byte line per slice counter
 constexpr int kRelaxThreads = 512;
 
@@ -173,7 +188,7 @@ __device__ __forceinline__ void update_row(const I* nrow, const T* arow, V bv, V
   }
   V inc = V(0);
   if (n[13] >= 0 && a[13] != T(0)) {
-    inc = r * (V(1.0) / V(a[13]));
+    inc = r * get_inv_diag<V>(n);
     foot[self] = xs[13] + inc;
   }
   if (rec) *rec = record_increment ? inc : foot[self];
@@ -505,6 +520,8 @@ __global__ void reorder_kernel(const int32_t* perm, const int32_t* inv, const in
   }
   sidx[p * kIdxSlots + 27] = I(p - group_off[group_of(keys[row])]);
   for (int k = 28; k < kIdxSlots; ++k) sidx[p * kIdxSlots + k] = I(-1);
+  const T diag = vals[row * kSlotsR + 13];
+  put_inv_diag<V>(sidx + p * kIdxSlots, diag != T(0) ? V(1.0) / V(diag) : V(0));
   sb[p] = b[row];
   sx[p] = x[row];
   skeys[p] = keys[row];

@@ -447,6 +447,7 @@ __global__ void assemble_sliced_kernel(const int64_t* keys, int64_t n, int d, Co
   v[27] = S(0);
   idx[27] = I(p - group_off[4 * c[2] + (c[0] & 1) + 2 * (c[1] & 1)]);
   for (int k = 28; k < 32; ++k) idx[k] = I(-1);
+  write_inv_diag<T>(idx, v[13] != S(0) ? T(1.0) / T(v[13]) : T(0));
   int4* vd = reinterpret_cast<int4*>(svals + p * 28);
   const int4* vs = reinterpret_cast<const int4*>(v);
   for (int q = 0; q < 28 * int(sizeof(S)) / 16; ++q) vd[q] = vs[q];

@@ -115,7 +115,7 @@ __global__ void mirror_operator_kernel(int64_t n, int depth, const int32_t* perm
   }
   tvals[p2 * kSlots + 27] = S(0);
   tidx[p2 * kIdxSlots + 27] = I(p2 - off2[sched_group(m)]);
-  for (int k = 28; k < kIdxSlots; ++k) tidx[p2 * kIdxSlots + k] = I(-1);
+  for (int k = 28; k < kIdxSlots; ++k) tidx[p2 * kIdxSlots + k] = row[k];  // 1 / A_ii: same diagonal
 }
 
 template <class T>
