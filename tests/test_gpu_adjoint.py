@@ -38,6 +38,8 @@ CASES = {
     "sliced_levels_screened": dict(depth=5, full_depth=3, point_weight=2.0, iters=3),
     "sliced_levels_psr": dict(depth=5, full_depth=3, point_weight=0.0, iters=3),
     "spsr_base0": dict(depth=4, full_depth=0, base_depth=0, point_weight=2.0, iters=2, samples_per_node=.5),
+    # the default 8 sweeps take the unrolled reverse kernels
+    "sliced_levels_8_sweeps": dict(depth=5, full_depth=3, point_weight=2.0, iters=8),
 }
 
 

@@ -3,6 +3,7 @@
 #include "../../include/psr_b200.h"
 #include "psr_internal.cuh"
 
+#include <algorithm>
 #include <mutex>
 
 namespace psr {
@@ -444,18 +445,20 @@ __global__ void isovalue_reverse_kernel(const T* weights, int64_t n, double g_is
   if (i < n) g_values[i] = T(g_iso / mass[0]) * weights[i];
 }
 
+// Total sample weight (float64), block sums added atomically (mass must start at zero).
 template <class T>
 __global__ void mass_kernel(const T* weights, int64_t n, double* mass) {
   __shared__ double red[256];
   double acc = 0.0;
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) acc += double(weights[i]);
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    acc += double(weights[i]);
   red[threadIdx.x] = acc;
   __syncthreads();
   for (int st = 128; st > 0; st >>= 1) {
     if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
     __syncthreads();
   }
-  if (threadIdx.x == 0) mass[0] = red[0];
+  if (threadIdx.x == 0) atomicAdd(mass, red[0]);
 }
 
 // cumulative_kernel reversed for one depth: g_coeff += g_cum; parents receive h * g_cum.
@@ -486,7 +489,8 @@ void field_backward(const int64_t* keys, const std::vector<int64_t>& offsets, co
                     T* g_coeff, T* g_cum, T* g_sums, cudaStream_t s) {
   if (g_iso != 0.0 && groups > 0) {
     DBuf<double> mass(1, s);
-    mass_kernel<T><<<1, 256, 0, s>>>(gweights, groups, mass.p);
+    mass.zero();
+    mass_kernel<T><<<std::min<int64_t>(blocks_for(groups), 592), 256, 0, s>>>(gweights, groups, mass.p);
     PSR_LAUNCH_CHECK();
     DBuf<T> gv(groups, s);
     isovalue_reverse_kernel<T><<<blocks_for(groups), kThreads, 0, s>>>(gweights, groups, g_iso, mass.p, gv.p);

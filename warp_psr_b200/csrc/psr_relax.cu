@@ -445,21 +445,37 @@ __global__ void xstart_kernel(const int64_t* skeys, const int32_t* group_off, in
 
 // Row-balanced strip boundaries: slice z's rows split into `strips` runs of x of about equal size.
 __global__ void strip_bounds_kernel(const int32_t* xstart, int n, int strips, int32_t* bounds) {
-  int z = blockIdx.x * blockDim.x + threadIdx.x;
-  if (z > n) return;
-  int nx = n + 2;
-  const int32_t* xs = xstart + int64_t(z * 4) * nx;
-  int total = 0;
-  for (int c = 0; c < 4; ++c) total += xs[c * nx + n + 1] - xs[c * nx];
+  // One thread per (slice z, boundary k): boundary k is the smallest Y in [1, n+1] with
+  // rows(x < Y) * strips >= k * rows(slice), found by binary search (rows(x < Y) grows with Y).
+  const int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (idx >= int64_t(n + 1) * (strips + 1)) return;
+  const int z = int(idx / (strips + 1)), k = int(idx % (strips + 1));
   int32_t* out = bounds + int64_t(z) * (strips + 1);
-  out[0] = 0;
-  int k = 1, below = 0;
-  for (int X = 0; X <= n && k < strips; ++X) {
-    for (int c = 0; c < 4; ++c) below += xs[c * nx + X + 1] - xs[c * nx + X];
-    while (k < strips && int64_t(below) * strips >= int64_t(k) * total) out[k++] = X + 1;
+  if (k == 0) {
+    out[0] = 0;
+    return;
   }
-  while (k < strips) out[k++] = n + 1;
-  out[strips] = n + 1;
+  if (k == strips) {
+    out[strips] = n + 1;
+    return;
+  }
+  const int nx = n + 2;
+  const int32_t* xs = xstart + int64_t(z * 4) * nx;
+  auto rows_below = [&](int Y) {
+    int r = 0;
+    for (int c = 0; c < 4; ++c) r += xs[c * nx + Y] - xs[c * nx];
+    return r;
+  };
+  const int64_t total = rows_below(n + 1);
+  int lo = 1, hi = n + 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (int64_t(rows_below(mid)) * strips >= int64_t(k) * total)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  out[k] = lo;
 }
 
 // Largest footprint, update-row count and staged right-hand-side span over all tasks.
@@ -621,7 +637,7 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
     if (forced >= 1 && forced <= 256) strips = forced;
   }
   DBuf<int32_t> bounds(int64_t(n + 1) * (strips + 1), s);
-  strip_bounds_kernel<<<blocks_for(n + 1), kThreads, 0, s>>>(xstart.p, n, strips, bounds.p);
+  strip_bounds_kernel<<<blocks_for(int64_t(n + 1) * (strips + 1)), kThreads, 0, s>>>(xstart.p, n, strips, bounds.p);
   PSR_LAUNCH_CHECK();
   const int64_t pad_end = int64_t(n + 1) * kPad;
   DBuf<int> flags(pad_end + 4 * kPad, s);

@@ -164,7 +164,7 @@ struct LevelReverse {
   T* row_gA = nullptr;
 };
 
-template <class T, class S, class I, bool SLICED>
+template <class T, class S, class I, bool SLICED, int ITERS = 0>
 __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= L.n) return;
@@ -176,8 +176,23 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
   for (int k = 0; k < 27; ++k) gA[k] = T(0);
   if (SLICED) {
     const int64_t p = L.inv[i], p2 = L.inv2[i];
-    const I* row = L.sidx + p * kIdxSlots;
     const int own = (c[0] & 1) + 2 * (c[1] & 1);
+    // the row's index record (vector loads) and its increments of every visit, loaded once
+    __align__(16) I row[kIdxSlots];
+    {
+      const int4* src = reinterpret_cast<const int4*>(L.sidx + p * kIdxSlots);
+      int4* dst = reinterpret_cast<int4*>(row);
+#pragma unroll
+      for (int q = 0; q < kIdxSlots * int(sizeof(I)) / 16; ++q) dst[q] = __ldg(src + q);
+    }
+    const int iters = ITERS > 0 ? ITERS : L.iters;
+    const T* mrow = L.mu + p2 * iters;
+    // fixed visit count (the common 8): records in registers, vector loads
+    T mu[ITERS > 0 ? ITERS : 1];
+    if constexpr (ITERS > 0) {
+#pragma unroll
+      for (int u = 0; u < ITERS; ++u) mu[u] = __ldg(mrow + u);  // mirrored visit u = forward visit ITERS-1-u
+    }
     for (int k = 0; k < 27; ++k) {
       const I idx = row[k];
       if (idx < 0) continue;
@@ -185,15 +200,26 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
       const int64_t pk = L.off[sched_group(q)] + int64_t(idx);
       const int qc = (q[0] & 1) + 2 * (q[1] & 1);
       // 0: the neighbour's value after this visit, 1: after the previous visit
-      const int delay = k == 13 ? 0 : (q[2] > c[2] || (q[2] == c[2] && qc < own)) ? 0 : 1;
+      const bool delayed = !(k == 13 || q[2] > c[2] || (q[2] == c[2] && qc < own));
       T acc = T(0);
-      const T* mrow = L.mu + p2 * L.iters;
-      const T* xrow = L.xhist + pk * L.iters;
-      for (int t = 0; t < L.iters; ++t) {
-        const T m = mrow[L.iters - 1 - t];
-        const int tv = t - delay;
-        const T xv = tv >= 0 ? xrow[tv] : T(0);
-        acc = acc - m * xv;
+      const T* xrow = L.xhist + pk * iters;
+      if constexpr (ITERS > 0) {
+        T xv[ITERS];
+#pragma unroll
+        for (int t = 0; t < ITERS; ++t) xv[t] = __ldg(xrow + t);
+#pragma unroll
+        for (int t = 0; t < ITERS; ++t) {
+          const T x_now = xv[t];
+          const T x_prev = t > 0 ? xv[t > 0 ? t - 1 : 0] : T(0);
+          acc = acc - mu[ITERS - 1 - t] * (delayed ? x_prev : x_now);
+        }
+      } else {
+        for (int t = 0; t < iters; ++t) {
+          const T m = mrow[iters - 1 - t];
+          const int tv = delayed ? t - 1 : t;
+          const T xv = tv >= 0 ? xrow[tv] : T(0);
+          acc = acc - m * xv;
+        }
       }
       gA[k] = acc;
     }
@@ -209,9 +235,16 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
   if (L.cross && L.ccols) {
     int ctr[3] = {c[0] >> 1, c[1] >> 1, c[2] >> 1};
     for (int a = 0; a < 3; ++a) q0c[a] = ctr[a] - 1;
+    __align__(16) int32_t ccr[kSlots];
+    {
+      const int4* src = reinterpret_cast<const int4*>(L.ccols + i * kSlots);
+      int4* dst = reinterpret_cast<int4*>(ccr);
+#pragma unroll
+      for (int q = 0; q < kSlots / 4; ++q) dst[q] = __ldg(src + q);
+    }
     for (int k = 0; k < 27; ++k) {
       gC[k] = T(0);
-      const int32_t col = L.ccols[i * kSlots + k];
+      const int32_t col = ccr[k];
       if (col < 0) continue;
       cpresent |= 1u << k;
       const T v = L.cvals[i * kSlots + k];
@@ -296,6 +329,73 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
       if (gw != T(0)) atomicAdd(L.g_w + index, gw);
     }
   }
+}
+
+// The per-row pass of a sliced level with the stored cross operator, unrolled so that every
+// per-slot quantity stays in registers: the operator adjoint of the row (written to row_gA,
+// 27 per row, for the per-point screening pass) and -C^T g_b into the coarser cumulative.
+template <class T, class I, int ITERS>
+__global__ void __launch_bounds__(128) level_rows_reverse_kernel(const int64_t* __restrict__ keys, int64_t n,
+                                                                 const int32_t* __restrict__ inv,
+                                                                 const int32_t* __restrict__ inv2,
+                                                                 const int32_t* __restrict__ off,
+                                                                 const I* __restrict__ sidx,
+                                                                 const T* __restrict__ xhist,
+                                                                 const T* __restrict__ mu_hist,
+                                                                 const T* __restrict__ g_b,
+                                                                 const int32_t* __restrict__ ccols,
+                                                                 const T* __restrict__ cvals, T* g_cum_prev,
+                                                                 T* row_gA) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int c[3];
+  key_coords(keys[i], c);
+  const int64_t p = inv[i], p2 = inv2[i];
+  const int own = (c[0] & 1) + 2 * (c[1] & 1);
+  __align__(16) I row[kIdxSlots];
+  {
+    const int4* src = reinterpret_cast<const int4*>(sidx + p * kIdxSlots);
+    int4* dst = reinterpret_cast<int4*>(row);
+#pragma unroll
+    for (int q = 0; q < kIdxSlots * int(sizeof(I)) / 16; ++q) dst[q] = __ldg(src + q);
+  }
+  T mu[ITERS];
+#pragma unroll
+  for (int u = 0; u < ITERS; ++u) mu[u] = __ldg(mu_hist + p2 * ITERS + u);  // mirrored visit u
+  T* out = row_gA ? row_gA + i * 27 : nullptr;
+#pragma unroll
+  for (int k = 0; k < 27; ++k) {
+    const I idx = row[k];
+    T acc = T(0);
+    if (idx >= 0) {
+      const int q[3] = {c[0] + k / 9 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k % 3 - 1};
+      const int64_t pk = __ldg(off + sched_group(q)) + int64_t(idx);
+      const int qc = (q[0] & 1) + 2 * (q[1] & 1);
+      const bool delayed = !(k == 13 || k % 3 == 2 || (k % 3 == 1 && qc < own));
+      const T* xrow = xhist + pk * ITERS;
+      T xv[ITERS];
+#pragma unroll
+      for (int t = 0; t < ITERS; ++t) xv[t] = __ldg(xrow + t);
+#pragma unroll
+      for (int t = 0; t < ITERS; ++t) {
+        const T x_prev = t > 0 ? xv[t > 0 ? t - 1 : 0] : T(0);
+        acc = acc - mu[ITERS - 1 - t] * (delayed ? x_prev : xv[t]);
+      }
+    }
+    if (out) out[k] = acc;
+  }
+  const T gb = g_b[i];
+  if (gb == T(0)) return;
+  __align__(16) int32_t cc[kSlots];
+  {
+    const int4* src = reinterpret_cast<const int4*>(ccols + i * kSlots);
+    int4* dst = reinterpret_cast<int4*>(cc);
+#pragma unroll
+    for (int q = 0; q < kSlots / 4; ++q) dst[q] = __ldg(src + q);
+  }
+#pragma unroll
+  for (int k = 0; k < 27; ++k)
+    if (cc[k] >= 0) atomicAdd(g_cum_prev + cc[k], -(__ldg(cvals + i * kSlots + k) * gb));
 }
 
 // Screening VJP per point (assembly_adjoint.py:69-100, gathered): a point of bin cell b
@@ -777,8 +877,9 @@ __global__ void root_reverse_kernel(const int64_t* keys, int nk, const int32_t* 
 template <class T>
 __global__ void points_reverse_kernel(const int64_t* keys, const T* vals, int64_t m, int d, T pw, const T* average,
                                       const T* w_out, const T* g_pos, const T* g_w, T* g_vals, T* g_average) {
-  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i >= m) return;
+  int64_t i0 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  const int64_t i = i0 < m ? i0 : m - 1;  // every thread reaches the block reduction
+  const bool live = i0 < m;
   const T* v = vals + 4 * i;
   T gv[4] = {T(0), T(0), T(0), T(0)};
   for (int a = 0; a < 3; ++a) {
@@ -786,13 +887,24 @@ __global__ void points_reverse_kernel(const int64_t* keys, const T* vals, int64_
     gv[a] = gv[a] + g / v[3];
     gv[3] = gv[3] - g * (v[a] / v[3]) / v[3];
   }
-  if (w_out[i] != T(0)) {
+  T gavg = T(0);
+  if (live && w_out[i] != T(0)) {
     const T g = g_w[i];
     const T scale = T(1 << d);
     gv[3] = gv[3] + g * scale * (pw * average[1]);
-    if (g != T(0)) atomicAdd(g_average + 1, g * v[3] * scale * pw);
+    gavg = g * v[3] * scale * pw;
   }
-  for (int a = 0; a < 4; ++a) g_vals[4 * i + a] = g_vals[4 * i + a] + gv[a];
+  if (live)
+    for (int a = 0; a < 4; ++a) g_vals[4 * i + a] = g_vals[4 * i + a] + gv[a];
+  // the mean-weight adjoint: block sum, one atomic per block
+  __shared__ T red[kThreads];
+  red[threadIdx.x] = gavg;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && red[0] != T(0)) atomicAdd(g_average + 1, red[0]);
 }
 
 // ------------------------------------------------------------------ normal loads reversed
@@ -1019,7 +1131,13 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
         rA.alloc(27 * n, s);
         L.row_gA = rA.p;
       }
-      level_reverse_kernel<T, S, I, true><<<blocks_for(n, 128), 128, 0, s>>>(L);
+      if (p.iters == 8 && L.ccols) {
+        level_rows_reverse_kernel<T, I, 8><<<blocks_for(n, 128), 128, 0, s>>>(
+            L.keys, n, L.inv, L.inv2, L.off, L.sidx, L.xhist, L.mu, L.g_b, L.ccols, L.cvals, L.g_cum_prev,
+            tp.screened ? rA.p : nullptr);
+      } else {
+        level_reverse_kernel<T, S, I, true, 0><<<blocks_for(n, 128), 128, 0, s>>>(L);
+      }
       PSR_LAUNCH_CHECK();
       if (tp.screened && tp.points[d].m) {
         const int64_t m = tp.points[d].m;
