@@ -120,8 +120,7 @@ def field_error(result, reference, queries):
 
 def run_ours(args, rank, world):
     import torch
-    import torch.distributed as dist
-    from warp_psr_b200 import reconstruct, reconstruct_differentiable, _lib
+    from warp_psr_b200 import reconstruct, reconstruct_differentiable, _lib, replicas
 
     device = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(device)
@@ -188,8 +187,7 @@ def run_ours(args, rank, world):
             total += a.elapsed_time(b)
         return total / k, last
 
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     launches0 = _lib.kernel_launches()
     finest.clear()
@@ -202,11 +200,8 @@ def run_ours(args, rank, world):
     fwd_ms = statistics.mean(x[0] for x in split)
     bwd_ms = statistics.mean(x[1] for x in split)
     torch.cuda.synchronize()
-    if world > 1:
-        t = torch.tensor([ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = t.item()
-        dist.barrier()
+    ms = replicas.max_over_ranks(ms, device)
+    replicas.barrier()
 
     # End to end through the public API with host buffers: pinned H2D copy of the cloud, the
     # solve+adjoint step, and the device-to-host read of the position and normal gradients.
@@ -221,10 +216,7 @@ def run_ours(args, rank, world):
         return None
 
     e2e_ms, _ = timed(e2e_step, args.steps)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = t.item()
+    e2e_ms = replicas.max_over_ranks(e2e_ms, device)
     # the forward alone, not differentiable (what reconstruct() costs)
     plain_ms, _ = timed(lambda: reconstruct(p_dev, n_dev, precision=args.precision, **CONFIG), max(1, args.steps // 2))
 

@@ -174,3 +174,11 @@ def test_omitted_nan_normal_and_positions_only():
     v, _, _ = res.evaluate(torch.tensor([[.1, .1, .1]], device="cuda", dtype=torch.float64), centered=True)
     v.sum().backward()
     assert torch.isfinite(P2.grad).all() and N2.grad is None
+
+
+def test_reconstruct_many_single_process():
+    from warp_psr_b200 import replicas
+    p0, m0 = cloud()
+    clouds = [(torch.tensor(p0, device="cuda"), torch.tensor(m0, device="cuda"))] * 2
+    out = replicas.reconstruct_many(clouds, depth=4, full_depth=2)
+    assert [o[0] for o in out] == [0, 1] and out[0][1] == out[1][1]
