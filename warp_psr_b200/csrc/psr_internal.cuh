@@ -197,9 +197,10 @@ void build_strip_schedule(const int64_t* keys, int64_t rows, int depth, StripSch
 // holds the initial guess and receives the result.
 //
 // `hist` (optional, rows x iters in schedule order: row p, visit t at p * iters + t) receives
-// per visit the new x of every row, or with `record_increment` the update r / A_ii.  `rev` runs the colours of a slice in the
-// order 3, 2, 1, 0: on the z-mirrored schedule this is the exact reverse of the forward
-// sequential order (used by the adjoint).
+// per visit the new x of every row, or with `record_increment` the update r / A_ii.  `rev`
+// runs the exact reverse of the forward sequential order over the same schedule-order rows:
+// slices 2^d .. 0 (logical slice z is stored slice 2^d - z) and the colours of a slice in the
+// order 3, 2, 1, 0 (used by the adjoint on the transposed operator).
 template <class T, class V, class I>
 void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sidx, const V* sb, V* x, int iters,
                             cudaStream_t s, float* ms, V* hist = nullptr, bool rev = false,

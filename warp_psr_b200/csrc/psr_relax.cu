@@ -80,7 +80,6 @@ struct StripLevel {
   int64_t rows;              // rows of the level
   int iters;                 // visits per slice
   int record_increment;      // hist holds the update r / A_ii (else the new x)
-  int rev;                   // colours in the order 3, 2, 1, 0 (the mirrored adjoint sweep)
 };
 
 __device__ __forceinline__ long long globaltimer() {
@@ -137,9 +136,9 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 
 // Footprint range (j * 4 + colour) of slot k for a row of colour C: slice z-1+(k%3),
 // colour of (x + k/9 - 1, y + (k/3)%3 - 1).
-template <int C>
+template <int C, bool M = false>
 __device__ __forceinline__ constexpr int slot_range(int k) {
-  return (k % 3) * 4 + (((C & 1) + k / 9 + 1) & 1) + 2 * (((C >> 1) + (k / 3) % 3 + 1) & 1);
+  return (M ? 2 - k % 3 : k % 3) * 4 + (((C & 1) + k / 9 + 1) & 1) + 2 * (((C >> 1) + (k / 3) % 3 + 1) & 1);
 }
 
 template <class T>
@@ -160,7 +159,7 @@ __device__ __forceinline__ void load_idx(const I* src, I out[kIdxSlots]) {
 // One row of colour C: r = b - sum_k x_k A_k in slot order; x_self += r / A_self.
 // A neighbour index outside the staged footprint (only possible for an operator whose slot
 // k is not the k-th neighbour) is reported through `error` and not accessed.
-template <int C, class T, class V, class I>
+template <int C, bool M, class T, class V, class I>
 __device__ __forceinline__ void update_row(const I* nrow, const T* arow, V bv, V* foot, const int* delta,
                                            unsigned total, int* error, V* rec, bool record_increment) {
   __align__(16) I n[kIdxSlots];  // filled with 16-byte vector loads
@@ -171,7 +170,7 @@ __device__ __forceinline__ void update_row(const I* nrow, const T* arow, V bv, V
   bool bad = false;
 #pragma unroll
   for (int k = 0; k < 27; ++k) {
-    unsigned fi = unsigned(int(n[k]) + delta[slot_range<C>(k)]);
+    unsigned fi = unsigned(int(n[k]) + delta[slot_range<C, M>(k)]);
     bool ok = n[k] >= 0 && fi < total;
     bad |= n[k] >= 0 && fi >= total;
     xs[k] = ok ? foot[fi] : V(0);
@@ -197,7 +196,7 @@ __device__ __forceinline__ void update_row(const I* nrow, const T* arow, V bv, V
 // `hist` (optional) points at this visit's record column (row p records at hist[p * iters]);
 // only the strip's own rows [o0, o1) write it (halo rows are recomputed by the neighbouring
 // strip, which owns them).
-template <int C, class T, class V, class I>
+template <int C, bool M, class T, class V, class I>
 __device__ __forceinline__ void phase(const StripLevel& L, bool staged, int p0, int p1, int rbase, int bshift,
                                       const I* s_idx, const T* s_vals, const V* s_b, V* foot, const int* delta,
                                       unsigned total, V* hist, int o0, int o1) {
@@ -209,16 +208,20 @@ __device__ __forceinline__ void phase(const StripLevel& L, bool staged, int p0, 
     V* rec = (hist && p >= o0 && p < o1) ? hist + int64_t(p) * L.iters : nullptr;
     if (staged) {
       int i = rbase + (p - p0);
-      update_row<C>(s_idx + int64_t(i) * kIdxSlots, s_vals + int64_t(i) * kSlotsR, s_b[bshift + (p - p0)], foot,
-                    delta, total, L.error, rec, inc);
+      update_row<C, M>(s_idx + int64_t(i) * kIdxSlots, s_vals + int64_t(i) * kSlotsR, s_b[bshift + (p - p0)], foot,
+                       delta, total, L.error, rec, inc);
     } else {
-      update_row<C>(gidx + int64_t(p) * kIdxSlots, gvals + int64_t(p) * kSlotsR, gb[p], foot, delta, total, L.error,
-                    rec, inc);
+      update_row<C, M>(gidx + int64_t(p) * kIdxSlots, gvals + int64_t(p) * kSlotsR, gb[p], foot, delta, total,
+                       L.error, rec, inc);
     }
   }
 }
 
-template <class T, class V, class I>
+// REV false: colours 0..3 in the stored slice order (the forward sweep).  REV true: the exact
+// reverse of that sweep on the same layout -- logical slice z is stored slice n - z (so slot
+// k's neighbour lies in logical slice z + 1 - k % 3) and the colours run 3..0.  One
+// instantiation per order keeps each kernel's body to its own four phases.
+template <class T, class V, class I, bool REV>
 __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t s_bar;
@@ -260,7 +263,9 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
     }
     const int2 zt = L.visits[task / L.strips];
     const int z = zt.x, t = zt.y, s = task % L.strips;
-    const int x0 = L.bounds[z * (L.strips + 1) + s], x1 = L.bounds[z * (L.strips + 1) + s + 1];
+    // stored slice of a logical slice (the mirrored sweep reads the forward layout)
+    auto phys = [&](int zz) { return REV ? L.n - zz : zz; };
+    const int x0 = L.bounds[phys(z) * (L.strips + 1) + s], x1 = L.bounds[phys(z) * (L.strips + 1) + s + 1];
     // All range lookups in one round: 24 footprint bounds, 8 update bounds, 8 own bounds.
     if (threadIdx.x < 40) {
       int i = threadIdx.x;
@@ -269,16 +274,16 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
         int v = 0;
         if (zz >= 0 && zz <= L.n) {
           int X = (i & 1) ? min(x1 + 4, L.n + 1) : max(x0 - 4, 0);
-          v = L.xstart[int64_t(zz * 4 + c) * nx + X];
+          v = L.xstart[int64_t(phys(zz) * 4 + c) * nx + X];
         }
         if (i & 1)
           s_hi[r] = v;
         else
           s_lo[r] = v;
       } else {
-        int k = i - 24, c = (k >> 1) & 3, own = k >= 8, h = own ? 0 : (L.rev ? c : 3 - c);
+        int k = i - 24, c = (k >> 1) & 3, own = k >= 8, h = own ? 0 : (REV ? c : 3 - c);
         int X = (k & 1) ? min(x1 + h, L.n + 1) : max(min(x0 - h, L.n + 1), 0);
-        int v = L.xstart[int64_t(z * 4 + c) * nx + X];
+        int v = L.xstart[int64_t(phys(z) * 4 + c) * nx + X];
         if (own) {
           if (k & 1)
             s_o1[c] = v;
@@ -299,7 +304,7 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
         s_base[r] = total;
         total += s_hi[r] - s_lo[r];
         int j = r >> 2, c = r & 3, zz = z + j - 1;
-        int gstart = (zz >= 0 && zz <= L.n) ? L.group_off[zz * 4 + c] : 0;
+        int gstart = (zz >= 0 && zz <= L.n) ? L.group_off[phys(zz) * 4 + c] : 0;
         s_delta[r] = s_base[r] + gstart - s_lo[r];
       }
       s_base[12] = total;
@@ -392,14 +397,14 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
     if (tr) tr[4] = globaltimer();
     {
       V* hv = L.hist ? reinterpret_cast<V*>(L.hist) + t : nullptr;
-#define PSR_PHASE(C)                                                                                             \
-  phase<C, T, V, I>(L, staged, s_p0[C], s_p1[C], s_rbase[C], s_bshift[C], s_idx, s_vals, s_b, foot, s_delta,   \
-                    unsigned(s_total), hv, s_o0[C], s_o1[C]);                                                  \
+#define PSR_PHASE(C, M)                                                                                          \
+  phase<C, M, T, V, I>(L, staged, s_p0[C], s_p1[C], s_rbase[C], s_bshift[C], s_idx, s_vals, s_b, foot, s_delta, \
+                       unsigned(s_total), hv, s_o0[C], s_o1[C]);                                               \
   __syncthreads();
-      if (!L.rev) {
-        PSR_PHASE(0) PSR_PHASE(1) PSR_PHASE(2) PSR_PHASE(3)
+      if (!REV) {
+        PSR_PHASE(0, false) PSR_PHASE(1, false) PSR_PHASE(2, false) PSR_PHASE(3, false)
       } else {
-        PSR_PHASE(3) PSR_PHASE(2) PSR_PHASE(1) PSR_PHASE(0)
+        PSR_PHASE(3, true) PSR_PHASE(2, true) PSR_PHASE(1, true) PSR_PHASE(0, true)
       }
 #undef PSR_PHASE
     }
@@ -680,7 +685,6 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
   L.rows = rows;
   L.iters = iters;
   L.record_increment = record_increment ? 1 : 0;
-  L.rev = rev ? 1 : 0;
   // Shared memory: the footprint, plus the staged rows of tasks that fit.
   const int64_t budget = std::min<int64_t>(device_smem_optin() - 4096, 220 * 1024);
   const int64_t fp_bytes = (int64_t(std::max(maxfp, 1)) * int64_t(sizeof(V)) + 15) & ~int64_t(15);
@@ -694,7 +698,7 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
   int64_t smem = fp_bytes + rc * (kSlotsR * int64_t(sizeof(T)) + kIdxSlots * int64_t(sizeof(I))) +
                  ((int64_t(L.b_cap) * int64_t(sizeof(V)) + 15) & ~int64_t(15));
   smem = std::max<int64_t>(smem, 16);
-  auto kernel = strip_gs_kernel<T, V, I>;
+  auto kernel = rev ? strip_gs_kernel<T, V, I, true> : strip_gs_kernel<T, V, I, false>;
   PSR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   const int64_t total_tasks = int64_t(visits.size()) * strips;
   const int grid = int(std::min<int64_t>(total_tasks, sms));

@@ -56,66 +56,31 @@ __device__ __forceinline__ T hat3_grad(const T p[3], const int c[3], int depth, 
 __device__ __forceinline__ int sched_group(const int c[3]) { return 4 * c[2] + (c[0] & 1) + 2 * (c[1] & 1); }
 
 // ------------------------------------------------------------------ mirrored, transposed operator
-// Mirrored schedule straight from the forward one: group (z, c) becomes group (2^d - z, c)
-// and keeps its rows and their order, so no sort is needed.
-__global__ void mirror_offsets_kernel(const int32_t* off, int groups, int nz, int32_t* off2) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  int32_t acc = 0;
-  for (int g2 = 0; g2 < groups; ++g2) {
-    off2[g2] = acc;
-    const int g = 4 * (nz - g2 / 4) + g2 % 4;
-    acc += off[g + 1] - off[g];
-  }
-  off2[groups] = acc;
-}
-
-__global__ void mirror_positions_kernel(const int32_t* perm, const int32_t* off, const int64_t* skeys,
-                                        const int32_t* off2, int64_t n, int depth, int32_t* perm2, int32_t* inv2,
-                                        int64_t* skeys2) {
+// Transposed operator in the forward schedule layout: slot k of row p holds A_{nbr, row}, the
+// neighbour's entry at the opposite offset (slot 26 - k); the index rows are the forward's.
+template <class S, class I>
+__global__ void transpose_values_kernel(int64_t n, const int64_t* skeys, const int32_t* off, const S* svals,
+                                        const I* sidx, S* tvals) {
   int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (p >= n) return;
   int c[3];
   key_coords(skeys[p], c);
-  const int nz = 1 << depth;
-  const int g = 4 * c[2] + (c[0] & 1) + 2 * (c[1] & 1);
-  const int g2 = 4 * (nz - c[2]) + (c[0] & 1) + 2 * (c[1] & 1);
-  const int64_t p2 = off2[g2] + (p - off[g]);
-  perm2[p2] = perm[p];
-  inv2[perm[p]] = int32_t(p2);
-  skeys2[p2] = basis_key(depth, c[0], c[1], nz - c[2]);
-}
-
-// Row p2 of the mirrored schedule: slot k2 (mirrored dz) holds A_{nbr, row} of the forward
-// operator (the neighbour's entry pointing back at the row); neighbour indices inside their
-// group are unchanged because whole (slice, colour) groups move together.
-template <class S, class I>
-__global__ void mirror_operator_kernel(int64_t n, int depth, const int32_t* perm2, const int32_t* orig_of,
-                                       const int32_t* inv, const int32_t* off, const int32_t* off2,
-                                       const int64_t* skeys2, const S* svals, const I* sidx, S* tvals, I* tidx) {
-  int64_t p2 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (p2 >= n) return;
-  const int64_t i = orig_of ? orig_of[perm2[p2]] : perm2[p2];
-  const int64_t p = inv[i];
-  int m[3];
-  key_coords(skeys2[p2], m);
-  const int nz = 1 << depth;
-  const int c[3] = {m[0], m[1], nz - m[2]};  // forward coordinates
   const I* row = sidx + p * kIdxSlots;
-  for (int k2 = 0; k2 < 27; ++k2) {
-    const int k = (k2 / 3) * 3 + (2 - k2 % 3);
+  __align__(16) S v[kSlots];
+  for (int k = 0; k < 27; ++k) {
     const I idx = row[k];
-    S v = S(0);
+    S a = S(0);
     if (idx >= 0) {
       int q[3] = {c[0] + k / 9 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k % 3 - 1};
       const int64_t pn = off[sched_group(q)] + int64_t(idx);
-      v = svals[pn * kSlots + (26 - k)];
+      a = svals[pn * kSlots + (26 - k)];
     }
-    tvals[p2 * kSlots + k2] = v;
-    tidx[p2 * kIdxSlots + k2] = idx;
+    v[k] = a;
   }
-  tvals[p2 * kSlots + 27] = S(0);
-  tidx[p2 * kIdxSlots + 27] = I(p2 - off2[sched_group(m)]);
-  for (int k = 28; k < kIdxSlots; ++k) tidx[p2 * kIdxSlots + k] = row[k];  // 1 / A_ii: same diagonal
+  v[27] = S(0);
+  int4* dst = reinterpret_cast<int4*>(tvals + p * kSlots);
+  const int4* src = reinterpret_cast<const int4*>(v);
+  for (int q = 0; q < kSlots * int(sizeof(S)) / 16; ++q) dst[q] = src[q];
 }
 
 template <class T>
@@ -1046,39 +1011,26 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
     DBuf<T> seed(n, s);
     axpy_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(g_coef + level_offsets[d], g_cum[d].p, n, seed.p);
     PSR_LAUNCH_CHECK();
-    // mirrored schedule (its "key order" is the forward key order: perm2 maps to forward rows)
-    const int nz = 1 << d, groups = 4 * (nz + 1);
-    StripSchedule S2;
-    S2.rows = n;
-    S2.depth = d;
-    S2.wide = st.sched.wide;
-    S2.perm.alloc(n, s);
-    S2.inv.alloc(n, s);
-    S2.off.alloc(groups + 1, s);
-    S2.skeys.alloc(n, s);
-    mirror_offsets_kernel<<<1, 32, 0, s>>>(st.sched.off.p, groups, nz, S2.off.p);
-    PSR_LAUNCH_CHECK();
-    mirror_positions_kernel<<<blocks_for(n), kThreads, 0, s>>>(st.sched.perm.p, st.sched.off.p, st.sched.skeys.p,
-                                                               S2.off.p, n, d, S2.perm.p, S2.inv.p, S2.skeys.p);
-    PSR_LAUNCH_CHECK();
-    const int32_t* inv2 = S2.inv.p;
+    // The reverse sweep runs on the forward schedule in mirrored slice order over the
+    // transposed operator; its increments are recorded at the forward positions.
     DBuf<T> b2(n + 4, s), M(n, s), mu(int64_t(p.iters) * n, s);
     b2.zero();
     M.zero();
-    gather_seed_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(S2.perm.p, nullptr, n, seed.p, b2.p);
+    gather_seed_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(st.sched.perm.p, nullptr, n, seed.p, b2.p);
     PSR_LAUNCH_CHECK();
+    const int32_t* inv2 = st.sched.inv.p;
     mark(kBwMirror);
     auto reverse_sweep = [&](auto s_tag, auto i_tag) {
       using S = decltype(s_tag);
       using I = decltype(i_tag);
       DBuf<S> tv(kSlots * n, s);
-      DBuf<I> ti(kIdxSlots * n, s);
-      mirror_operator_kernel<S, I><<<blocks_for(n), kThreads, 0, s>>>(
-          n, d, S2.perm.p, nullptr, st.sched.inv.p, st.sched.off.p, S2.off.p, S2.skeys.p,
-          reinterpret_cast<const S*>(st.svals.p), reinterpret_cast<const I*>(st.sidx.p), tv.p, ti.p);
+      transpose_values_kernel<S, I><<<blocks_for(n), kThreads, 0, s>>>(n, st.sched.skeys.p, st.sched.off.p,
+                                                                       reinterpret_cast<const S*>(st.svals.p),
+                                                                       reinterpret_cast<const I*>(st.sidx.p), tv.p);
       PSR_LAUNCH_CHECK();
       mark(kBwMirror);
-      relax_strips_scheduled<S, T, I>(S2, tv.p, ti.p, b2.p, M.p, p.iters, s, nullptr, mu.p, true, true);
+      relax_strips_scheduled<S, T, I>(st.sched, tv.p, reinterpret_cast<const I*>(st.sidx.p), b2.p, M.p, p.iters, s,
+                                      nullptr, mu.p, true, true);
       mark(kBwSweep);
     };
     if (tp.mixed) {
