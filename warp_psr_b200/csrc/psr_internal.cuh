@@ -175,6 +175,13 @@ void relax_sliced_ell(const int32_t* cols, const T* vals, const V* b, V* x, cons
 
 // Index rows of the schedule-order operator: 32 slots (0..26 neighbours, 27 own index); the
 // padding slots 28..31 carry 1 / A_ii in the vector precision (write_inv_diag).
+// An absent neighbour in those index rows is the most negative index: its footprint position
+// (index + a non-negative offset below 2^15 for 16-bit rows, below 2^31 for 32-bit, taken
+// unsigned) always lies past the footprint's end, where the relaxation keeps a +0 entry.
+template <class I>
+__host__ __device__ constexpr I idx_absent() {
+  return sizeof(I) == 2 ? I(-32768) : I(-2147483647 - 1);
+}
 template <class V, class I>
 __host__ __device__ __forceinline__ void write_inv_diag(I* row, V inv) {
   static_assert(4 * sizeof(I) >= sizeof(V), "index padding too small for the reciprocal");

@@ -433,7 +433,7 @@ __global__ void assemble_sliced_kernel(const int64_t* keys, int64_t n, int d, Co
   __align__(16) I idx[32];
   for (int k = 0; k < 27; ++k) {
     v[k] = S(0);
-    idx[k] = I(-1);
+    idx[k] = idx_absent<I>();
     if (col[k] >= 0) {
       const double* x = table + (c[0] * 3 + k / 9) * 2;
       const double* y = table + (c[1] * 3 + (k / 3) % 3) * 2;
