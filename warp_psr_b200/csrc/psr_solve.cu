@@ -670,38 +670,33 @@ __global__ void __launch_bounds__(512) relax_colors_kernel(const int32_t* cols, 
 }
 
 // The same relaxation with x held in shared memory for the whole call (levels whose x fits):
-// identical arithmetic and order, without a round trip to L2 per neighbour read.
+// identical arithmetic and order, without a round trip to L2 per neighbour read.  Every slot
+// takes part in the sum: an absent slot (column -1, value +0) reads the +0 entry kept at
+// xs_sh[n], and r - (+0 * +0) = r exactly, so the result is bitwise that of skipping it; the
+// rows hold their k-th neighbour in slot k, so the diagonal is slot 13.  The unsigned clamp
+// keeps every read inside the n + 1 entries.
 template <class T>
 __device__ __forceinline__ void gs_row_shared(const int32_t* __restrict__ cols, const T* __restrict__ vals,
-                                              const T* __restrict__ b, T* xs_sh, int32_t row, T* rec) {
+                                              const T* __restrict__ b, T* xs_sh, int32_t row, T* rec, unsigned n) {
   const int4* cr = reinterpret_cast<const int4*>(cols + int64_t(row) * kSlots);
-  int cc[kSlots];
+  __align__(16) int cc[kSlots];
 #pragma unroll
-  for (int q = 0; q < kSlots / 4; ++q) {
-    int4 v = __ldg(cr + q);
-    cc[4 * q] = v.x;
-    cc[4 * q + 1] = v.y;
-    cc[4 * q + 2] = v.z;
-    cc[4 * q + 3] = v.w;
-  }
-  T aa[kSlots];
-  const T* vr = vals + int64_t(row) * kSlots;
+  for (int q = 0; q < kSlots / 4; ++q) reinterpret_cast<int4*>(cc)[q] = __ldg(cr + q);
+  __align__(16) T aa[kSlots];
+  const int4* vr = reinterpret_cast<const int4*>(vals + int64_t(row) * kSlots);
 #pragma unroll
-  for (int q = 0; q < kSlots; ++q) aa[q] = __ldg(vr + q);
+  for (int q = 0; q < kSlots * int(sizeof(T)) / 16; ++q) reinterpret_cast<int4*>(aa)[q] = __ldg(vr + q);
   T xs[27];
 #pragma unroll
-  for (int k = 0; k < 27; ++k) xs[k] = cc[k] >= 0 ? xs_sh[cc[k]] : T(0);
+  for (int k = 0; k < 27; ++k) xs[k] = xs_sh[min(unsigned(cc[k]), n)];
   T r = b[row];
+#pragma unroll
+  for (int k = 0; k < 27; ++k) r = r - xs[k] * T(aa[k]);
   T diagonal = T(0);
   T xi = T(0);
-#pragma unroll
-  for (int k = 0; k < 27; ++k) {
-    if (cc[k] < 0) continue;
-    r = r - xs[k] * T(aa[k]);
-    if (cc[k] == row) {
-      diagonal = aa[k];
-      xi = xs[k];
-    }
+  if (cc[13] == row) {
+    diagonal = aa[13];
+    xi = xs[13];
   }
   if (rec) {
     rec[0] = xi;
@@ -717,12 +712,14 @@ __global__ void __launch_bounds__(512) relax_colors_shared_kernel(const int32_t*
   extern __shared__ __align__(16) unsigned char relax_smem[];
   T* xs = reinterpret_cast<T*>(relax_smem);
   for (int64_t i = threadIdx.x; i < n; i += blockDim.x) xs[i] = x[i];
+  if (threadIdx.x == 0) xs[n] = T(0);  // the entry absent slots read
   __syncthreads();
   for (int it = 0; it < iters; ++it)
     for (int cc = 0; cc < 8; ++cc) {
       int g = forward ? cc : 7 - cc;
       for (int j = group_off[g] + threadIdx.x; j < group_off[g + 1]; j += blockDim.x)
-        gs_row_shared(cols, vals, b, xs, rows[j], hist ? hist + 2 * (int64_t(it) * n + rows[j]) : nullptr);
+        gs_row_shared(cols, vals, b, xs, rows[j], hist ? hist + 2 * (int64_t(it) * n + rows[j]) : nullptr,
+                      unsigned(n));
       __syncthreads();
     }
   for (int64_t i = threadIdx.x; i < n; i += blockDim.x) x[i] = xs[i];
@@ -734,7 +731,7 @@ constexpr size_t kRelaxSharedBytes = 200 * 1024;
 template <class T>
 static void relax_colors(const int32_t* cols, const T* vals, const T* b, T* x, const int32_t* rows,
                          const int32_t* group_off, int iters, int forward, T* hist, int64_t n, cudaStream_t s) {
-  const size_t bytes = size_t(n) * sizeof(T);
+  const size_t bytes = size_t(n + 1) * sizeof(T);  // x and a +0 entry
   if (n > 0 && bytes <= kRelaxSharedBytes) {
     static bool configured = false;
     if (!configured) {
