@@ -143,7 +143,7 @@ __device__ __forceinline__ uint32_t neighbours27(const ColumnView& cv, int d, co
 // ------------------------------------------------------------------ A6 normal loads (normal_stencils.py:210-260)
 // `nvals` are 4-wide normal coefficients indexed by (hash result - noff).
 template <class T>
-__global__ void normal_stencil_kernel(const int64_t* keys, int64_t n, int test_depth, int normal_depth, ColumnView cv,
+__global__ void __launch_bounds__(256, 6) normal_stencil_kernel(const int64_t* keys, int64_t n, int test_depth, int normal_depth, ColumnView cv,
                                       int64_t noff, const T* nvals, const double* table, int width, int first,
                                       double* out) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
@@ -412,7 +412,7 @@ __global__ void assemble_level_kernel(const int64_t* keys, int64_t n, int d, Col
 // indices inside their (slice, colour) group (slot 27 = the row's own index), and
 // b = T(load) + 0.5*T(point load).
 template <class T, class S, class I, bool SCREEN>
-__global__ void assemble_sliced_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t off,
+__global__ void __launch_bounds__(128, 12) assemble_sliced_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t off,
                                        const double* table, PointsView<T> P, const double* load, const int32_t* inv,
                                        const int32_t* group_off, S* svals, I* sidx, T* sb) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
@@ -461,7 +461,7 @@ __global__ void assemble_sliced_kernel(const int64_t* keys, int64_t n, int d, Co
 // applied to the coarser cumulative solution: b = b - C cumulative (solver.py:428-446).
 // With ccols_out / cvals_out (adjoint tape) the row's cross operator is kept (28 slots).
 template <class T, bool SCREEN>
-__global__ void cross_apply_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t coff,
+__global__ void __launch_bounds__(128, 8) cross_apply_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t coff,
                                    const double* table, PointsView<T> P, const T* cumulative, T* b,
                                    const int32_t* inv, int32_t* ccols_out = nullptr, T* cvals_out = nullptr) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;

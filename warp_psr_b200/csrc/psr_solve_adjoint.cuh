@@ -876,7 +876,7 @@ __global__ void points_reverse_kernel(const int64_t* keys, const T* vals, int64_
 // Transpose of normal_stencil_kernel: for each normal coefficient j (at normal_depth) gather
 // sum_i g_i * (x', y', z' integrals) over the test rows i whose window covers j.
 template <class T>
-__global__ void normal_stencil_reverse_kernel(const int64_t* nkeys, int64_t m, int test_depth, int normal_depth,
+__global__ void __launch_bounds__(256, 5) normal_stencil_reverse_kernel(const int64_t* nkeys, int64_t m, int test_depth, int normal_depth,
                                               ColumnView tcv, int64_t toff, const double* g_test, const double* table,
                                               int width, int first, T* g_vals) {
   int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
