@@ -103,8 +103,8 @@ __global__ void normal_table_kernel(int test_depth, int normal_depth, int first,
 }
 
 // Columns of the 27 neighbours q = ctr + (dx, dy, dz) at depth d (slot order), found with
-// one column probe per (dx, dy) and a scan over three consecutive z.
-__device__ __forceinline__ uint32_t neighbours27(const ColumnView& cv, int d, const int ctr[3], int64_t off,
+// one column probe per (dx, dy) and a scan over three consecutive z (any column index).
+__device__ __forceinline__ uint32_t neighbours27_scan(const ColumnView& cv, int d, const int ctr[3], int64_t off,
                                                  int32_t col[27]) {
   const int lim = 1 << d;
   uint32_t present = 0;
@@ -135,6 +135,68 @@ __device__ __forceinline__ uint32_t neighbours27(const ColumnView& cv, int d, co
         present |= 1u << k;
         ++j;
       }
+    }
+  }
+  return present;
+}
+
+// The same with the dense column table (depth <= 12): the nine column ranges are read
+// together and their lower bounds of z = ctr_z - 1 advance in lock step, so each step's nine
+// loads are in flight at once (the row's dependent-load chain is one binary search long, not
+// nine); then the up to three keys after each bound are matched to dz.  Same result.
+__device__ __forceinline__ uint32_t neighbours27(const ColumnView& cv, int d, const int ctr[3], int64_t off,
+                                                 int32_t col[27]) {
+  if (!cv.dense) return neighbours27_scan(cv, d, ctr, off, col);
+  const int lim = 1 << d;
+  const int side = lim + 1;
+  const int z0 = ctr[2] - 1;
+  const int2* dense = cv.dense + dense_column_base(d);
+  int32_t lo[9], hi[9], end[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    const int qx = ctr[0] + c / 3 - 1, qy = ctr[1] + c % 3 - 1;
+    lo[c] = 0;
+    end[c] = 0;
+    if (unsigned(qx) <= unsigned(lim) && unsigned(qy) <= unsigned(lim)) {
+      const int2 e = __ldg(dense + int64_t(qx) * side + qy);
+      if (e.x >= 0) {
+        lo[c] = e.x;
+        end[c] = e.x + e.y;
+      }
+    }
+    hi[c] = end[c];
+  }
+  for (int step = 0; step < 32; ++step) {
+    bool active = false;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) active |= lo[c] < hi[c];
+    if (!active) break;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      if (lo[c] < hi[c]) {
+        const int32_t mid = (lo[c] + hi[c]) >> 1;
+        if (int(__ldg(cv.keys + mid) & 65535) < z0)
+          lo[c] = mid + 1;
+        else
+          hi[c] = mid;
+      }
+    }
+  }
+  uint32_t present = 0;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    constexpr int kNone = -0x40000000;  // below every z0 + dz
+    int zs[3];
+#pragma unroll
+    for (int e = 0; e < 3; ++e) zs[e] = lo[c] + e < end[c] ? int(__ldg(cv.keys + lo[c] + e) & 65535) : kNone;
+#pragma unroll
+    for (int dz = 0; dz < 3; ++dz) {
+      int32_t found = -1;
+#pragma unroll
+      for (int e = 0; e < 3; ++e)
+        if (zs[e] == z0 + dz) found = int32_t(lo[c] + e - off);
+      col[c * 3 + dz] = found;
+      if (found >= 0) present |= 1u << (c * 3 + dz);
     }
   }
   return present;
