@@ -18,17 +18,17 @@ std::atomic<long long> g_kernel_launches{0};
 
 void set_last_error(const std::string& message) { g_error = message; }
 
-__global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, int64_t* keys, int32_t* vals,
-                                   uint64_t mask, int32_t value_offset) {
+__global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, longlong2* slots, uint64_t mask,
+                                   int32_t value_offset) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   int64_t key = src[i];
   uint64_t h = HashView::mix(uint64_t(key)) & mask;
   while (true) {
-    unsigned long long prev = atomicCAS(reinterpret_cast<unsigned long long*>(keys + h), ~0ULL,
+    unsigned long long prev = atomicCAS(reinterpret_cast<unsigned long long*>(&slots[h].x), ~0ULL,
                                         static_cast<unsigned long long>(key));
     if (prev == ~0ULL || prev == static_cast<unsigned long long>(key)) {
-      vals[h] = int32_t(i) + value_offset;
+      slots[h].y = int64_t(int32_t(i) + value_offset);
       return;
     }
     h = (h + 1) & mask;
@@ -36,8 +36,7 @@ __global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, i
 }
 
 // Column heads of sorted keys: (depth, x, y) changes.
-__global__ void column_insert_kernel(const int64_t* __restrict__ keys, int64_t n, int64_t* hkeys, int32_t* hvals,
-                                     uint64_t mask) {
+__global__ void column_insert_kernel(const int64_t* __restrict__ keys, int64_t n, longlong2* slots, uint64_t mask) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   int64_t k = keys[i];
@@ -45,10 +44,10 @@ __global__ void column_insert_kernel(const int64_t* __restrict__ keys, int64_t n
   int64_t key = (k >> 16) << 16;
   uint64_t h = HashView::mix(uint64_t(key)) & mask;
   while (true) {
-    unsigned long long prev = atomicCAS(reinterpret_cast<unsigned long long*>(hkeys + h), ~0ULL,
+    unsigned long long prev = atomicCAS(reinterpret_cast<unsigned long long*>(&slots[h].x), ~0ULL,
                                         static_cast<unsigned long long>(key));
     if (prev == ~0ULL || prev == static_cast<unsigned long long>(key)) {
-      hvals[h] = int32_t(i);
+      slots[h].y = int64_t(i);
       return;
     }
     h = (h + 1) & mask;

@@ -150,17 +150,18 @@ __host__ __device__ __forceinline__ void tree_coords(int64_t k, int c[3]) {
 // Open addressing with linear probing over a power-of-two table at most half full.  A
 // lookup returns exactly the index the reference's binary search over the sorted key
 // array returns (or -1), so it can replace find_key anywhere.
+// Open-addressing table of 16-byte slots {key, value} (key -1 = empty): a probe is one
+// 16-byte load that brings the value with the key.
 struct HashView {
-  const int64_t* keys = nullptr;
-  const int32_t* vals = nullptr;
+  const longlong2* slots = nullptr;
   uint64_t mask = 0;
   __device__ __forceinline__ int32_t find(int64_t key) const {
-    if (!keys) return -1;
+    if (!slots) return -1;
     uint64_t h = mix(uint64_t(key)) & mask;
     while (true) {
-      int64_t k = __ldg(keys + h);
-      if (k == key) return __ldg(vals + h);
-      if (k == -1) return -1;
+      const longlong2 e = __ldg(slots + h);
+      if (e.x == key) return int32_t(e.y);
+      if (e.x == -1) return -1;
       h = (h + 1) & mask;
     }
   }
@@ -174,12 +175,11 @@ struct HashView {
   }
 };
 
-__global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, int64_t* keys, int32_t* vals,
-                                   uint64_t mask, int32_t value_offset);
+__global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, longlong2* slots, uint64_t mask,
+                                   int32_t value_offset);
 
 struct HashMap {
-  DBuf<int64_t> keys;
-  DBuf<int32_t> vals;
+  DBuf<longlong2> slots;
   uint64_t mask = 0;
   int64_t count = 0;
   // Build from n unique keys; key i maps to value_offset + i.
@@ -188,19 +188,17 @@ struct HashMap {
     uint64_t cap = 16;
     while (cap < uint64_t(2 * n + 1)) cap <<= 1;
     mask = cap - 1;
-    keys.alloc(int64_t(cap), s);
-    vals.alloc(int64_t(cap), s);
-    PSR_CUDA(cudaMemsetAsync(keys.p, 0xff, cap * sizeof(int64_t), s));
+    slots.alloc(int64_t(cap), s);
+    PSR_CUDA(cudaMemsetAsync(slots.p, 0xff, cap * sizeof(longlong2), s));
     if (n > 0) {
-      hash_insert_kernel<<<blocks_for(n), kThreads, 0, s>>>(src, n, keys.p, vals.p, mask, value_offset);
+      hash_insert_kernel<<<blocks_for(n), kThreads, 0, s>>>(src, n, slots.p, mask, value_offset);
       PSR_LAUNCH_CHECK();
     }
   }
   HashView view() const {
     HashView v;
     if (count > 0) {
-      v.keys = keys.p;
-      v.vals = vals.p;
+      v.slots = slots.p;
       v.mask = mask;
     }
     return v;
@@ -279,8 +277,7 @@ struct ColumnView {
   }
 };
 
-__global__ void column_insert_kernel(const int64_t* __restrict__ keys, int64_t n, int64_t* hkeys, int32_t* hvals,
-                                     uint64_t mask);
+__global__ void column_insert_kernel(const int64_t* __restrict__ keys, int64_t n, longlong2* slots, uint64_t mask);
 __global__ void dense_column_kernel(const int64_t* __restrict__ keys, int64_t n, int2* dense, int32_t* error);
 __global__ void dense_count_kernel(const int64_t* __restrict__ keys, int64_t n, int2* dense);
 
@@ -310,11 +307,10 @@ struct ColumnIndex {
       uint64_t cap = 16;
       while (cap < uint64_t(2 * n + 1)) cap <<= 1;
       map.mask = cap - 1;
-      map.keys.alloc(int64_t(cap), s);
-      map.vals.alloc(int64_t(cap), s);
-      PSR_CUDA(cudaMemsetAsync(map.keys.p, 0xff, cap * sizeof(int64_t), s));
+      map.slots.alloc(int64_t(cap), s);
+      PSR_CUDA(cudaMemsetAsync(map.slots.p, 0xff, cap * sizeof(longlong2), s));
       if (n > 0) {
-        column_insert_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, map.keys.p, map.vals.p, map.mask);
+        column_insert_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, map.slots.p, map.mask);
         PSR_LAUNCH_CHECK();
       }
       view_.h = map.view();

@@ -357,10 +357,23 @@ __global__ void bin_fill_kernel(const uint64_t* keys, const int32_t* heads, cons
   bstart[u] = int32_t(i);
 }
 
+// Point positions and weights gathered into bin order, so the points of a bin are read
+// without the id indirection.
+template <class T>
+__global__ void bin_order_points_kernel(const int32_t* ids, int64_t m, const T* pos, const T* w, T* spos, T* sw) {
+  int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (j >= m) return;
+  const int64_t i = ids[j];
+  for (int a = 0; a < 3; ++a) spos[3 * j + a] = pos[3 * i + a];
+  sw[j] = w[i];
+}
+
 template <class T>
 struct PointsView {
   const T* pos = nullptr;
   const T* w = nullptr;
+  const T* spos = nullptr;          // pos and w in bin order (spos[3j + a] = pos[3 ids[j] + a])
+  const T* sw = nullptr;
   const int32_t* ids = nullptr;     // point ids sorted by bin (stable)
   const int32_t* bstart = nullptr;  // per unique bin, start into ids; count+1 entries
   HashView bins;                    // basis key of a bin cell -> unique bin index
@@ -369,7 +382,7 @@ struct PointsView {
 template <class T>
 struct PointsData {
   int64_t m = 0, nbins = 0;
-  DBuf<T> pos, w;
+  DBuf<T> pos, w, spos, sw;
   DBuf<int32_t> ids, bstart;
   DBuf<int64_t> bkeys;
   HashMap bins;
@@ -377,6 +390,8 @@ struct PointsData {
     PointsView<T> v;
     v.pos = pos.p;
     v.w = w.p;
+    v.spos = spos.p;
+    v.sw = sw.p;
     v.ids = ids.p;
     v.bstart = bstart.p;
     v.bins = bins.view();
@@ -410,9 +425,8 @@ __device__ __forceinline__ double screening_row(const PointsView<T>& P, const in
     int32_t u = P.bins.find(basis_key(d, cell[0], cell[1], cell[2]));
     if (u < 0) continue;
     for (int32_t j = P.bstart[u]; j < P.bstart[u + 1]; ++j) {
-      int32_t index = P.ids[j];
-      T p[3] = {P.pos[3 * index], P.pos[3 * index + 1], P.pos[3 * index + 2]};
-      T weight = P.w[index];
+      T p[3] = {P.spos[3 * j], P.spos[3 * j + 1], P.spos[3 * j + 2]};
+      T weight = P.sw[j];
       if (weight == T(0)) continue;
       T phi = hat3(p, c, d);
       rhs += double(phi * weight);
@@ -1145,6 +1159,12 @@ static PointsData<T> make_points(const DensityData<T>& D, const NormalData<T>& N
     PSR_LAUNCH_CHECK();
     int Db = d > 0 ? d : 1;
     sort_pairs(bk.p, sbk.p, ids.p, P.ids.p, m, 3 * Db, s);
+  }
+  P.spos.alloc(3 * m, s);
+  P.sw.alloc(m, s);
+  if (m) {
+    bin_order_points_kernel<T><<<blocks_for(m), kThreads, 0, s>>>(P.ids.p, m, P.pos.p, P.w.p, P.spos.p, P.sw.p);
+    PSR_LAUNCH_CHECK();
   }
   DBuf<int32_t> heads(m, s), prefix(m, s);
   int64_t u = 0;

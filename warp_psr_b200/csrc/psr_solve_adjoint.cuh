@@ -252,9 +252,8 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
     int32_t u = L.P.bins.find(basis_key(L.d, cell[0], cell[1], cell[2]));
     if (u < 0) continue;
     for (int32_t j = L.P.bstart[u]; j < L.P.bstart[u + 1]; ++j) {
-      const int32_t index = L.P.ids[j];
-      const T p[3] = {L.P.pos[3 * index], L.P.pos[3 * index + 1], L.P.pos[3 * index + 2]};
-      const T w = L.P.w[index];
+      const T p[3] = {L.P.spos[3 * j], L.P.spos[3 * j + 1], L.P.spos[3 * j + 2]};
+      const T w = L.P.sw[j];
       if (w == T(0)) continue;
       T dphi[3];
       const T phi = hat3_grad(p, c, L.d, dphi);
@@ -289,6 +288,7 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
           for (int a = 0; a < 3; ++a) gp[a] = gp[a] + (gwp * tr) * dphi[a] + (gwp * phi) * dtr[a];
         }
       }
+      const int32_t index = L.P.ids[j];
       for (int a = 0; a < 3; ++a)
         if (gp[a] != T(0)) atomicAdd(L.g_pos + 3 * index + a, gp[a]);
       if (gw != T(0)) atomicAdd(L.g_w + index, gw);
