@@ -251,6 +251,83 @@ __global__ void __launch_bounds__(256, 6) normal_stencil_kernel(const int64_t* k
   out[i] = value;
 }
 
+// The same with the dense column table and a compile-time window W: for each x the W
+// columns' ranges are read together and their lower bounds of z0 advance in lock step, and
+// the up to W keys after each bound (increasing z, so in the z-loop's order) are loaded
+// together.  The additions run in the same (x, y, z) order: same result.
+template <class T, int W>
+__global__ void __launch_bounds__(256, 4) normal_stencil_dense_kernel(const int64_t* keys, int64_t n, int test_depth,
+                                                                      int normal_depth, ColumnView cv, int64_t noff,
+                                                                      const T* nvals, const double* table, int first,
+                                                                      double* out) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int c[3];
+  key_coords(keys[i], c);
+  const int ctr[3] = {normal_center(c[0], test_depth, normal_depth), normal_center(c[1], test_depth, normal_depth),
+                      normal_center(c[2], test_depth, normal_depth)};
+  const int lim = 1 << normal_depth;
+  const int side = lim + 1;
+  const int z0 = ctr[2] + first;
+  const int2* dense = cv.dense + dense_column_base(normal_depth);
+  double value = 0.0;
+  for (int x = 0; x < W; ++x) {
+    const int nx = ctr[0] + x + first;
+    if (nx < 0 || nx >= lim) continue;
+    const double* ix = table + (c[0] * W + x) * 2;
+    int32_t lo[W], hi[W], end[W];
+#pragma unroll
+    for (int y = 0; y < W; ++y) {
+      const int ny = ctr[1] + y + first;
+      lo[y] = 0;
+      end[y] = 0;
+      if (ny >= 0 && ny < lim) {
+        const int2 e = __ldg(dense + int64_t(nx) * side + ny);
+        if (e.x >= 0) {
+          lo[y] = e.x;
+          end[y] = e.x + e.y;
+        }
+      }
+      hi[y] = end[y];
+    }
+    for (int step = 0; step < 32; ++step) {
+      bool active = false;
+#pragma unroll
+      for (int y = 0; y < W; ++y) active |= lo[y] < hi[y];
+      if (!active) break;
+#pragma unroll
+      for (int y = 0; y < W; ++y) {
+        if (lo[y] < hi[y]) {
+          const int32_t mid = (lo[y] + hi[y]) >> 1;
+          if (int(__ldg(cv.keys + mid) & 65535) < z0)
+            lo[y] = mid + 1;
+          else
+            hi[y] = mid;
+        }
+      }
+    }
+#pragma unroll
+    for (int y = 0; y < W; ++y) {
+      const double* iy = table + (c[1] * W + y) * 2;
+      int dz[W];
+#pragma unroll
+      for (int e = 0; e < W; ++e)
+        dz[e] = lo[y] + e < end[y] ? int(__ldg(cv.keys + lo[y] + e) & 65535) - z0 : W;
+#pragma unroll
+      for (int e = 0; e < W; ++e) {
+        if (dz[e] >= W) break;  // past the window (z ascending)
+        if (z0 + dz[e] >= lim) continue;
+        const double* iz = table + (c[2] * W + dz[e]) * 2;
+        const T* v = nvals + 4 * (int64_t(lo[y] + e) - noff);
+        value += double(v[0]) * ix[1] * iy[0] * iz[0];
+        value += double(v[1]) * ix[0] * iy[1] * iz[0];
+        value += double(v[2]) * ix[0] * iy[0] * iz[1];
+      }
+    }
+  }
+  out[i] = value;
+}
+
 // normal_loads.py:27-63 — degree-1 prolongation of normal coefficients (issue #35).
 template <class T>
 __global__ void prolong_normals_kernel(const int64_t* keys, int64_t n, int d, HashView nh, const T* nvals,
@@ -1228,8 +1305,15 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
     DBuf<double> table(int64_t(res + 1) * width * 2, s);
     normal_table_kernel<<<blocks_for(res + 1), kThreads, 0, s>>>(test_d, normal_d, first, width, table.p);
     PSR_LAUNCH_CHECK();
-    normal_stencil_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(keys_at(test_d), n, test_d, normal_d, h, noff, nvals,
-                                                                table.p, width, first, out.p);
+    if (h.dense && width == 4)
+      normal_stencil_dense_kernel<T, 4><<<blocks_for(n), kThreads, 0, s>>>(keys_at(test_d), n, test_d, normal_d, h,
+                                                                          noff, nvals, table.p, first, out.p);
+    else if (h.dense && width == 6)
+      normal_stencil_dense_kernel<T, 6><<<blocks_for(n), kThreads, 0, s>>>(keys_at(test_d), n, test_d, normal_d, h,
+                                                                          noff, nvals, table.p, first, out.p);
+    else
+      normal_stencil_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(keys_at(test_d), n, test_d, normal_d, h, noff,
+                                                                  nvals, table.p, width, first, out.p);
     PSR_LAUNCH_CHECK();
   };
   DBuf<T> prev;
