@@ -351,9 +351,9 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
         }
       }
       if (tr) tr[1] = globaltimer();
+      // slice z after visit t-1 (two waves back); the newer dependencies are awaited below
+      // while this slice is staged
       bool ok = !s_fail;
-      if (ok && z + 1 <= L.n) ok = wait_at_least(L.done + (z + 1) * kPad, (t + 1) * L.strips, L.error);
-      if (ok && z > 0) ok = wait_at_least(L.done + (z - 1) * kPad, t * L.strips, L.error);
       if (ok) ok = wait_at_least(L.done + z * kPad, t * L.strips, L.error);
       if (!ok) {
         atomicCAS(L.error, 0, 1);
@@ -368,12 +368,13 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
       return;
     }
     if (tr) tr[3] = globaltimer();
-    // Stage the footprint: slice z+1 after visit t, slices z and z-1 after visit t-1.
+    // Stage the footprint: slice z+1 after visit t, slices z and z-1 after visit t-1.  Warp 0
+    // waits for slices z+1 and z-1 while the other warps stage slice z, then all stage the rest.
     {
       const V* cur = (t & 1) ? xb1 : xb0;
       const V* prev = (t & 1) ? xb0 : xb1;
       const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-      for (int r = warp; r < 12; r += nwarps) {
+      auto stage_range = [&](int r) {
         const V* src = ((r >> 2) == 2 ? cur : prev) + s_lo[r];
         V* dst = foot + s_base[r];
         const int cnt = s_hi[r] - s_lo[r];
@@ -386,7 +387,27 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
           for (int u = 0; u < 4; ++u)
             if (i0 + 32 * u < cnt) dst[i0 + 32 * u] = v[u];
         }
+      };
+      if (warp == 0) {
+        if (lane == 0) {
+          bool ok = true;
+          if (z + 1 <= L.n) ok = wait_at_least(L.done + (z + 1) * kPad, (t + 1) * L.strips, L.error);
+          if (ok && z > 0) ok = wait_at_least(L.done + (z - 1) * kPad, t * L.strips, L.error);
+          if (!ok) {
+            atomicCAS(L.error, 0, 1);
+            s_fail = 1;
+          }
+        }
+        __syncwarp();
+      } else {
+        for (int r = 4 + warp - 1; r < 8; r += nwarps - 1) stage_range(r);
       }
+      __syncthreads();
+      if (s_fail) {
+        if (staged) mbar_wait(&s_bar, parity);
+        return;
+      }
+      for (int q = warp; q < 8; q += nwarps) stage_range(q < 4 ? q : q + 4);
     }
     if (threadIdx.x == 0) foot[s_total] = V(0);  // the entry absent slots read
     if (staged && !mbar_wait(&s_bar, parity)) {
