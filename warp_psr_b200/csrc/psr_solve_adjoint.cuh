@@ -300,9 +300,8 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
 // per-slot quantity stays in registers: the operator adjoint of the row (written to row_gA,
 // 27 per row, for the per-point screening pass) and -C^T g_b into the coarser cumulative.
 template <class T, class I, int ITERS>
-__global__ void __launch_bounds__(128) level_rows_reverse_kernel(const int64_t* __restrict__ keys, int64_t n,
-                                                                 const int32_t* __restrict__ inv,
-                                                                 const int32_t* __restrict__ inv2,
+__global__ void __launch_bounds__(128) level_rows_reverse_kernel(const int64_t* __restrict__ skeys, int64_t n,
+                                                                 const int32_t* __restrict__ perm,
                                                                  const int32_t* __restrict__ off,
                                                                  const I* __restrict__ sidx,
                                                                  const T* __restrict__ xhist,
@@ -311,11 +310,13 @@ __global__ void __launch_bounds__(128) level_rows_reverse_kernel(const int64_t* 
                                                                  const int32_t* __restrict__ ccols,
                                                                  const T* __restrict__ cvals, T* g_cum_prev,
                                                                  T* row_gA) {
-  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i >= n) return;
+  // one thread per schedule position: consecutive threads are neighbours in one (slice,
+  // colour) group, so their neighbours' visit records are read together
+  const int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (p >= n) return;
   int c[3];
-  key_coords(keys[i], c);
-  const int64_t p = inv[i], p2 = inv2[i];
+  key_coords(skeys[p], c);
+  const int64_t i = perm[p];
   const int own = (c[0] & 1) + 2 * (c[1] & 1);
   __align__(16) I row[kIdxSlots];
   {
@@ -326,7 +327,7 @@ __global__ void __launch_bounds__(128) level_rows_reverse_kernel(const int64_t* 
   }
   T mu[ITERS];
 #pragma unroll
-  for (int u = 0; u < ITERS; ++u) mu[u] = __ldg(mu_hist + p2 * ITERS + u);  // mirrored visit u
+  for (int u = 0; u < ITERS; ++u) mu[u] = __ldg(mu_hist + p * ITERS + u);  // reverse visit u
   T* out = row_gA ? row_gA + i * 27 : nullptr;
 #pragma unroll
   for (int k = 0; k < 27; ++k) {
@@ -1085,8 +1086,8 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
       }
       if (p.iters == 8 && L.ccols) {
         level_rows_reverse_kernel<T, I, 8><<<blocks_for(n, 128), 128, 0, s>>>(
-            L.keys, n, L.inv, L.inv2, L.off, L.sidx, L.xhist, L.mu, L.g_b, L.ccols, L.cvals, L.g_cum_prev,
-            tp.screened ? rA.p : nullptr);
+            st.sched.skeys.p, n, st.sched.perm.p, L.off, L.sidx, L.xhist, L.mu, L.g_b, L.ccols, L.cvals,
+            L.g_cum_prev, tp.screened ? rA.p : nullptr);
       } else {
         level_reverse_kernel<T, S, I, true, 0><<<blocks_for(n, 128), 128, 0, s>>>(L);
       }
