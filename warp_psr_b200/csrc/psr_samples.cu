@@ -518,14 +518,15 @@ __global__ void first_keys_kernel(const int32_t* first, int64_t n, uint32_t* key
 template <class T>
 __global__ void normal_splat_kernel(const int32_t* order, int64_t n, const T* sums, const T* nsums, const T* weights,
                                     const T* dw, int minimum, int maximum, uint64_t* rkeys, int32_t* rids, T* rvals) {
-  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i >= n) return;
+  // one thread per record (54 per sample): neighbouring threads write neighbouring records
+  const int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (r >= 54 * n) return;
+  const int64_t i = r / 54;
+  const int k = int(r % 54);
   int D = maximum > 0 ? maximum : 1;
   uint64_t sentinel = uint64_t(1) << (3 * D + 4);
-  for (int k = 0; k < 54; ++k) {
-    rkeys[54 * i + k] = sentinel;
-    rids[54 * i + k] = int32_t(54 * i + k);
-  }
+  rkeys[r] = sentinel;
+  rids[r] = int32_t(r);
   int64_t src = order[i];
   T w = weights[src];
   T nm[3] = {nsums[3 * src] / w, nsums[3 * src + 1] / w, nsums[3 * src + 2] / w};
@@ -551,15 +552,15 @@ __global__ void normal_splat_kernel(const int32_t* order, int64_t n, const T* su
   for (int a = 0; a < 3; ++a) quadratic(double((p[a] - T(c[a]) * h) / h), b[a]);
   bool second = fabs(1.0 - double(dx)) > 1e-06;
   T sw = dw[2 * src + 1];
-  for (int k = 0; k < 54; ++k) {
-    if (k >= 27 && !second) break;
+  {
+    if (k >= 27 && !second) return;
     T fraction = k < 27 ? dx : T(1.0) - dx;
     int q = k % 27;
     int x = q / 9, y = q / 3 % 3, z = q % 3;
     int t[3] = {c[0] + x - 1, c[1] + y - 1, c[2] + z - 1};
     if (dmin(t[0], dmin(t[1], t[2])) >= 0 && dmax(t[0], dmax(t[1], t[2])) < nn) {
       T bw = T(b[0][x] * b[1][y] * b[2][z]);
-      int64_t dst = 54 * i + k;
+      const int64_t dst = r;
       rkeys[dst] = (uint64_t(top) << (3 * D)) | (uint64_t(t[0]) << (2 * D)) | (uint64_t(t[1]) << D) | uint64_t(t[2]);
       for (int a = 0; a < 3; ++a) rvals[3 * dst + a] = nm[a] * sw / (h * h * h) * fraction * bw;
     }
@@ -665,7 +666,7 @@ NormalData<T> build_normals(const SampleGroups<T>& g, const DensityData<T>& D, i
     DBuf<uint64_t> rkeys(r, s), skeys(r, s);
     DBuf<int32_t> rids(r, s), rorder(r, s);
     DBuf<T> rvals(3 * r, s);
-    normal_splat_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(order.p, n, g.sums.p, g.normal_sums.p, g.weights.p,
+    normal_splat_kernel<T><<<blocks_for(54 * n), kThreads, 0, s>>>(order.p, n, g.sums.p, g.normal_sums.p, g.weights.p,
                                                               D.dw.p, minimum, maximum, rkeys.p, rids.p, rvals.p);
     PSR_LAUNCH_CHECK();
     sort_pairs(rkeys.p, skeys.p, rids.p, rorder.p, r, 3 * Db + 5, s);
