@@ -492,16 +492,26 @@ __device__ __forceinline__ T hat3(const T p[3], const int c[3], int depth) {  //
 // hat; every other slot would receive exactly +0.0, so skipping them leaves each
 // accumulator's sequence of nonzero additions, and hence its value, unchanged.
 template <class T>
+// `rin` (optional): the eight cells' point ranges found by an earlier pass over the same row
+// (the sliced assembly hands them to the cross term); `rout` (optional) receives them.
 __device__ __forceinline__ double screening_row(const PointsView<T>& P, const int c[3], int d, int trial_depth,
-                                                const int q0[3], uint32_t present, double acc[27]) {
+                                                const int q0[3], uint32_t present, double acc[27],
+                                                const int2* rin = nullptr, int2* rout = nullptr) {
   double rhs = 0.0;
   const int nt = 1 << trial_depth;
   for (int k8 = 0; k8 < 8; ++k8) {
-    int cell[3] = {c[0] - k8 / 4, c[1] - (k8 / 2) % 2, c[2] - k8 % 2};
-    if (dmin(cell[0], dmin(cell[1], cell[2])) < 0 || dmax(cell[0], dmax(cell[1], cell[2])) >= (1 << d)) continue;
-    int32_t u = P.bins.find(basis_key(d, cell[0], cell[1], cell[2]));
-    if (u < 0) continue;
-    for (int32_t j = P.bstart[u]; j < P.bstart[u + 1]; ++j) {
+    int2 range = make_int2(0, 0);
+    if (rin) {
+      range = rin[k8];
+    } else {
+      int cell[3] = {c[0] - k8 / 4, c[1] - (k8 / 2) % 2, c[2] - k8 % 2};
+      if (dmin(cell[0], dmin(cell[1], cell[2])) >= 0 && dmax(cell[0], dmax(cell[1], cell[2])) < (1 << d)) {
+        int32_t u = P.bins.find(basis_key(d, cell[0], cell[1], cell[2]));
+        if (u >= 0) range = make_int2(P.bstart[u], P.bstart[u + 1]);
+      }
+      if (rout) rout[k8] = range;
+    }
+    for (int32_t j = range.x; j < range.y; ++j) {
       T p[3] = {P.spos[3 * j], P.spos[3 * j + 1], P.spos[3 * j + 2]};
       T weight = P.sw[j];
       if (weight == T(0)) continue;
@@ -567,7 +577,8 @@ __global__ void assemble_level_kernel(const int64_t* keys, int64_t n, int d, Col
 template <class T, class S, class I, bool SCREEN>
 __global__ void __launch_bounds__(128, 12) assemble_sliced_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t off,
                                        const double* table, PointsView<T> P, const double* load, const int32_t* inv,
-                                       const int32_t* group_off, S* svals, I* sidx, T* sb) {
+                                       const int32_t* group_off, S* svals, I* sidx, T* sb,
+                                       int2* ranges_out = nullptr) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   int c[3];
@@ -579,7 +590,7 @@ __global__ void __launch_bounds__(128, 12) assemble_sliced_kernel(const int64_t*
   double pl = 0.0;
   if (SCREEN) {
     int q0[3] = {c[0] - 1, c[1] - 1, c[2] - 1};
-    pl = screening_row(P, c, d, d, q0, present, acc);
+    pl = screening_row(P, c, d, d, q0, present, acc, nullptr, ranges_out ? ranges_out + 8 * i : nullptr);
   }
   const int64_t p = inv[i];
   __align__(16) S v[28];  // written to global memory as 16-byte vectors
@@ -616,7 +627,8 @@ __global__ void __launch_bounds__(128, 12) assemble_sliced_kernel(const int64_t*
 template <class T, bool SCREEN>
 __global__ void __launch_bounds__(128, 8) cross_apply_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t coff,
                                    const double* table, PointsView<T> P, const T* cumulative, T* b,
-                                   const int32_t* inv, int32_t* ccols_out = nullptr, T* cvals_out = nullptr) {
+                                   const int32_t* inv, int32_t* ccols_out = nullptr, T* cvals_out = nullptr,
+                                   const int2* ranges_in = nullptr) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   int c[3];
@@ -628,7 +640,7 @@ __global__ void __launch_bounds__(128, 8) cross_apply_kernel(const int64_t* keys
   for (int k = 0; k < 27; ++k) acc[k] = 0.0;
   if (SCREEN) {
     int q0[3] = {ctr[0] - 1, ctr[1] - 1, ctr[2] - 1};
-    screening_row(P, c, d, d - 1, q0, present, acc);
+    screening_row(P, c, d, d - 1, q0, present, acc, ranges_in ? ranges_in + 8 * i : nullptr);
   }
   T s = T(0);
   for (int k = 0; k < 27; ++k) {
@@ -1406,6 +1418,7 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
     DBuf<T> vals, b;
     StripSchedule sched;
     DBuf<char> svals, sidx;
+    DBuf<int2> cell_ranges;  // the screening cells' point ranges of each row, assembly -> cross term
     if (!sliced) {
       cols.alloc(kSlots * n, s);
       vals.alloc(kSlots * n, s);
@@ -1421,6 +1434,7 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
       PSR_LAUNCH_CHECK();
     } else {
       build_strip_schedule(keys_at(d), n, d, sched, s);
+      if (screened) cell_ranges.alloc(8 * n, s);
       const int sbytes = mixed ? 4 : int(sizeof(T));
       const int ibytes = sched.wide ? 4 : 2;
       svals.alloc(kSlots * n * sbytes, s);
@@ -1434,7 +1448,8 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
         I* si = reinterpret_cast<I*>(sidx.p);
         if (screened)
           assemble_sliced_kernel<T, S, I, true><<<blocks_for(n, 128), 128, 0, s>>>(
-              keys_at(d), n, d, bcv, level_offsets[d], table.p, pv, loads[d].p, sched.inv.p, sched.off.p, sv, si, b.p);
+              keys_at(d), n, d, bcv, level_offsets[d], table.p, pv, loads[d].p, sched.inv.p, sched.off.p, sv, si, b.p,
+              cell_ranges.p);
         else
           assemble_sliced_kernel<T, S, I, false><<<blocks_for(n, 128), 128, 0, s>>>(
               keys_at(d), n, d, bcv, level_offsets[d], table.p, pv, loads[d].p, sched.inv.p, sched.off.p, sv, si, b.p);
@@ -1563,7 +1578,7 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
       if (screened)
         cross_apply_kernel<T, true><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d - 1],
                                                                         ctable.p, pv, cumulative.p, b.p, sched.inv.p,
-                                                                        ccols.p, cvals.p);
+                                                                        ccols.p, cvals.p, cell_ranges.p);
       else
         cross_apply_kernel<T, false><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d - 1],
                                                                          ctable.p, pv, cumulative.p, b.p,
