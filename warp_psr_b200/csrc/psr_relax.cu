@@ -374,11 +374,12 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
       const V* cur = (t & 1) ? xb1 : xb0;
       const V* prev = (t & 1) ? xb0 : xb1;
       const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-      auto stage_range = [&](int r) {
+      // range r staged by `parts` warps, part `part` of them (4 loads in flight per lane)
+      auto stage_range = [&](int r, int part, int parts) {
         const V* src = ((r >> 2) == 2 ? cur : prev) + s_lo[r];
         V* dst = foot + s_base[r];
         const int cnt = s_hi[r] - s_lo[r];
-        for (int i0 = lane; i0 < cnt; i0 += 128) {
+        for (int i0 = part * 128 + lane; i0 < cnt; i0 += 128 * parts) {
           V v[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u)
@@ -400,14 +401,22 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
         }
         __syncwarp();
       } else {
-        for (int r = 4 + warp - 1; r < 8; r += nwarps - 1) stage_range(r);
+        // slice z: 4 ranges over the other warps
+        const int parts = max(1, (nwarps - 1) / 4);
+        for (int q = warp - 1; q < 4 * parts; q += nwarps - 1) stage_range(4 + q / parts, q % parts, parts);
       }
       __syncthreads();
       if (s_fail) {
         if (staged) mbar_wait(&s_bar, parity);
         return;
       }
-      for (int q = warp; q < 8; q += nwarps) stage_range(q < 4 ? q : q + 4);
+      {  // slices z-1 and z+1: 8 ranges over all warps
+        const int parts = max(1, nwarps / 8);
+        for (int q = warp; q < 8 * parts; q += nwarps) {
+          const int rr = q / parts;
+          stage_range(rr < 4 ? rr : rr + 4, q % parts, parts);
+        }
+      }
     }
     if (threadIdx.x == 0) foot[s_total] = V(0);  // the entry absent slots read
     if (staged && !mbar_wait(&s_bar, parity)) {
