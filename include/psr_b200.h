@@ -148,8 +148,10 @@ int psr_isovalue_static(int32_t dtype, const void* values, const void* weights, 
  * stopping points).  Seeds (result dtype; NULL = zero): g_coefficients and g_cumulative
  * (total values each), g_iso, g_normalization (5, the adjoint of psr_info.normalization).
  * positions/normals are the forward's inputs (unchanged since), n points of input dtype
- * `dtype`; g_positions and g_normals (n x 3, input dtype) are written.  The tape stays, so
- * the pass can be repeated with other seeds. */
+ * `dtype`; g_positions and g_normals (n x 3, input dtype) are written, stream-ordered on
+ * `stream` (the call returns without waiting for the device; psr_result_info waits for the
+ * pass when it reports backward_ms).  The tape stays, so the pass can be repeated with other
+ * seeds. */
 int psr_backward(psr_result* result, const void* positions, const void* normals, int64_t n, int32_t dtype,
                  const void* g_coefficients, const void* g_cumulative, double g_iso, const void* g_normalization,
                  void* g_positions, void* g_normals, void* stream);

@@ -102,7 +102,10 @@ struct psr_result {
   double stage_ms[8] = {0};
   SolveStats stats;
   StageSink sink;
-  double backward_ms[8] = {0};  // last reverse pass, per stage (psr_info.backward_ms)
+  // last reverse pass, per stage (psr_info.backward_ms): its event marks are read when the
+  // info is asked for, so the pass itself ends without a host synchronisation
+  mutable double backward_ms[8] = {0};
+  mutable psr::EventMarks bw_marks;
 };
 
 namespace psr {
@@ -276,7 +279,8 @@ void backward(psr_result* R, const T* pos, const T* nrm, int64_t n, const T* g_c
     g_cum.zero();
   g_sums.zero();
   HashView hv = R->hash.view();
-  EventMarks marks;
+  EventMarks& marks = R->bw_marks;
+  if (marks.pending()) marks.collect(R->backward_ms, kBwSlots);
   marks.begin(s);
   field_backward<T>(R->keys.p, R->level_offsets, hv, reinterpret_cast<const T*>(R->coefficients.p),
                     reinterpret_cast<const T*>(R->cumulative.p), prm.depth, tp.G.sums.p, tp.G.weights.p, tp.G.count,
@@ -295,8 +299,6 @@ void backward(psr_result* R, const T* pos, const T* nrm, int64_t n, const T* g_c
   samples_backward<T>(tp.G, tp.D, tp.N, prm.depth, prm.kernel_depth, prm.base_depth, prm.samples_per_node, prm.scale,
                       g_agg, g_avg.p, g_nvals.p, g_sums.p, g_norm, pos, nrm, n, g_pos, g_nrm, s);
   marks.mark(kBwSamples, s);
-  PSR_CUDA(cudaStreamSynchronize(s));
-  marks.collect(R->backward_ms, kBwSlots);
 }
 
 
@@ -409,6 +411,7 @@ int psr_result_info(const psr_result* R, psr_info* info) {
   info->relax_finest_ms = R->stats.level_relax_ms.empty() ? 0.0 : R->stats.level_relax_ms.back();
   info->relax_finest_row_visits = R->stats.finest_row_visits;
   for (int i = 0; i < 5; ++i) info->normalization[i] = R->normalization[i];
+  if (R->bw_marks.pending()) R->bw_marks.collect(R->backward_ms, kBwSlots);
   for (int i = 0; i < 8; ++i) info->backward_ms[i] = R->backward_ms[i];
   return PSR_OK;
 }

@@ -55,7 +55,9 @@ struct EventMarks {
     PSR_CUDA(cudaEventRecord(e, s));
     marks.emplace_back(slot, e);
   }
-  void collect(double* out, int slots) {  // after synchronisation
+  bool pending() const { return start != nullptr; }
+  void collect(double* out, int slots) {  // waits for the last mark
+    if (!marks.empty()) cudaEventSynchronize(marks.back().second);
     for (int i = 0; i < slots; ++i) out[i] = 0;
     cudaEvent_t prev = start;
     for (auto& m : marks) {
@@ -67,6 +69,13 @@ struct EventMarks {
     if (start) cudaEventDestroy(start);
     marks.clear();
     start = nullptr;
+  }
+  EventMarks() = default;
+  EventMarks(const EventMarks&) = delete;
+  EventMarks& operator=(const EventMarks&) = delete;
+  ~EventMarks() {
+    for (auto& m : marks) cudaEventDestroy(m.second);
+    if (start) cudaEventDestroy(start);
   }
 };
 enum { kBwField, kBwMirror, kBwSweep, kBwOperator, kBwBase, kBwPoints, kBwNormalLoads, kBwSamples, kBwSlots };

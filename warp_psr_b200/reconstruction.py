@@ -255,6 +255,38 @@ def reconstruct(positions, normals, *, depth=6, full_depth=3, base_depth=None, s
 BACKWARD_STAGES = ("field", "mirrored_operators", "reverse_sweeps", "operator_adjoints", "base_multigrid",
                    "point_constraints", "normal_loads", "splats_density_samples")
 
+class _BackwardStats(dict):
+    """Holds the forward's result and, once a reverse pass ran, ``"backward_ms"``: the device
+    ms per stage of the last pass (BACKWARD_STAGES), read from the library on first access so
+    the pass itself needs no host synchronisation."""
+
+    def __init__(self):
+        super().__init__()
+        self._pending = None
+
+    def reverse_pass_done(self, result):
+        self._pending = result
+
+    def _settle(self):
+        if self._pending is not None:
+            result, self._pending = self._pending, None
+            info = _lib.Info()
+            _lib.check(_lib.load().psr_result_info(result.field._handle.ptr, ctypes.byref(info)))
+            super().__setitem__("backward_ms", dict(zip(BACKWARD_STAGES, (float(v) for v in info.backward_ms))))
+
+    def __getitem__(self, key):
+        self._settle()
+        return super().__getitem__(key)
+
+    def get(self, key, default=None):
+        self._settle()
+        return super().get(key, default)
+
+    def __contains__(self, key):
+        self._settle()
+        return super().__contains__(key)
+
+
 class _ReconstructFunction(torch.autograd.Function):
     """Forward: a differentiable reconstruction.  Outputs the per-level coefficients, the
     cumulative coefficients, the isovalue and the 5-value sample normalisation; backward is
@@ -292,9 +324,7 @@ class _ReconstructFunction(torch.autograd.Function):
                 result.field._handle.ptr, p.data_ptr(), n.data_ptr(), p.shape[0], dtype_code,
                 ptr(keep[0]), ptr(keep[1]), float(g_iso) if g_iso is not None else 0.0, ptr(keep[2]),
                 g_p.data_ptr(), g_n.data_ptr(), _stream(p.device)))
-        info = _lib.Info()
-        _lib.check(_lib.load().psr_result_info(result.field._handle.ptr, ctypes.byref(info)))
-        ctx.box["backward_ms"] = dict(zip(BACKWARD_STAGES, (float(v) for v in info.backward_ms)))
+        ctx.box.reverse_pass_done(result)
         return (g_p if ctx.needs_input_grad[0] else None), (g_n if ctx.needs_input_grad[1] else None), None, None
 
 
@@ -330,8 +360,8 @@ class _EvaluateFunction(torch.autograd.Function):
                 g_norm.data_ptr(), _stream(q.device)))
         g_iso = None
         if ctx.centered and gv is not None:
-            valid = torch.isfinite(gv)
-            g_iso = -gv[valid].sum()
+            # masked sum without boolean indexing (which would wait for the device)
+            g_iso = -torch.where(torch.isfinite(gv), gv, torch.zeros_like(gv)).sum()
         return g_coef, g_cum, g_iso, g_norm, g_q, None, None
 
 
@@ -382,7 +412,7 @@ def reconstruct_differentiable(positions, normals, **options):
             raise ValueError(f"{name} must be a constant scalar; only positions and normals support gradients")
     if options.get("keep_stages"):
         raise ValueError("keep_stages is not available for differentiable reconstructions")
-    box = {}
+    box = _BackwardStats()
     coefficients, cumulative, iso, normalization = _ReconstructFunction.apply(positions, normals, box, options)
     out = DifferentiableReconstruction(coefficients, cumulative, iso, normalization, box["result"])
     out.backward_stats = box  # box["backward_ms"]: device ms per stage of the last reverse pass
