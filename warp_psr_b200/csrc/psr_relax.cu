@@ -811,7 +811,11 @@ void build_strip_schedule(const int64_t* keys, int64_t rows, int depth, StripSch
   max_group_kernel<<<blocks_for(groups), kThreads, 0, s>>>(S.off.p, groups, gmax.p);
   PSR_LAUNCH_CHECK();
   // Group-relative neighbour indices fit 16 bits unless a (slice, colour) group is huge.
+  // PSR_INDEX_WIDTH=32 takes the 32-bit rows regardless (test override: the huge-group path
+  // on small levels).
   S.wide = read_scalar(gmax.p, s) >= 32767;
+  if (const char* env = std::getenv("PSR_INDEX_WIDTH"))
+    if (std::atoi(env) == 32) S.wide = true;
 }
 
 template <class T, class V, class I>
