@@ -7,6 +7,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -288,7 +289,11 @@ struct ColumnIndex {
   // `max_depth` bounds the depth of every key (coordinates within [0, 2^d]).
   void build(const int64_t* keys, int64_t n, int max_depth, cudaStream_t s) {
     view_ = ColumnView();
-    if (max_depth <= kDenseColumnDepth) {
+    // PSR_COLUMN_INDEX=hash takes the hashed column index at any depth (test override: the
+    // path of depths beyond the dense tables on small cases).
+    const char* mode = std::getenv("PSR_COLUMN_INDEX");
+    const bool force_hash = mode && mode[0] == 'h';
+    if (max_depth <= kDenseColumnDepth && !force_hash) {
       const int64_t size = dense_column_base(max_depth + 1);
       table.alloc(size, s);
       PSR_CUDA(cudaMemsetAsync(table.p, 0xff, size * sizeof(int2), s));
