@@ -1,6 +1,8 @@
-"""The hashed column index (used for depths beyond the dense per-depth tables, i.e. above 12)
-forced on small cases with PSR_COLUMN_INDEX=hash: reconstructions, field evaluation and the
-reverse pass agree with the dense-table path."""
+"""Paths that only large inputs take, forced on small cases: the hashed column index (used
+for depths beyond the dense per-depth tables, above 12; PSR_COLUMN_INDEX=hash) and the base
+relaxation with x in global memory (base levels too large for shared memory;
+PSR_BASE_RELAX=global).  Reconstructions, field evaluation and the reverse pass agree with
+the default paths."""
 import numpy as np
 import pytest
 import torch
@@ -43,4 +45,39 @@ def test_reverse_pass_with_hashed_columns_agrees(monkeypatch):
         (v * seed).sum().backward()
         grads.append(torch.cat([P.grad.flatten(), N.grad.flatten()]))
     # equal up to the summation order of atomic accumulations
+    torch.testing.assert_close(grads[1], grads[0], rtol=1e-10, atol=1e-13)
+
+
+@pytest.mark.parametrize("case", ["spsr_base1_depth4", "psr_base0_constant_mode"])
+def test_base_relaxation_in_global_memory_is_identical(monkeypatch, case):
+    """PSR_BASE_RELAX=global: the base levels' colour relaxation with x in global memory (the
+    path of base levels too large for shared memory) gives the shared-memory path's result."""
+    from warp_psr_b200 import reconstruct
+    p0, m0 = cloud()
+    opts = {k: v for k, v in CASES[case].items()}
+    runs = []
+    for mode in (None, "global"):
+        if mode:
+            monkeypatch.setenv("PSR_BASE_RELAX", mode)
+        r = reconstruct(torch.tensor(p0, device="cuda"), torch.tensor(m0, device="cuda"), **opts)
+        runs.append((r.field.coefficients.cpu().numpy(), r.iso_value))
+    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    assert runs[0][1] == runs[1][1]
+
+
+def test_reverse_base_relaxation_in_global_memory_agrees(monkeypatch):
+    from warp_psr_b200 import reconstruct_differentiable
+    p0, m0 = cloud()
+    q = torch.tensor(QUERIES, device="cuda", dtype=torch.float64)
+    seed = torch.tensor(SEED, device="cuda", dtype=torch.float64)
+    grads = []
+    for mode in (None, "global"):
+        if mode:
+            monkeypatch.setenv("PSR_BASE_RELAX", mode)
+        P = torch.tensor(p0, device="cuda", requires_grad=True)
+        N = torch.tensor(m0, device="cuda", requires_grad=True)
+        res = reconstruct_differentiable(P, N, **CASES["spsr_base1_depth4"])
+        v, _, _ = res.evaluate(q, centered=True)
+        (v * seed).sum().backward()
+        grads.append(torch.cat([P.grad.flatten(), N.grad.flatten()]))
     torch.testing.assert_close(grads[1], grads[0], rtol=1e-10, atol=1e-13)

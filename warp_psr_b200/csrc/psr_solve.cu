@@ -897,7 +897,11 @@ template <class T>
 static void relax_colors(const int32_t* cols, const T* vals, const T* b, T* x, const int32_t* rows,
                          const int32_t* group_off, int iters, int forward, T* hist, int64_t n, cudaStream_t s) {
   const size_t bytes = size_t(n + 1) * sizeof(T);  // x and a +0 entry
-  if (n > 0 && bytes <= kRelaxSharedBytes) {
+  // PSR_BASE_RELAX=global keeps x in global memory at any size (test override: the path of
+  // base levels too large for shared memory, on small cases).
+  const char* mode = std::getenv("PSR_BASE_RELAX");
+  const bool force_global = mode && mode[0] == 'g';
+  if (n > 0 && bytes <= kRelaxSharedBytes && !force_global) {
     static bool configured = false;
     if (!configured) {
       PSR_CUDA(cudaFuncSetAttribute(relax_colors_shared_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
