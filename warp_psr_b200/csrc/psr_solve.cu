@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(256, 6) normal_stencil_kernel(const int64_t* k
 // the up to W keys after each bound (increasing z, so in the z-loop's order) are loaded
 // together.  The additions run in the same (x, y, z) order: same result.
 template <class T, int W>
-__global__ void __launch_bounds__(256, 4) normal_stencil_dense_kernel(const int64_t* keys, int64_t n, int test_depth,
+__global__ void __launch_bounds__(256, W == 4 ? 5 : 4) normal_stencil_dense_kernel(const int64_t* keys, int64_t n, int test_depth,
                                                                       int normal_depth, ColumnView cv, int64_t noff,
                                                                       const T* nvals, const double* table, int first,
                                                                       double* out) {
@@ -644,7 +644,10 @@ __global__ void __launch_bounds__(128, 8) cross_apply_kernel(const int64_t* keys
   }
   T s = T(0);
   for (int k = 0; k < 27; ++k) {
-    if (col[k] < 0) continue;
+    if (col[k] < 0) {
+      if (cvals_out) cvals_out[i * kSlots + k] = T(0);
+      continue;
+    }
     const double* x = table + (c[0] * 3 + k / 9) * 2;
     const double* y = table + (c[1] * 3 + (k / 3) % 3) * 2;
     const double* z = table + (c[2] * 3 + k % 3) * 2;
@@ -655,6 +658,7 @@ __global__ void __launch_bounds__(128, 8) cross_apply_kernel(const int64_t* keys
   }
   if (ccols_out)
     for (int k = 0; k < kSlots; ++k) ccols_out[i * kSlots + k] = k < 27 ? col[k] : -1;
+  if (cvals_out) cvals_out[i * kSlots + 27] = T(0);
   const int64_t p = inv ? inv[i] : i;
   b[p] = -s + b[p];
 }
@@ -1576,8 +1580,7 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
       DBuf<T> cvals;
       if (tp) {
         ccols.alloc(kSlots * n, s);
-        cvals.alloc(kSlots * n, s);
-        cvals.zero();
+        cvals.alloc(kSlots * n, s);  // every slot written by the cross kernel
       }
       if (screened)
         cross_apply_kernel<T, true><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d - 1],
