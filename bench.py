@@ -58,6 +58,10 @@ class Clocks:
         self.index = index
         self.proc = None
         self.lines = []
+        self.first = 0  # samples before this index precede the timed region
+
+    def start_timing(self):
+        self.first = len(self.lines)
 
     def __enter__(self):
         try:
@@ -85,7 +89,7 @@ class Clocks:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for line in self.lines:
+        for line in self.lines[self.first:]:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 7:
                 continue
@@ -169,10 +173,6 @@ def run_ours(args, rank, world):
                    "relax_row_visits": r.diagnostics["relax_row_visits"]}
         return summary, P.grad, N.grad
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-
     def timed(fn, k):
         total = 0.0
         last = None
@@ -187,14 +187,23 @@ def run_ours(args, rank, world):
             total += a.elapsed_time(b)
         return total / k, last
 
-    replicas.barrier()
-    torch.cuda.synchronize()
-    launches0 = _lib.kernel_launches()
-    finest.clear()
-    split.clear()
-    bw_stages.clear()
-    with Clocks(device.index) as clocks:
+    # The clock sampler (an nvidia-smi process) starts before the warm-up, so that its start
+    # does not fall into a timed step; only the samples taken while timing are summarised.
+    clocks = Clocks(device.index).__enter__()
+    try:
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        replicas.barrier()
+        torch.cuda.synchronize()
+        launches0 = _lib.kernel_launches()
+        finest.clear()
+        split.clear()
+        bw_stages.clear()
+        clocks.start_timing()
         ms, (result, _, _) = timed(step, args.steps)
+    finally:
+        clocks.__exit__(None, None, None)
     launches = _lib.kernel_launches() - launches0
     bw_stage_ms = {k: round(statistics.mean(b[k] for b in bw_stages), 3) for k in bw_stages[0]} if bw_stages else {}
     fwd_ms = statistics.mean(x[0] for x in split)
