@@ -84,9 +84,9 @@ __global__ void transpose_values_kernel(int64_t n, const int64_t* skeys, const i
 }
 
 template <class T>
-__global__ void gather_seed_kernel(const int32_t* perm2, const int32_t* orig_of, int64_t n, const T* seed, T* b2) {
-  int64_t p2 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (p2 < n) b2[p2] = seed[orig_of ? orig_of[perm2[p2]] : perm2[p2]];
+__global__ void gather_seed_kernel(const int32_t* perm, int64_t n, const T* seed, T* out) {
+  int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (p < n) out[p] = seed[perm[p]];
 }
 
 // ------------------------------------------------------------------ fused level reverse kernel
@@ -108,8 +108,7 @@ struct LevelReverse {
   const int32_t* off = nullptr;
   const I* sidx = nullptr;
   const T* xhist = nullptr;    // n x iters forward x after each visit (schedule order)
-  const T* mu = nullptr;       // n x iters increments of the reversed sweep (mirrored schedule order)
-  const int32_t* inv2 = nullptr;  // key index -> mirrored schedule position
+  const T* mu = nullptr;       // n x iters increments of the reversed sweep (schedule order)
   // base level: explicit operator adjoint (28 slots, key order)
   const T* g_A = nullptr;
   // cross
@@ -140,7 +139,7 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
   T gA[27];
   for (int k = 0; k < 27; ++k) gA[k] = T(0);
   if (SLICED) {
-    const int64_t p = L.inv[i], p2 = L.inv2[i];
+    const int64_t p = L.inv[i];
     const int own = (c[0] & 1) + 2 * (c[1] & 1);
     // the row's index record (vector loads) and its increments of every visit, loaded once
     __align__(16) I row[kIdxSlots];
@@ -151,7 +150,7 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
       for (int q = 0; q < kIdxSlots * int(sizeof(I)) / 16; ++q) dst[q] = __ldg(src + q);
     }
     const int iters = ITERS > 0 ? ITERS : L.iters;
-    const T* mrow = L.mu + p2 * iters;
+    const T* mrow = L.mu + p * iters;
     // fixed visit count (the common 8): records in registers, vector loads
     T mu[ITERS > 0 ? ITERS : 1];
     if constexpr (ITERS > 0) {
@@ -1014,12 +1013,11 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
     PSR_LAUNCH_CHECK();
     // The reverse sweep runs on the forward schedule in mirrored slice order over the
     // transposed operator; its increments are recorded at the forward positions.
-    DBuf<T> b2(n + 4, s), M(n, s), mu(int64_t(p.iters) * n, s);
-    b2.zero();
+    DBuf<T> sb(n + 4, s), M(n, s), mu(int64_t(p.iters) * n, s);
+    sb.zero();
     M.zero();
-    gather_seed_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(st.sched.perm.p, nullptr, n, seed.p, b2.p);
+    gather_seed_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(st.sched.perm.p, n, seed.p, sb.p);
     PSR_LAUNCH_CHECK();
-    const int32_t* inv2 = st.sched.inv.p;
     mark(kBwMirror);
     auto reverse_sweep = [&](auto s_tag, auto i_tag) {
       using S = decltype(s_tag);
@@ -1030,7 +1028,7 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
                                                                        reinterpret_cast<const I*>(st.sidx.p), tv.p);
       PSR_LAUNCH_CHECK();
       mark(kBwMirror);
-      relax_strips_scheduled<S, T, I>(st.sched, tv.p, reinterpret_cast<const I*>(st.sidx.p), b2.p, M.p, p.iters, s,
+      relax_strips_scheduled<S, T, I>(st.sched, tv.p, reinterpret_cast<const I*>(st.sidx.p), sb.p, M.p, p.iters, s,
                                       nullptr, mu.p, true, true);
       mark(kBwSweep);
     };
@@ -1068,7 +1066,6 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
       L.sidx = reinterpret_cast<const I*>(st.sidx.p);
       L.xhist = st.hist.p;
       L.mu = mu.p;
-      L.inv2 = inv2;
       L.cross = true;
       L.ccols = st.ccols.p;
       L.cvals = st.cvals.p;
