@@ -324,9 +324,12 @@ __global__ void __launch_bounds__(128) level_rows_reverse_kernel(const int64_t* 
 #pragma unroll
     for (int q = 0; q < kIdxSlots * int(sizeof(I)) / 16; ++q) dst[q] = __ldg(src + q);
   }
-  T mu[ITERS];
+  // visit records as 16-byte vector loads (a row's ITERS values are contiguous and aligned)
+  static_assert(ITERS * sizeof(T) % 16 == 0, "visit records in 16-byte vectors");
+  __align__(16) T mu[ITERS];  // reverse visit u
 #pragma unroll
-  for (int u = 0; u < ITERS; ++u) mu[u] = __ldg(mu_hist + p * ITERS + u);  // reverse visit u
+  for (int q = 0; q < ITERS * int(sizeof(T)) / 16; ++q)
+    reinterpret_cast<int4*>(mu)[q] = __ldg(reinterpret_cast<const int4*>(mu_hist + p * ITERS) + q);
   T* out = row_gA ? row_gA + i * 27 : nullptr;
 #pragma unroll
   for (int k = 0; k < 27; ++k) {
@@ -337,10 +340,10 @@ __global__ void __launch_bounds__(128) level_rows_reverse_kernel(const int64_t* 
       const int64_t pk = __ldg(off + sched_group(q)) + int64_t(idx);
       const int qc = (q[0] & 1) + 2 * (q[1] & 1);
       const bool delayed = !(k == 13 || k % 3 == 2 || (k % 3 == 1 && qc < own));
-      const T* xrow = xhist + pk * ITERS;
-      T xv[ITERS];
+      const int4* xrow = reinterpret_cast<const int4*>(xhist + pk * ITERS);
+      __align__(16) T xv[ITERS];
 #pragma unroll
-      for (int t = 0; t < ITERS; ++t) xv[t] = __ldg(xrow + t);
+      for (int q = 0; q < ITERS * int(sizeof(T)) / 16; ++q) reinterpret_cast<int4*>(xv)[q] = __ldg(xrow + q);
 #pragma unroll
       for (int t = 0; t < ITERS; ++t) {
         const T x_prev = t > 0 ? xv[t > 0 ? t - 1 : 0] : T(0);
