@@ -517,26 +517,27 @@ __device__ __forceinline__ int colour8(const int c[3]) { return (c[0] & 1) + 2 *
 template <class T>
 __global__ void relax_operator_adjoint_kernel(const int64_t* keys, const int32_t* cols, const T* vals, int64_t n,
                                               int iters, int forward, const T* hist_fwd, const T* hist_rev, T* g_A) {
-  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i >= n) return;
+  // one thread per (row, slot)
+  const int64_t t0 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (t0 >= 27 * n) return;
+  const int64_t i = t0 / 27;
+  const int k = int(t0 % 27);
   int ci[3];
   key_coords(keys[i], ci);
   const int pos_i = forward ? colour8(ci) : 7 - colour8(ci);
-  T diag_i = T(0);
-  for (int k = 0; k < 27; ++k)
-    if (cols[i * kSlots + k] == int32_t(i)) diag_i = vals[i * kSlots + k];
+  // the rows hold their k-th neighbour in slot k, so a row's own column is slot 13
+  const T diag_i = cols[i * kSlots + 13] == int32_t(i) ? vals[i * kSlots + 13] : T(0);
   if (diag_i == T(0)) return;
   const T inv_i = T(1.0) / diag_i;
-  for (int k = 0; k < 27; ++k) {
+  {
     const int32_t c = cols[i * kSlots + k];
-    if (c < 0) continue;
+    if (c < 0) return;
     int ck[3];
     key_coords(keys[c], ck);
     const int pos_k = forward ? colour8(ck) : 7 - colour8(ck);
     T diag_k = T(0);
-    if (c == int32_t(i) || pos_k < pos_i)
-      for (int q = 0; q < 27; ++q)
-        if (cols[int64_t(c) * kSlots + q] == c) diag_k = vals[int64_t(c) * kSlots + q];
+    if ((c == int32_t(i) || pos_k < pos_i) && cols[int64_t(c) * kSlots + 13] == c)
+      diag_k = vals[int64_t(c) * kSlots + 13];
     T acc = T(0);
     for (int t = 0; t < iters; ++t) {
       const T mu = hist_rev[2 * (int64_t(iters - 1 - t) * n + i) + 1] * inv_i;
@@ -568,7 +569,7 @@ static void relax_colors_adjoint(const int64_t* keys, const int32_t* cols, const
   DBuf<T> M(n, s), hist_rev(2 * int64_t(iters) * n, s);
   M.zero();
   relax_colors<T>(cols, vals_t, lambda, M.p, rows, group_off, iters, forward ? 0 : 1, hist_rev.p, n, s);
-  relax_operator_adjoint_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(keys, cols, vals, n, iters, forward, hist_fwd,
+  relax_operator_adjoint_kernel<T><<<blocks_for(27 * n), kThreads, 0, s>>>(keys, cols, vals, n, iters, forward, hist_fwd,
                                                                        hist_rev.p, g_A);
   PSR_LAUNCH_CHECK();
   adjoint_out_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(cols, vals_t, M.p, n, lambda, g_b);
@@ -598,11 +599,14 @@ template <class T>
 __global__ void galerkin_reverse_kernel(const int64_t* fine_keys, int64_t nf, const int32_t* fcols,
                                         const int32_t* pcol, const T* pval, const int64_t* coarse_keys,
                                         const int32_t* ccols, const T* g_Ac, T* g_Af) {
-  int64_t a = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (a >= nf) return;
-  for (int e = 0; e < 27; ++e) {
+  // one thread per (fine row, slot): 27x the threads of a row loop, same sums
+  const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (t >= 27 * nf) return;
+  const int64_t a = t / 27;
+  const int e = int(t % 27);
+  {
     const int32_t b = fcols[a * kSlots + e];
-    if (b < 0) continue;
+    if (b < 0) return;
     T total = T(0);
     for (int u = 0; u < 8; ++u) {
       const int32_t ci = pcol[a * 8 + u];
@@ -1199,7 +1203,7 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
     // Galerkin products, coarsest first
     for (int l = 0; l < base; ++l) {
       const int64_t nf = count_at(l + 1);
-      galerkin_reverse_kernel<T><<<blocks_for(nf), kThreads, 0, s>>>(keys_at(l + 1), nf, tp.mcols[l + 1].p,
+      galerkin_reverse_kernel<T><<<blocks_for(27 * nf), kThreads, 0, s>>>(keys_at(l + 1), nf, tp.mcols[l + 1].p,
                                                                      tp.pcol[l + 1].p, tp.pval[l + 1].p, keys_at(l),
                                                                      tp.mcols[l].p, gA[l].p, gA[l + 1].p);
       PSR_LAUNCH_CHECK();
