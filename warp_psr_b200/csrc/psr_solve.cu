@@ -1028,66 +1028,95 @@ void relax_sliced_ell(const int32_t* cols, const T* vals, const V* b, V* x, cons
 }
 
 // ------------------------------------------------------------------ A10 base solve (solver.py:241-317)
-// Galerkin R A P on a complete regular level (all nodes of [0, 2^d]^3 present): one thread
-// per coarse row, products summed in the fixed order of the oracle's sparse product.
+// Galerkin R A P on a complete regular level (all nodes of [0, 2^d]^3 present), products
+// summed in the fixed order of the oracle's sparse product.
+// One 128-thread block per coarse row: the 27 fine rows of R^T are found once (one thread
+// each); each of the 125 sums over the fine neighbourhood is one thread (its contributions
+// arrive in fine-row order k); each of the 27 coarse slots is one thread summing over the
+// fine neighbourhood in order o.
 template <class T>
-__global__ void galerkin_kernel(const int64_t* coarse_keys, int64_t nc, int d /*fine*/, HashView bh, int64_t foff,
-                                int64_t coff, const int32_t* fcols, const T* fvals, int32_t* ccols, T* cvals) {
-  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+__global__ void __launch_bounds__(128) galerkin_block_kernel(const int64_t* coarse_keys, int64_t nc, int d /*fine*/,
+                                                             HashView bh, int64_t foff, int64_t coff,
+                                                             const int32_t* fcols, const T* fvals, int32_t* ccols,
+                                                             T* cvals) {
+  const int64_t i = blockIdx.x;
   if (i >= nc) return;
+  __shared__ int64_t s_fr[27];
+  __shared__ T s_r[27];
+  __shared__ T s_acc[125];
+  __shared__ int s_touched[125];
   int c[3];
   key_coords(coarse_keys[i], c);
-  int lim = 1 << d;
-  T acc[125];
-  uint64_t touched[2] = {0, 0};
-  for (int o = 0; o < 125; ++o) acc[o] = T(0);
-  for (int k = 0; k < 27; ++k) {  // rows of R = columns of P: fine nodes 2c + {-1,0,1}^3
-    int f[3] = {2 * c[0] + k / 9 - 1, 2 * c[1] + (k / 3) % 3 - 1, 2 * c[2] + k % 3 - 1};
-    if (dmin(f[0], dmin(f[1], f[2])) < 0 || dmax(f[0], dmax(f[1], f[2])) > lim) continue;
-    int32_t g = bh.find(basis_key(d, f[0], f[1], f[2]));
-    if (g < 0) continue;
-    int64_t fr = int64_t(g) - foff;
-    T h[3];
-    for (int a = 0; a < 3; ++a) h[a] = T(1.0) - fabs(T(f[a]) * T(0.5) - T(c[a]));
-    T r = h[0] * h[1] * h[2];
-    for (int e = 0; e < 27; ++e) {
+  const int lim = 1 << d;
+  const int tid = threadIdx.x;
+  if (tid < 27) {  // rows of R = columns of P: fine nodes 2c + {-1,0,1}^3
+    const int k = tid;
+    const int f[3] = {2 * c[0] + k / 9 - 1, 2 * c[1] + (k / 3) % 3 - 1, 2 * c[2] + k % 3 - 1};
+    int64_t fr = -1;
+    T r = T(0);
+    if (!(dmin(f[0], dmin(f[1], f[2])) < 0 || dmax(f[0], dmax(f[1], f[2])) > lim)) {
+      const int32_t g = bh.find(basis_key(d, f[0], f[1], f[2]));
+      if (g >= 0) {
+        fr = int64_t(g) - foff;
+        T h[3];
+        for (int a = 0; a < 3; ++a) h[a] = T(1.0) - fabs(T(f[a]) * T(0.5) - T(c[a]));
+        r = h[0] * h[1] * h[2];
+      }
+    }
+    s_fr[k] = fr;
+    s_r[k] = r;
+  }
+  __syncthreads();
+  if (tid < 125) {  // fine neighbour j = 2c - 2 + (o / 25, o / 5 % 5, o % 5)
+    const int o = tid;
+    T a = T(0);
+    int touched = 0;
+    for (int k = 0; k < 27; ++k) {
+      const int64_t fr = s_fr[k];
+      if (fr < 0) continue;
+      const int ex = o / 25 - k / 9, ey = (o / 5) % 5 - (k / 3) % 3, ez = o % 5 - k % 3;
+      if (ex < 0 || ex > 2 || ey < 0 || ey > 2 || ez < 0 || ez > 2) continue;
+      const int e = ex * 9 + ey * 3 + ez;
       if (fcols[fr * kSlots + e] < 0) continue;
-      int j[3] = {f[0] + e / 9 - 1, f[1] + (e / 3) % 3 - 1, f[2] + e % 3 - 1};
-      int o = (j[0] - 2 * c[0] + 2) * 25 + (j[1] - 2 * c[1] + 2) * 5 + (j[2] - 2 * c[2] + 2);
-      acc[o] = acc[o] + r * fvals[fr * kSlots + e];
-      touched[o >> 6] |= uint64_t(1) << (o & 63);
+      a = a + s_r[k] * fvals[fr * kSlots + e];
+      touched = 1;
     }
+    s_acc[o] = a;
+    s_touched[o] = touched;
   }
-  T cacc[27];
-  uint32_t ctouched = 0;
-  for (int k = 0; k < 27; ++k) cacc[k] = T(0);
-  for (int o = 0; o < 125; ++o) {
-    if (!((touched[o >> 6] >> (o & 63)) & 1)) continue;
-    int j[3] = {2 * c[0] - 2 + o / 25, 2 * c[1] - 2 + (o / 5) % 5, 2 * c[2] - 2 + o % 5};
-    for (int k = 0; k < 8; ++k) {
-      int jj[3] = {j[0] / 2 + k / 4, j[1] / 2 + (k / 2) % 2, j[2] / 2 + k % 2};
-      T h[3];
-      for (int a = 0; a < 3; ++a) h[a] = T(1.0) - fabs(T(j[a]) * T(0.5) - T(jj[a]));
-      T w = h[0] * h[1] * h[2];
-      if (!(w > T(0))) continue;
-      if (dmax(jj[0], dmax(jj[1], jj[2])) > (lim >> 1)) continue;
-      int s = (jj[0] - c[0] + 1) * 9 + (jj[1] - c[1] + 1) * 3 + (jj[2] - c[2] + 1);
-      cacc[s] = cacc[s] + acc[o] * w;
-      ctouched |= 1u << s;
+  __syncthreads();
+  if (tid < 27) {  // coarse slot
+    const int sk = tid;
+    T cs = T(0);
+    bool ct = false;
+    for (int o = 0; o < 125; ++o) {
+      if (!s_touched[o]) continue;
+      const int j[3] = {2 * c[0] - 2 + o / 25, 2 * c[1] - 2 + (o / 5) % 5, 2 * c[2] - 2 + o % 5};
+      for (int k = 0; k < 8; ++k) {
+        const int jj[3] = {j[0] / 2 + k / 4, j[1] / 2 + (k / 2) % 2, j[2] / 2 + k % 2};
+        const int sl = (jj[0] - c[0] + 1) * 9 + (jj[1] - c[1] + 1) * 3 + (jj[2] - c[2] + 1);
+        if (sl != sk) continue;
+        T h[3];
+        for (int a = 0; a < 3; ++a) h[a] = T(1.0) - fabs(T(j[a]) * T(0.5) - T(jj[a]));
+        const T w = h[0] * h[1] * h[2];
+        if (!(w > T(0))) continue;
+        if (dmax(jj[0], dmax(jj[1], jj[2])) > (lim >> 1)) continue;
+        cs = cs + s_acc[o] * w;
+        ct = true;
+      }
     }
-  }
-  for (int k = 0; k < 27; ++k) {
     int32_t col = -1;
-    if ((ctouched >> k) & 1) {
-      int q[3] = {c[0] + k / 9 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k % 3 - 1};
-      int32_t g = bh.find(basis_key(d - 1, q[0], q[1], q[2]));
+    if (ct) {
+      const int q[3] = {c[0] + sk / 9 - 1, c[1] + (sk / 3) % 3 - 1, c[2] + sk % 3 - 1};
+      const int32_t g = bh.find(basis_key(d - 1, q[0], q[1], q[2]));
       col = g >= 0 ? int32_t(g - coff) : -1;
     }
-    ccols[i * kSlots + k] = col;
-    cvals[i * kSlots + k] = col >= 0 ? cacc[k] : T(0);
+    ccols[i * kSlots + sk] = col;
+    cvals[i * kSlots + sk] = col >= 0 ? cs : T(0);
+  } else if (tid == 27) {
+    ccols[i * kSlots + 27] = -1;
+    cvals[i * kSlots + 27] = T(0);
   }
-  ccols[i * kSlots + 27] = -1;
-  cvals[i * kSlots + 27] = T(0);
 }
 
 __device__ __forceinline__ int root_row(int64_t key) {  // solver.py:30-33
@@ -1489,8 +1518,9 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
         mv[l].alloc(kSlots * nl, s);
         const int32_t* fc = l + 1 == base ? cols.p : mc[l + 1].p;
         const T* fv = l + 1 == base ? vals.p : mv[l + 1].p;
-        galerkin_kernel<T><<<blocks_for(nl, 64), 64, 0, s>>>(keys_at(l), nl, l + 1, bh, level_offsets[l + 1],
-                                                            level_offsets[l], fc, fv, mc[l].p, mv[l].p);
+        if (nl > 0)
+          galerkin_block_kernel<T><<<unsigned(nl), 128, 0, s>>>(keys_at(l), nl, l + 1, bh, level_offsets[l + 1],
+                                                                level_offsets[l], fc, fv, mc[l].p, mv[l].p);
         PSR_LAUNCH_CHECK();
       }
       for (int l = 0; l <= base; ++l) {
