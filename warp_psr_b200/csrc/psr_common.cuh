@@ -166,6 +166,23 @@ struct HashView {
       h = (h + 1) & mask;
     }
   }
+  // First probe only: the value, -1 (absent) or -2 (slot taken by another key: continue
+  // with find_from(key, h)).  Lets a caller put several first probes in flight together.
+  __device__ __forceinline__ int32_t first_probe(int64_t key, uint64_t& h) const {
+    if (!slots) return -1;
+    h = mix(uint64_t(key)) & mask;
+    const longlong2 e = __ldg(slots + h);
+    if (e.x == key) return int32_t(e.y);
+    return e.x == -1 ? -1 : -2;
+  }
+  __device__ __forceinline__ int32_t find_from(int64_t key, uint64_t h) const {
+    while (true) {
+      h = (h + 1) & mask;
+      const longlong2 e = __ldg(slots + h);
+      if (e.x == key) return int32_t(e.y);
+      if (e.x == -1) return -1;
+    }
+  }
   __host__ __device__ static __forceinline__ uint64_t mix(uint64_t x) {
     x ^= x >> 31;
     x *= 0x7fb5d329728ea185ULL;

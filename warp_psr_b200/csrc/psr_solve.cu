@@ -671,17 +671,28 @@ __global__ void prolongation_kernel(const int64_t* fine, int64_t n, int d, HashV
   if (i >= n) return;
   int f[3];
   key_coords(fine[i], f);
-  int out = 0;
+  // the parents' weights, then their first hash probes together, collisions after
+  T wk[8];
+  int64_t key8[8];
+  uint64_t h8[8];
+  int32_t g8[8];
+#pragma unroll
   for (int k = 0; k < 8; ++k) {
-    int c[3] = {f[0] / 2 + k / 4, f[1] / 2 + (k / 2) % 2, f[2] / 2 + k % 2};
+    const int c[3] = {f[0] / 2 + k / 4, f[1] / 2 + (k / 2) % 2, f[2] / 2 + k % 2};
     T h[3];
     for (int a = 0; a < 3; ++a) h[a] = T(1.0) - fabs(T(f[a]) * T(0.5) - T(c[a]));
-    T weight = h[0] * h[1] * h[2];
-    int32_t column = -1;
-    if (weight > T(0)) {
-      int32_t g = bh.find(basis_key(d - 1, c[0], c[1], c[2]));
-      column = g >= 0 ? int32_t(g - coff) : -1;
-    }
+    wk[k] = h[0] * h[1] * h[2];
+    key8[k] = basis_key(d - 1, c[0], c[1], c[2]);
+    h8[k] = 0;
+    g8[k] = wk[k] > T(0) ? bh.first_probe(key8[k], h8[k]) : -1;
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (g8[k] == -2) g8[k] = bh.find_from(key8[k], h8[k]);
+  int out = 0;
+  for (int k = 0; k < 8; ++k) {
+    const T weight = wk[k];
+    const int32_t column = g8[k] >= 0 ? int32_t(g8[k] - coff) : -1;
     if (column >= 0) {
       pcol[i * 8 + out] = column;
       pval[i * 8 + out] = weight;
