@@ -370,12 +370,28 @@ __global__ void density_eval_kernel(HashView h, const T* lvals, const T* sums, c
   double b[3][3];
   for (int a = 0; a < 3; ++a) quadratic(double((p[a] - T(c[a]) * hh) / hh), b[a]);
   T value = T(0);
-  for (int k = 0; k < 27; ++k) {
-    int x = k / 9, y = k / 3 % 3, z = k % 3;
-    int t[3] = {c[0] + x - 1, c[1] + y - 1, c[2] + z - 1};
-    if (dmin(t[0], dmin(t[1], t[2])) >= 0 && dmax(t[0], dmax(t[1], t[2])) < n) {
-      int32_t idx = h.find(basis_key(d, t[0], t[1], t[2]));
-      if (idx >= 0) value = value + T(b[0][x] * b[1][y] * b[2][z] * double(lvals[idx]));
+  // per x-plane, the nine first hash probes issued together (collisions resolved after); the
+  // sum still runs in slot order
+  for (int x = 0; x < 3; ++x) {
+    int64_t key9[9];
+    uint64_t h9[9];
+    int32_t idx9[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const int y = q / 3, z = q % 3;
+      const int t[3] = {c[0] + x - 1, c[1] + y - 1, c[2] + z - 1};
+      const bool inside = dmin(t[0], dmin(t[1], t[2])) >= 0 && dmax(t[0], dmax(t[1], t[2])) < n;
+      key9[q] = basis_key(d, t[0], t[1], t[2]);
+      h9[q] = 0;
+      idx9[q] = inside ? h.first_probe(key9[q], h9[q]) : -1;
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q)
+      if (idx9[q] == -2) idx9[q] = h.find_from(key9[q], h9[q]);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const int y = q / 3, z = q % 3;
+      if (idx9[q] >= 0) value = value + T(b[0][x] * b[1][y] * b[2][z] * double(lvals[idx9[q]]));
     }
   }
   dens[i * stride + d] = value;

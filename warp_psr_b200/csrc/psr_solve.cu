@@ -337,19 +337,37 @@ __global__ void prolong_normals_kernel(const int64_t* keys, int64_t n, int d, Ha
   int c[3];
   key_coords(keys[i], c);
   T value[4] = {T(0), T(0), T(0), T(0)};
-  int32_t j = nh.find(keys[i]);
+  // the own record's and the parents' first hash probes issued together, collisions after
+  uint64_t hj = 0;
+  int32_t j = nh.first_probe(keys[i], hj);
+  T wk[8];
+  int64_t key8[8];
+  uint64_t h8[8];
+  int32_t q8[8];
+#pragma unroll
+  for (int corner = 0; corner < 8; ++corner) {
+    int p[3] = {c[0] / 2, c[1] / 2, c[2] / 2};
+    T weight = T(1.0);
+    for (int axis = 0; axis < 3; ++axis) {
+      if ((corner >> axis) & 1) p[axis] += 1;
+      weight = weight * (T(1.0) - fabs(T(c[axis]) * T(0.5) - T(p[axis])));
+    }
+    wk[corner] = weight;
+    key8[corner] = basis_key(d - 1, p[0], p[1], p[2]);
+    h8[corner] = 0;
+    q8[corner] = (d > 0 && weight > T(0)) ? bh.first_probe(key8[corner], h8[corner]) : -1;
+  }
+  if (j == -2) j = nh.find_from(keys[i], hj);
+#pragma unroll
+  for (int corner = 0; corner < 8; ++corner)
+    if (q8[corner] == -2) q8[corner] = bh.find_from(key8[corner], h8[corner]);
   if (j >= 0)
     for (int a = 0; a < 4; ++a) value[a] = nvals[4 * int64_t(j) + a];
   if (d > 0) {
     for (int corner = 0; corner < 8; ++corner) {
-      int p[3] = {c[0] / 2, c[1] / 2, c[2] / 2};
-      T weight = T(1.0);
-      for (int axis = 0; axis < 3; ++axis) {
-        if ((corner >> axis) & 1) p[axis] += 1;
-        weight = weight * (T(1.0) - fabs(T(c[axis]) * T(0.5) - T(p[axis])));
-      }
+      const T weight = wk[corner];
       if (weight > T(0)) {
-        int32_t q = bh.find(basis_key(d - 1, p[0], p[1], p[2]));
+        const int32_t q = q8[corner];
         if (q >= 0) {
           const T* pv = prev + 4 * (int64_t(q) - prev_off);
           for (int a = 0; a < 4; ++a) value[a] = value[a] + pv[a] * weight;
