@@ -1250,12 +1250,6 @@ __global__ void unpermute_kernel(const int32_t* perm, int64_t n, const T* in, T*
   if (p < n) out[perm[p]] = in[p];
 }
 
-template <class T>
-__global__ void narrow_kernel(const T* in, int64_t n, float* out) {
-  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i < n) out[i] = float(in[i]);
-}
-
 // ------------------------------------------------------------------ adjoint tape of the solve
 // What the reverse pass needs from the forward solve, kept only when a reconstruction is
 // differentiable.  Everything is in the forward's own layout.
