@@ -175,13 +175,6 @@ void solve_backward(void* tape, const TreeData& tree, const DensityData<T>& D, c
                     const Params& p, const T* g_coef, std::vector<DBuf<T>>& g_agg, T* g_average, T* g_nvals,
                     cudaStream_t s, EventMarks* marks = nullptr);
 
-// Ordered sliced relaxation on an ELL level (28 slots per row; slot k < 27 is the k-th
-// lexicographic neighbour, -1 absent).  Rows are referenced through `rows` grouped by
-// (x&1) + 2(y&1) + 4z with `group_off` (4*(2^depth+1)+1 entries).
-template <class T, class V>
-void relax_sliced_ell(const int32_t* cols, const T* vals, const V* b, V* x, const int32_t* rows,
-                      const int32_t* group_off, int depth, int iters, cudaStream_t s, float* ms);
-
 // Index rows of the schedule-order operator: 32 slots (0..26 neighbours, 27 own index); the
 // padding slots 28..31 carry 1 / A_ii in the vector precision (write_inv_diag).
 // An absent neighbour in those index rows is the most negative index: its footprint position

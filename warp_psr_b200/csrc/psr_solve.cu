@@ -784,74 +784,6 @@ __device__ __forceinline__ void gs_row(const int32_t* __restrict__ cols, const T
   if (diagonal != T(0)) st_x(x, row, xi + r * (V(1.0) / V(diagonal)));
 }
 
-__device__ __forceinline__ int ld_acquire(const int* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release(int* p, int v) {
-  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Bounded wait: returns false if `*p >= v` did not happen within the iteration limit.
-__device__ __forceinline__ bool wait_geq(const int* p, int v, const int* error) {
-  for (long long it = 0; it < (1LL << 26); ++it) {
-    if (ld_acquire(p) >= v) return true;
-    if ((it & 63) == 63 && *(volatile const int*)error) return false;
-    __nanosleep(it < 256 ? 20 : 200);
-  }
-  return false;
-}
-
-// Persistent dependency-scheduled sliced Gauss-Seidel.  Tasks (slice z, visit t) are taken
-// from a counter in the reference's sequential order (relaxation.py:121-126).  Visit t of
-// slice z waits for visit t of z+1 and visit t-1 of z-1 (relaxation.py:128-135); the four
-// colours of a slice run in order inside one CTA.  Any schedule honouring these edges is
-// bitwise identical to the sequential order.  A task only waits on tasks taken earlier, so
-// the scheme cannot deadlock; every wait is bounded and reports PSR_ETIMEOUT.
-template <class T, class V>
-__global__ void __launch_bounds__(512) sliced_gs_kernel(const int32_t* __restrict__ cols, const T* __restrict__ vals,
-                                                         const V* __restrict__ b, V* x,
-                                                         const int32_t* __restrict__ rows,
-                                                         const int32_t* __restrict__ group_off,
-                                                         const int2* __restrict__ tasks, int ntasks, int nslices,
-                                                         int* progress, int* counter, int* error) {
-  __shared__ int s_task, s_fail;
-  while (true) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      s_task = atomicAdd(counter, 1);
-      s_fail = 0;
-    }
-    __syncthreads();
-    int task = s_task;
-    if (task >= ntasks) return;
-    int z = tasks[task].x, t = tasks[task].y;
-    if (threadIdx.x == 0) {
-      bool ok = true;
-      if (z + 1 < nslices) ok = ok && wait_geq(progress + z + 1, t + 1, error);
-      if (z > 0) ok = ok && wait_geq(progress + z - 1, t, error);
-      ok = ok && wait_geq(progress + z, t, error);
-      if (!ok) {
-        atomicExch(error, 1);
-        s_fail = 1;
-      }
-    }
-    __syncthreads();
-    if (s_fail) return;
-    for (int c = 0; c < 4; ++c) {
-      int g = 4 * z + c;
-      int end = group_off[g + 1];
-      for (int j = group_off[g] + threadIdx.x; j < end; j += blockDim.x) gs_row(cols, vals, b, x, rows[j]);
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-      __threadfence();
-      st_release(progress + z, t + 1);
-    }
-  }
-}
-
 // Eight-colour relaxation of a small level by one CTA (relaxation.py:261-271).  With `hist`
 // (adjoint tape) visit `it` of row i stores (old x, r) at hist[2 * (it * n + i)].
 template <class T>
@@ -1006,54 +938,6 @@ static Schedule make_schedule(const int64_t* keys, int64_t n, int depth, bool sl
   group_offsets_kernel<<<blocks_for(S.groups + 1), kThreads, 0, s>>>(sg.p, n, S.groups, S.off.p);
   PSR_LAUNCH_CHECK();
   return S;
-}
-
-static int sm_count() {
-  static int count = 0;
-  if (!count) {
-    int dev = 0;
-    PSR_CUDA(cudaGetDevice(&dev));
-    PSR_CUDA(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev));
-  }
-  return count;
-}
-
-template <class T, class V>
-void relax_sliced_ell(const int32_t* cols, const T* vals, const V* b, V* x, const int32_t* rows,
-                      const int32_t* group_off, int depth, int iters, cudaStream_t s, float* ms) {
-  if (iters <= 0) return;
-  int n = 1 << depth;
-  std::vector<int2> tasks;
-  for (int front = n; front > -iters; --front)
-    for (int z = std::max(front, 0); z < std::min(front + iters, n + 1); ++z) tasks.push_back(make_int2(z, z - front));
-  int ntasks = int(tasks.size());
-  DBuf<int2> dtasks(ntasks, s);
-  PSR_CUDA(cudaMemcpyAsync(dtasks.p, tasks.data(), ntasks * sizeof(int2), cudaMemcpyHostToDevice, s));
-  DBuf<int> flags(n + 1 + 2, s);
-  flags.zero();
-  int* progress = flags.p;
-  int* counter = flags.p + n + 1;
-  int* error = flags.p + n + 2;
-  int grid = std::min(ntasks, 2 * sm_count());
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (ms) {
-    PSR_CUDA(cudaEventCreate(&e0));
-    PSR_CUDA(cudaEventCreate(&e1));
-    PSR_CUDA(cudaEventRecord(e0, s));
-  }
-  sliced_gs_kernel<T, V><<<grid, 512, 0, s>>>(cols, vals, b, x, rows, group_off, dtasks.p, ntasks, n + 1, progress,
-                                              counter, error);
-  PSR_LAUNCH_CHECK();
-  if (ms) {
-    PSR_CUDA(cudaEventRecord(e1, s));
-  }
-  int err = read_scalar(error, s);
-  if (ms) {
-    PSR_CUDA(cudaEventElapsedTime(ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-  }
-  if (err) throw Error(4, "ordered relaxation: a dependency wait timed out");
 }
 
 // ------------------------------------------------------------------ A10 base solve (solver.py:241-317)
@@ -1719,11 +1603,5 @@ template void solve_levels<double>(const TreeData&, const DensityData<double>&, 
                                    cudaStream_t, SolveStats*, StageSink*, std::shared_ptr<void>*);
 #include "psr_solve_adjoint.cuh"
 
-template void relax_sliced_ell<float, float>(const int32_t*, const float*, const float*, float*, const int32_t*,
-                                             const int32_t*, int, int, cudaStream_t, float*);
-template void relax_sliced_ell<double, double>(const int32_t*, const double*, const double*, double*, const int32_t*,
-                                               const int32_t*, int, int, cudaStream_t, float*);
-template void relax_sliced_ell<float, double>(const int32_t*, const float*, const double*, double*, const int32_t*,
-                                              const int32_t*, int, int, cudaStream_t, float*);
 
 }  // namespace psr
