@@ -16,7 +16,7 @@
 //    float64 stencil loads (normal_loads.py:114-190) like every other profile;
 //  * Galerkin products (warp.sparse.bsr_mm) and root CG dot products use a fixed
 //    sequential order;
-//  * the normal average (normals.py:427-442) and the isovalue (reconstruction.py:77-93)
+//  * the normal average (normals.py:132-163) and the isovalue (reconstruction.py:77-93)
 //    use the fixed blocked orders that the CUDA kernels use (see `blocked_*` below).
 #include <algorithm>
 #include <array>
@@ -72,7 +72,7 @@ inline int64_t find_key(const std::vector<int64_t>& keys, int64_t key) {
   return -1;
 }
 
-// keyed.py:334-340
+// keyed.py:23-30
 inline int64_t morton(const int c[3], int depth) {
   int64_t m = 0;
   for (int bit = 0; bit < depth; ++bit)
@@ -80,7 +80,7 @@ inline int64_t morton(const int c[3], int depth) {
   return m;
 }
 
-// Stable order of `keys` (a stable radix sort in the reference, keyed.py:413-419,435).
+// Stable order of `keys` (a stable radix sort in the reference, keyed.py:102-108,122-124).
 std::vector<int64_t> stable_order(const std::vector<int64_t>& keys) {
   std::vector<int64_t> ids(keys.size());
   std::iota(ids.begin(), ids.end(), 0);
@@ -88,7 +88,7 @@ std::vector<int64_t> stable_order(const std::vector<int64_t>& keys) {
   return ids;
 }
 
-// keyed.py:422-453 — sort records by key (stable), sum each key's values in record order.
+// keyed.py:66-94,111-142 — sort records by key (stable), sum each key's values in record order.
 template <class T>
 void reduce_records(const std::vector<int64_t>& keys, const std::vector<T>& values /* 4 per record */,
                     std::vector<int64_t>& out_keys, std::vector<T>& out_values) {
@@ -424,7 +424,7 @@ Density<T> build_density(const Samples<T>& s, int depth, int kernel_depth, doubl
   return D;
 }
 
-// ---------------------------------------------------------------- A3 normals (normals.py:311-524)
+// ---------------------------------------------------------------- A3 normals (normals.py:33-245)
 // Fixed blocked order shared with the CUDA kernel: blocks of 1024 contributions summed
 // serially (in T, input order) inside a block, then the block totals serially.
 template <class T>
@@ -446,11 +446,11 @@ Normals<T> build_normal_field(const Samples<T>& s, const Density<T>& D, int mini
   Normals<T> N;
   size_t n = s.keys.size();
   std::vector<int64_t> fk(s.first.begin(), s.first.end());
-  auto order = stable_order(fk);  // normals.py:468-477
+  auto order = stable_order(fk);  // normals.py:36-43,192-202
   std::vector<int64_t> rk(54 * n, kInvalid);
   std::vector<T> rv(4 * 54 * n, T(0));
 #pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < int64_t(n); ++i) {  // normals.py:325-383
+  for (int64_t i = 0; i < int64_t(n); ++i) {  // normals.py:46-104
     int64_t src = order[i];
     T w = s.weights[src];
     T nm[3] = {s.normal_sums[3 * src] / w, s.normal_sums[3 * src + 1] / w, s.normal_sums[3 * src + 2] / w};
@@ -490,8 +490,8 @@ Normals<T> build_normal_field(const Samples<T>& s, const Density<T>& D, int mini
     }
   }
   reduce_records(rk, rv, N.keys, N.values);
-  for (auto& v : N.values) v = -v;  // normals.py:385-388
-  std::vector<T> contrib(3 * n, T(0));  // normals.py:411-425
+  for (auto& v : N.values) v = -v;  // normals.py:106-110,219-221
+  std::vector<T> contrib(3 * n, T(0));  // normals.py:132-147
   for (size_t i = 0; i < n; ++i) {
     int64_t src = order[i];
     T w = s.weights[src];
@@ -510,7 +510,7 @@ Normals<T> build_normal_field(const Samples<T>& s, const Density<T>& D, int mini
     N.average[1] = total[1] / total[2];
     N.average[2] = total[2];
   }
-  N.offsets.resize(maximum + 2);  // normals.py:296-308
+  N.offsets.resize(maximum + 2);  // normals.py:17-31,228-232
   for (int d = 0; d <= maximum + 1; ++d)
     N.offsets[d] = size_t(std::lower_bound(N.keys.begin(), N.keys.end(), int64_t(d) << 48) - N.keys.begin());
   return N;
@@ -594,7 +594,7 @@ Tree build_tree(const Normals<T>& N, int depth, int full_depth, int base_depth) 
 }
 
 // ---------------------------------------------------------------- A5 operators
-// stiffness.py:285-306 1-D hat mass/stiffness integrals (float64)
+// stiffness.py:14-36 1-D hat mass/stiffness integrals (float64)
 void hat_integrals(int depth, int index, int trial_depth, int trial_index, double out[2]) {
   int resolution = 1 << depth;
   int ratio = 1 << (depth - trial_depth);
@@ -614,7 +614,7 @@ void hat_integrals(int depth, int index, int trial_depth, int trial_index, doubl
   }
 }
 
-// stiffness.py:309-380 — CSR rows in lexicographic neighbour order, float64 values.
+// stiffness.py:38-108 — CSR rows in lexicographic neighbour order, float64 values.
 Csr<double> level_stiffness(const std::vector<int64_t>& rows, const std::vector<int64_t>& cols, int depth,
                             int trial_depth) {
   Csr<double> A;
@@ -672,7 +672,7 @@ struct Points {
   std::vector<int64_t> bin_ids;
 };
 
-// constraints.py:187-251
+// constraints.py:20-84
 template <class T>
 Points<T> point_constraints(const Density<T>& D, const Normals<T>& N, const Tree& tree, int depth, double pw,
                             bool exact) {
@@ -764,7 +764,7 @@ std::vector<double> add_screening(Csr<double>& A, const std::vector<int64_t>& ro
   return load;
 }
 
-// ---------------------------------------------------------------- A9 transfers (transfer_stencils.py:116-167)
+// ---------------------------------------------------------------- A9 transfers (transfer_stencils.py:12-66)
 template <class T>
 Csr<T> prolongation(const std::vector<int64_t>& coarse, const std::vector<int64_t>& fine, int depth) {
   Csr<T> P;
@@ -889,7 +889,7 @@ inline int normal_center(int index, int test_depth, int normal_depth) {  // norm
   return index;
 }
 
-// normal_stencils.py:210-260
+// normal_stencils.py:11-70
 template <class T>
 std::vector<double> normal_stencil(const std::vector<int64_t>& keys, const int64_t* nkeys, const T* nvals, size_t nrec,
                                    int test_depth, int normal_depth) {
@@ -1339,7 +1339,7 @@ void evaluate_query(const std::vector<int64_t>& keys, const T* coeff, const T* c
 }
 
 template <class T>
-T det3(const T m[9]) {  // transforms.py:216-222
+T det3(const T m[9]) {  // transforms.py:16-22
   return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) + m[2] * (m[3] * m[7] - m[4] * m[6]);
 }
 template <class T>
@@ -1359,7 +1359,7 @@ T minor4(const T m[16], int row, int col) {
   return det3(out);
 }
 template <class T>
-void reference_inverse(const T m[16], T out[16]) {  // transforms.py:238-253
+void reference_inverse(const T m[16], T out[16]) {  // transforms.py:38-53
   T det = T(0);
   for (int c = 0; c < 4; ++c) {
     if (c % 2 == 0)
@@ -1521,7 +1521,7 @@ Result<T>* reconstruct(const T* pos, const T* nrm, int64_t count, const Params& 
   double total, mass;
   blocked_isovalue(values, S.weights, total, mass);
   R->iso = T(total / mass);
-  T s = S.transform[0];  // transforms.py:255-280
+  T s = S.transform[0];  // transforms.py:55-79
   T m[16] = {T(0), s, T(0), S.transform[1], T(0), T(0), s, S.transform[2], s, T(0), T(0), S.transform[3],
              T(0), T(0), T(0), T(1)};
   reference_inverse(m, R->transforms[0]);

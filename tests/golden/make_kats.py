@@ -13,7 +13,7 @@ Each record keeps what pins the path without PoissonRecon or Warp being runnable
 Only fixtures whose inputs are regenerable from a seeded shape are kept
 (``external`` inputs are dropped).  Usage::
 
-    python tests/golden/make_kats.py /root/reference/docs/results > tests/golden/kats.json
+    python tests/golden/make_kats.py <warp-psr checkout>/docs/results > tests/golden/kats.json
 """
 import json
 import sys

@@ -301,7 +301,7 @@ __global__ void morton_kernel(const int64_t* keys, int64_t n, int d, uint64_t* c
   if (i >= n) return;
   int c[3];
   key_coords(keys[i], c);
-  uint64_t m = 0;  // keyed.py:334-340
+  uint64_t m = 0;  // keyed.py:23-30
   for (int bit = 0; bit < d; ++bit)
     for (int a = 0; a < 3; ++a) m |= uint64_t((c[a] >> bit) & 1) << (3 * bit + a);
   codes[i] = m;
@@ -521,7 +521,7 @@ DensityData<T> build_density(const SampleGroups<T>& g, int depth, int kernel_dep
   return D;
 }
 
-// ------------------------------------------------------------------ A3 normals.py:311-524
+// ------------------------------------------------------------------ A3 normals.py:33-245
 __global__ void first_keys_kernel(const int32_t* first, int64_t n, uint32_t* keys, int32_t* ids) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
@@ -529,7 +529,7 @@ __global__ void first_keys_kernel(const int32_t* first, int64_t n, uint32_t* key
   ids[i] = int32_t(i);
 }
 
-// normals.py:325-383 — 54 records per group: two 27-node degree-2 splats on the same
+// normals.py:46-104 — 54 records per group: two 27-node degree-2 splats on the same
 // node `top` (issue #12), weighted by dx and 1-dx.
 template <class T>
 __global__ void normal_splat_kernel(const int32_t* order, int64_t n, const T* sums, const T* nsums, const T* weights,
@@ -598,11 +598,11 @@ __global__ void normal_reduce_kernel(const uint64_t* keys, const int32_t* order,
   }
   uint64_t mask = (uint64_t(1) << D) - 1;
   out_keys[g] = basis_key(int(k >> (3 * D)), int((k >> (2 * D)) & mask), int((k >> D) & mask), int(k & mask));
-  for (int a = 0; a < 3; ++a) out_values[4 * g + a] = -acc[a];  // normals.py:385-388
+  for (int a = 0; a < 3; ++a) out_values[4 * g + a] = -acc[a];  // normals.py:106-110,219-221
   out_values[4 * g + 3] = -T(0);
 }
 
-// normals.py:411-425 contributions (raw depth * w, splat weight * w, w) in first-index
+// normals.py:132-147 contributions (raw depth * w, splat weight * w, w) in first-index
 // order; zero for groups whose mean normal vanishes.
 template <class T>
 __global__ void average_contrib_kernel(const int32_t* order, int64_t n, const T* nsums, const T* weights, const T* dw,

@@ -70,7 +70,7 @@ __global__ void normal_splat_reverse_kernel(const int32_t* order, int64_t n, con
     const T fraction = k < 27 ? dx : T(1.0) - dx;
     const int q = k % 27, x = q / 9, y = q / 3 % 3, z = q % 3;
     const T bw = T(b[0][x] * b[1][y] * b[2][z]);
-    // records are negated when reduced (normals.py:385-388)
+    // records are negated when reduced (normals.py:106-110,219-221)
     const T gr[3] = {-g_nvals[4 * int64_t(slot)], -g_nvals[4 * int64_t(slot) + 1], -g_nvals[4 * int64_t(slot) + 2]};
     const T G = gr[0] * nmw[0] + gr[1] * nmw[1] + gr[2] * nmw[2];
     for (int a = 0; a < 3; ++a) g_nmw[a] = g_nmw[a] + gr[a] * sw * inv_h3 * fraction * bw;

@@ -16,7 +16,7 @@ namespace psr {
 constexpr int kSlots = 28;
 
 // ------------------------------------------------------------------ 1-D integral tables
-// stiffness.py:285-306 — mass (.x) and stiffness (.y) integrals of Neumann hats.
+// stiffness.py:14-36 — mass (.x) and stiffness (.y) integrals of Neumann hats.
 __device__ void hat_integrals(int depth, int index, int trial_depth, int trial_index, double out[2]) {
   int resolution = 1 << depth;
   int ratio = 1 << (depth - trial_depth);
@@ -202,7 +202,7 @@ __device__ __forceinline__ uint32_t neighbours27(const ColumnView& cv, int d, co
   return present;
 }
 
-// ------------------------------------------------------------------ A6 normal loads (normal_stencils.py:210-260)
+// ------------------------------------------------------------------ A6 normal loads (normal_stencils.py:11-70)
 // `nvals` are 4-wide normal coefficients indexed by (hash result - noff).
 template <class T>
 __global__ void __launch_bounds__(256, 6) normal_stencil_kernel(const int64_t* keys, int64_t n, int test_depth, int normal_depth, ColumnView cv,
@@ -409,7 +409,7 @@ __global__ void add3_kernel(const double* same, const double* finer, const doubl
   out[i] = parent ? parent[i] + v : v;
 }
 
-// ------------------------------------------------------------------ A5 point constraints (constraints.py:187-251)
+// ------------------------------------------------------------------ A5 point constraints (constraints.py:20-84)
 template <class T>
 __global__ void points_kernel(const int64_t* keys, const T* vals, int64_t m, int d, T pw, const T* average,
                               HashView support, bool exact, T* pos, T* w, uint64_t* bin_keys, int32_t* ids) {
@@ -553,7 +553,7 @@ __device__ __forceinline__ double screening_row(const PointsView<T>& P, const in
 }
 
 // ------------------------------------------------------------------ A5/A7 level assembly
-// Same-level operator rows (stiffness.py:309-380 + screening) and b = T(load) + 0.5*T(point load).
+// Same-level operator rows (stiffness.py:38-108 + screening) and b = T(load) + 0.5*T(point load).
 template <class T, bool SCREEN>
 __global__ void assemble_level_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t off,
                                       const double* table, PointsView<T> P, const double* load, int32_t* cols,
@@ -681,7 +681,7 @@ __global__ void __launch_bounds__(128, 8) cross_apply_kernel(const int64_t* keys
   b[p] = -s + b[p];
 }
 
-// ------------------------------------------------------------------ A9 transfers (transfer_stencils.py:116-151)
+// ------------------------------------------------------------------ A9 transfers (transfer_stencils.py:12-66)
 template <class T>
 __global__ void prolongation_kernel(const int64_t* fine, int64_t n, int d, HashView bh, int64_t coff, int32_t* pcol,
                                     T* pval) {
