@@ -44,7 +44,7 @@ enum { PSR_FLOAT32 = 0, PSR_FLOAT64 = 1 };
 /* Solve precision.  PSR_PRECISION_INPUT follows the input dtype exactly like the reference
  * (float32 in, float32 solve; float64 in, float64 solve).  PSR_PRECISION_MIXED keeps
  * float32 operator storage and runs the vector arithmetic of the ordered relaxation in
- * float64 (see DESIGN notes in the package). */
+ * float64: coefficients are float64, the relaxation reads half the operator bytes. */
 enum { PSR_PRECISION_INPUT = 0, PSR_PRECISION_MIXED = 1 };
 
 /* reconstruct() keyword arguments (reconstruction.py:137-153); all fields required. */
@@ -68,7 +68,7 @@ typedef struct psr_info {
   int64_t basis_counts[16]; /* active basis functions per depth (0 beyond depth) */
   int64_t support_counts[16];
   double iso_value;
-  double cube_to_model[16]; /* row-major 4x4 (transforms.py:255-280, first matrix) */
+  double cube_to_model[16]; /* row-major 4x4 (transforms.py:55-79, first matrix) */
   double model_to_cube[16]; /* row-major 4x4 (second matrix) */
   double stage_ms[8];       /* samples, density, normal_field, tree, assembly_and_solve, field, isovalue, total */
   double relax_ms;          /* device time of the ordered sliced relaxation kernels (CUDA events) */
@@ -90,17 +90,21 @@ typedef struct psr_arrays {
   const int64_t* support_keys[16]; /* signed tree keys of each depth's non-ghost support (device) */
 } psr_arrays;
 
-/* Zero-copy handle mirroring warp-psr's DeviceField struct (device_field.py:19-28). */
+/* Zero-copy handle mirroring warp-psr's DeviceField struct (device_field.py:19-28), passed
+ * by value to CUDA kernels that evaluate the field with psr_evaluate_field (psr_field.cuh). */
 typedef struct psr_field_handle {
-  const int64_t* keys;
-  const void* coefficients;
-  const void* cumulative;
-  int64_t count;
+  const int64_t* keys;      /* sorted basis keys of all levels (device) */
+  const void* coefficients; /* per-level corrections, dtype (device) */
+  const void* cumulative;   /* cumulative coefficients, dtype (device); NULL = direct evaluation */
+  int64_t count;            /* keys */
   double linear[9];         /* model -> unit cube, row-major */
   double translation[3];
   int32_t depth;
   int32_t dtype;
   double iso_value;
+  const void* hash_slots;   /* open-addressing table of {int64 key, int64 index} slots, key -1 = empty
+                               (device); NULL = binary search of keys */
+  uint64_t hash_mask;       /* slots - 1 (a power of two minus one) */
 } psr_field_handle;
 
 int psr_reconstruct(const void* positions, const void* normals, int64_t n, int32_t dtype, const psr_params* params,
@@ -137,9 +141,10 @@ int psr_isovalue(int32_t dtype, const void* values, const void* weights, int64_t
  * pool already holds the device memory, real-time loops that must not allocate).  Its
  * scratch is a fixed 64 KiB array in the library's device image, held by every GPU that
  * loads the library until the process exits; n is limited to 4,194,304 values (PSR_EINVAL
- * beyond).  The first call on a device looks up that array's address (no allocation); make
- * it before any stream capture.  All calls share the array, so calls that overlap on the
- * GPU (e.g. on different streams) race; results are stream-ordered, no synchronisation. */
+ * beyond).  Every call looks up that array's address in the current context (no
+ * allocation); the first call on a device also loads the library's module, so make it
+ * before any stream capture.  All calls share the array, so calls that overlap on the GPU
+ * (e.g. on different streams) race; results are stream-ordered, no synchronisation. */
 int psr_isovalue_static(int32_t dtype, const void* values, const void* weights, int64_t n, void* out, void* stream);
 
 /* Reverse pass of a reconstruction made with params.differentiable (warp-psr

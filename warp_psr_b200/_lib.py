@@ -50,6 +50,7 @@ class FieldHandle(ctypes.Structure):
         ("keys", ctypes.c_void_p), ("coefficients", ctypes.c_void_p), ("cumulative", ctypes.c_void_p),
         ("count", ctypes.c_int64), ("linear", ctypes.c_double * 9), ("translation", ctypes.c_double * 3),
         ("depth", ctypes.c_int32), ("dtype", ctypes.c_int32), ("iso_value", ctypes.c_double),
+        ("hash_slots", ctypes.c_void_p), ("hash_mask", ctypes.c_uint64),
     ]
 
 

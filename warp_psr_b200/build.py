@@ -30,7 +30,7 @@ def nvcc():
 
 def _compile(src, verbose):
     obj = OUT / (src.stem + ".o")
-    deps = list(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "psr_b200.h", src]
+    deps = list(CSRC.glob("*.cuh")) + list((HERE.parent / "include").glob("*.h*")) + [src]
     if obj.exists() and obj.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
         return obj, ""
     cmd = [nvcc(), *ARCH, *FLAGS, "-c", str(src), "-o", str(obj)]
@@ -55,6 +55,23 @@ def build(verbose=False):
         if res.returncode:
             raise RuntimeError(f"link failed:\n{res.stderr}")
     return LIB
+
+
+INCLUDE = HERE.parent / "include"
+
+
+def build_user_library(sources, output, extra_flags=()):
+    """Compiles CUDA sources of an application that evaluates reconstructed fields inside its
+    own kernels (``#include "psr_field.cuh"``, then ``psr_evaluate_field(handle, x, y, z)``)
+    into a shared library for sm_100a.  The application's own flags apply (FMA contraction
+    stays on by default); the header's arithmetic does not depend on them.  Returns the path."""
+    output = Path(output)
+    cmd = [nvcc(), *ARCH, "-std=c++17", "-O3", "-lineinfo", "-I", str(INCLUDE), "-Xcompiler", "-fPIC", "-shared",
+           *map(str, sources), "-o", str(output), *extra_flags]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode:
+        raise RuntimeError(f"nvcc failed:\n{res.stderr}")
+    return output
 
 
 if __name__ == "__main__":

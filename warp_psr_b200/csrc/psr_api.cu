@@ -552,6 +552,9 @@ int psr_device_field(const psr_result* R, psr_field_handle* h) {
   h->depth = R->depth;
   h->dtype = R->dtype;
   h->iso_value = R->iso;
+  const HashView hv = R->hash.view();
+  h->hash_slots = hv.slots;
+  h->hash_mask = hv.mask;
   return PSR_OK;
 }
 

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
+#include "../../include/psr_field.cuh"
+
 #include <atomic>
 #include <cstdint>
 #include <cstdlib>
@@ -183,14 +185,8 @@ struct HashView {
       if (e.x == -1) return -1;
     }
   }
-  __host__ __device__ static __forceinline__ uint64_t mix(uint64_t x) {
-    x ^= x >> 31;
-    x *= 0x7fb5d329728ea185ULL;
-    x ^= x >> 27;
-    x *= 0x81dadef4bc2dd44dULL;
-    x ^= x >> 33;
-    return x;
-  }
+  // the mixer of psr_field.cuh, so kernels outside the library probe the same tables
+  __host__ __device__ static __forceinline__ uint64_t mix(uint64_t x) { return psr_field::hash_mix(x); }
 };
 
 __global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, longlong2* slots, uint64_t mask,

@@ -1,10 +1,10 @@
 // A11/A12: cumulative coefficients, field evaluation, isovalue and evaluation transforms
-// (warp-psr field.py:187-421, reconstruction.py:18-116, transforms.py:211-280).
+// (warp-psr field.py:187-421, reconstruction.py:18-116, transforms.py:11-86).
 #include "../../include/psr_b200.h"
 #include "psr_internal.cuh"
 
 #include <algorithm>
-#include <mutex>
+#include <exception>
 
 namespace psr {
 
@@ -42,47 +42,26 @@ void cumulative_coefficients(const int64_t* keys, const std::vector<int64_t>& of
   }
 }
 
-// field.py:370-393 — one level's contribution: left-owned neighbour cell, right-owned piece.
+// The per-query evaluation (field.py:365-421) is psr_field.cuh's, the same code user
+// kernels include, so psr_evaluate and psr_evaluate_field agree bit for bit.
 template <class T>
-__device__ __forceinline__ void add_level(const HashView& h, const T* coeff, const T p[3], int d, T r[4]) {
-  int n = 1 << d;
-  T t[3], f[3];
-  int cell[3], base[3];
-  for (int a = 0; a < 3; ++a) {
-    t[a] = p[a] * T(n);
-    cell[a] = min(max(int(ceil(t[a])) - 1, 0), n - 1);
-    base[a] = int(floor(t[a]));
-    f[a] = t[a] - T(base[a]);
-  }
-  for (int corner = 0; corner < 8; ++corner) {
-    int node[3] = {cell[0] + corner / 4, cell[1] + (corner / 2) % 2, cell[2] + corner % 2};
-    if (min(node[0] - base[0], min(node[1] - base[1], node[2] - base[2])) < 0) continue;
-    int32_t idx = h.find(basis_key(d, node[0], node[1], node[2]));
-    if (idx < 0) continue;
-    T hh[3], sg[3];
-    for (int a = 0; a < 3; ++a) {
-      hh[a] = T(1) - f[a];
-      sg[a] = T(-1);
-      if (node[a] > base[a]) {
-        hh[a] = f[a];
-        sg[a] = T(1);
-      }
-    }
-    T c = coeff[idx];
-    r[0] = r[0] + c * hh[0] * hh[1] * hh[2];
-    r[1] = r[1] + c * T(n) * sg[0] * hh[1] * hh[2];
-    r[2] = r[2] + c * T(n) * hh[0] * sg[1] * hh[2];
-    r[3] = r[3] + c * T(n) * hh[0] * hh[1] * sg[2];
-  }
+__device__ __forceinline__ psr_field::View<T> field_view(const HashView& h, const int64_t* keys, const T* coeff,
+                                                        const T* cumulative, int depth) {
+  return psr_field::View<T>{keys, coeff, cumulative, 0, h.slots, h.mask, depth};
 }
 
-// field.py:395-421 reference evaluation kernel.  In the cube frame (centroids of the
-// reconstruction's isovalue, reconstruction.py:273-280) the query is sums/weights and the
-// transform is the identity.
 template <class T>
-__global__ void evaluate_kernel(const HashView h, const T* coeff, const T* cumulative, const T* queries, int64_t nq,
-                                const T* linear, const T* translation, int depth, T* values, T* gradients,
-                                int32_t* valid, int cube_frame, const T* gsums, const T* gweights) {
+__device__ __forceinline__ void add_level(const HashView& h, const T* coeff, const T p[3], int d, T r[4]) {
+  psr_field::add_level(field_view<T>(h, nullptr, coeff, coeff, d), coeff, p, d, r);
+}
+
+// Model-frame queries, or (cube_frame) the centroids of the isovalue, q = sums / weights
+// with the identity transform (reconstruction.py:273-280).
+template <class T>
+__global__ void evaluate_kernel(const HashView h, const int64_t* keys, const T* coeff, const T* cumulative,
+                                const T* queries, int64_t nq, const T* linear, const T* translation, int depth,
+                                T* values, T* gradients, int32_t* valid, int cube_frame, const T* gsums,
+                                const T* gweights) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= nq) return;
   T L[9], tr[3], q[3];
@@ -96,60 +75,21 @@ __global__ void evaluate_kernel(const HashView h, const T* coeff, const T* cumul
     for (int a = 0; a < 3; ++a) tr[a] = translation[a];
     for (int a = 0; a < 3; ++a) q[a] = queries[3 * i + a];
   }
-  T p[3];
-  for (int r = 0; r < 3; ++r) p[r] = L[3 * r] * q[0] + L[3 * r + 1] * q[1] + L[3 * r + 2] * q[2] + tr[r];
-  bool ok = isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]) && dmin(p[0], dmin(p[1], p[2])) >= T(0) &&
-            dmax(p[0], dmax(p[1], p[2])) <= T(1);
-  if (valid) valid[i] = ok;
-  if (!ok) {
-    T nan = T(NAN);
-    values[i] = nan;
-    if (gradients)
-      for (int a = 0; a < 3; ++a) gradients[3 * i + a] = nan;
-    return;
-  }
-  int leaf = 0;
-  for (int d = depth; d >= 0; --d) {
-    int n = 1 << d;
-    int c[3];
-    for (int a = 0; a < 3; ++a) c[a] = min(max(int(ceil(p[a] * T(n))) - 1, 0), n - 1);
-    if (h.find(basis_key(d, c[0], c[1], c[2])) >= 0) {
-      leaf = d;
-      break;
-    }
-  }
-  for (int a = 0; a < 3; ++a) {
-    if (p[a] == T(0))
-      p[a] = T(1e-6);
-    else if (p[a] == T(1))
-      p[a] = T(1.0 - 1e-6);
-  }
-  T r[4] = {T(0), T(0), T(0), T(0)};
-  add_level(h, coeff, p, leaf, r);
-  if (leaf > 0) {
-    T s[4] = {T(0), T(0), T(0), T(0)};
-    add_level(h, cumulative, p, leaf - 1, s);
-    for (int a = 0; a < 4; ++a) r[a] = r[a] + s[a];
-  }
-  if (leaf < depth) {
-    T s[4] = {T(0), T(0), T(0), T(0)};
-    add_level(h, coeff, p, leaf + 1, s);
-    for (int a = 0; a < 4; ++a) r[a] = r[a] + s[a];
-  }
-  values[i] = r[0];
+  const psr_field::Result<T> r = psr_field::evaluate(field_view<T>(h, keys, coeff, cumulative, depth), L, tr, q);
+  if (valid) valid[i] = r.valid;
+  values[i] = r.value;
   if (gradients)
-    for (int a = 0; a < 3; ++a) gradients[3 * i + a] = L[a] * r[1] + L[3 + a] * r[2] + L[6 + a] * r[3];
+    for (int a = 0; a < 3; ++a) gradients[3 * i + a] = r.gradient[a];
 }
 
 template <class T>
 void evaluate_queries(const int64_t* keys, const HashView& h, const T* coeff, const T* cumulative, const T* queries,
                       int64_t nq, const T* linear, const T* translation, int depth, T* values, T* gradients,
                       int32_t* valid, bool cube_frame, const T* group_sums, const T* group_weights, cudaStream_t s) {
-  (void)keys;
   if (nq <= 0) return;
-  evaluate_kernel<T><<<blocks_for(nq, 128), 128, 0, s>>>(h, coeff, cumulative, queries, nq, linear, translation, depth,
-                                                         values, gradients, valid, cube_frame ? 1 : 0, group_sums,
-                                                         group_weights);
+  evaluate_kernel<T><<<blocks_for(nq, 128), 128, 0, s>>>(h, keys, coeff, cumulative, queries, nq, linear, translation,
+                                                         depth, values, gradients, valid, cube_frame ? 1 : 0,
+                                                         group_sums, group_weights);
   PSR_LAUNCH_CHECK();
 }
 
@@ -208,7 +148,7 @@ void isovalue(const T* values, const T* weights, int64_t n, T* out, cudaStream_t
   PSR_LAUNCH_CHECK();
 }
 
-// transforms.py:216-280 — cofactor inverse of the cube->model matrix, applied twice.
+// transforms.py:16-79 — cofactor inverse of the cube->model matrix, applied twice.
 template <class T>
 __device__ T det3(const T m[9]) {
   return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) + m[2] * (m[3] * m[7] - m[4] * m[6]);
@@ -272,28 +212,22 @@ void evaluation_transforms(const T* normalization, T* transforms, cudaStream_t s
 constexpr int64_t kStaticIsoBlocks = 4096;  // at most 4096 * 1024 = 4,194,304 values per call
 static __device__ __align__(256) double g_iso_scratch[2 * kStaticIsoBlocks];
 
-// Device address of g_iso_scratch for the current device, looked up once per device (the
-// host-side name is only a stand-in for the device array and must not be passed to kernels).
+// Device address of g_iso_scratch in the current context.  The host-side name is only a
+// stand-in for the device array and must not be passed to kernels.  The address belongs to
+// the context that loaded this library's module, so it is looked up on every call (no
+// allocation): a cached address would go stale after cudaDeviceReset or under a context the
+// caller made current itself.  The first call on a device also loads the module.
 static double* static_iso_scratch() {
-  static std::mutex lock;
-  static double* ptrs[64] = {nullptr};
-  int dev = 0;
-  PSR_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) throw Error(1, "device ordinal out of range for the static isovalue scratch");
-  std::lock_guard<std::mutex> guard(lock);
-  if (!ptrs[dev]) {
-    void* p = nullptr;
-    PSR_CUDA(cudaGetSymbolAddress(&p, g_iso_scratch));
-    ptrs[dev] = static_cast<double*>(p);
-  }
-  return ptrs[dev];
+  void* p = nullptr;
+  PSR_CUDA(cudaGetSymbolAddress(&p, g_iso_scratch));
+  return static_cast<double*>(p);
 }
 
 template <class T>
 static void isovalue_static(const T* values, const T* weights, int64_t n, T* out, cudaStream_t s) {
   const int64_t blocks = (n + 1023) / 1024;
   if (blocks > kStaticIsoBlocks)
-    throw Error(1, "psr_isovalue_static: at most 4,194,304 values per call (use psr_isovalue beyond that)");
+    throw Error(PSR_EINVAL, "psr_isovalue_static: at most 4,194,304 values per call (use psr_isovalue beyond that)");
   double* partial = static_iso_scratch();
   // Each block writes its own two partial sums before the finishing kernel reads exactly
   // `blocks` of them, so no slot has to start at zero.
@@ -551,5 +485,8 @@ extern "C" int psr_isovalue_static(int32_t dtype, const void* values, const void
   } catch (const psr::Error& e) {
     psr::set_last_error(e.what());
     return e.code;
+  } catch (const std::exception& e) {
+    psr::set_last_error(e.what());
+    return PSR_ECUDA;
   }
 }
