@@ -80,6 +80,8 @@ struct StripLevel {
   int64_t rows;              // rows of the level
   int iters;                 // visits per slice
   int record_increment;      // hist holds the update r / A_ii (else the new x)
+  int poll_log2;             // a dependency wait gives up after 2^poll_log2 polls
+  int stall;                 // test override: the newest-slice wait targets a count nothing reaches
 };
 
 __device__ __forceinline__ long long globaltimer() {
@@ -94,8 +96,9 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
   return v;
 }
 
-__device__ __forceinline__ bool wait_at_least(const int* p, int v, const int* error) {
-  for (long long it = 0; it < (1LL << 26); ++it) {
+__device__ __forceinline__ bool wait_at_least(const int* p, int v, const int* error, int poll_log2) {
+  const long long limit = 1LL << poll_log2;
+  for (long long it = 0; it < limit; ++it) {
     if (ld_acquire(p) >= v) return true;
     if ((it & 63) == 63 && *(volatile const int*)error) return false;
     __nanosleep(it < 512 ? 32 : 256);
@@ -354,7 +357,7 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
       // slice z after visit t-1 (two waves back); the newer dependencies are awaited below
       // while this slice is staged
       bool ok = !s_fail;
-      if (ok) ok = wait_at_least(L.done + z * kPad, t * L.strips, L.error);
+      if (ok) ok = wait_at_least(L.done + z * kPad, t * L.strips, L.error, L.poll_log2);
       if (!ok) {
         atomicCAS(L.error, 0, 1);
         s_fail = 1;
@@ -392,8 +395,10 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
       if (warp == 0) {
         if (lane == 0) {
           bool ok = true;
-          if (z + 1 <= L.n) ok = wait_at_least(L.done + (z + 1) * kPad, (t + 1) * L.strips, L.error);
-          if (ok && z > 0) ok = wait_at_least(L.done + (z - 1) * kPad, t * L.strips, L.error);
+          if (z + 1 <= L.n)
+            ok = wait_at_least(L.done + (z + 1) * kPad, (t + 1) * L.strips + (L.stall ? (1 << 30) : 0), L.error,
+                               L.poll_log2);
+          if (ok && z > 0) ok = wait_at_least(L.done + (z - 1) * kPad, t * L.strips, L.error, L.poll_log2);
           if (!ok) {
             atomicCAS(L.error, 0, 1);
             s_fail = 1;
@@ -679,6 +684,14 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
   int* caps_dev = flags.p + pad_end + 2 * kPad;
   DBuf<int32_t> bounds;
   std::vector<int> caps;
+  // 16-bit index rows reach the footprint through offsets below 2^15 (idx_absent).
+  // PSR_RELAX_FOOTPRINT_LIMIT lowers that bound (test override: the strip narrowing below,
+  // which only very large levels need, on small levels).
+  int fp_limit = 32767;
+  if (const char* env = std::getenv("PSR_RELAX_FOOTPRINT_LIMIT")) {
+    const int forced = std::atoi(env);
+    if (forced >= 1 && forced < fp_limit) fp_limit = forced;
+  }
   while (true) {
     bounds.alloc(int64_t(n + 1) * (strips + 1), s);
     strip_bounds_kernel<<<blocks_for(int64_t(n + 1) * (strips + 1)), kThreads, 0, s>>>(xstart.p, n, strips,
@@ -689,12 +702,11 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
                                                                         rev ? 1 : 0, caps_dev);
     PSR_LAUNCH_CHECK();
     caps = read_vector(caps_dev, 3, s);
-    // 16-bit index rows reach the footprint through offsets below 2^15 (idx_absent): narrow
-    // the strips until the largest footprint fits.
-    if (sizeof(I) == 4 || caps[0] <= 32767 || strips >= 256) break;
+    // narrow the strips until the largest footprint fits the 16-bit offsets
+    if (sizeof(I) == 4 || caps[0] <= fp_limit || strips >= 256) break;
     strips = std::min(256, 2 * strips);
   }
-  if (sizeof(I) == 2 && caps[0] > 32767)
+  if (sizeof(I) == 2 && caps[0] > fp_limit)
     throw Error(4, "ordered relaxation: a strip footprint exceeds the 16-bit index range");
   const int maxfp = caps[0], maxrows = caps[1], maxb = caps[2];
   // Slice-visits in wave order (relaxation.py:128-143): wave q = 2t + n - z holds slices two
@@ -727,6 +739,15 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
   L.rows = rows;
   L.iters = iters;
   L.record_increment = record_increment ? 1 : 0;
+  L.poll_log2 = 26;
+  // PSR_RELAX_STALL_TEST=1 (tests of the timeout path): every wait on the newest slice waits
+  // for a count that no task publishes and gives up after 4096 polls, so the launch ends with
+  // PSR_ETIMEOUT without a fault and the context stays usable.
+  if (const char* env = std::getenv("PSR_RELAX_STALL_TEST"))
+    if (std::atoi(env) == 1) {
+      L.stall = 1;
+      L.poll_log2 = 12;
+    }
   // Shared memory: the footprint, plus the staged rows of tasks that fit.
   const int64_t budget = std::min<int64_t>(device_smem_optin() - 4096, 220 * 1024);
   // the footprint plus its +0 entry at index `total`
@@ -736,6 +757,12 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
   L.cap = std::max(maxfp, 1);
   int64_t rc = std::min<int64_t>(maxrows, (budget - fp_bytes - 4 * 16) / per_row);
   rc = std::max<int64_t>(rc, 0);
+  // PSR_RELAX_ROW_CAP caps the staged rows per task (test override: 0 sends every task down
+  // the global-memory row path that only tasks too large for shared memory take).
+  if (const char* env = std::getenv("PSR_RELAX_ROW_CAP")) {
+    const int forced = std::atoi(env);
+    if (forced >= 0) rc = std::min<int64_t>(rc, forced);
+  }
   L.row_cap = int(rc);
   L.b_cap = int(std::min<int64_t>(maxb, rc + 4 * per16) / per16 * per16);
   int64_t smem = fp_bytes + rc * (kSlotsR * int64_t(sizeof(T)) + kIdxSlots * int64_t(sizeof(I))) +
