@@ -1,9 +1,10 @@
 """Full CUDA reconstruction vs the CPU oracle and the reference's known answers.
 
-Integer results (tree keys, group keys, normal record keys) must be identical; floating
-point stages must agree with the oracle within the tolerances below, which are a few ulps
-of the input precision (both sides follow the same arithmetic order; transcendental
-library calls may differ by an ulp).
+Integer results (tree keys, group keys, normal record keys) must be identical.  Floating
+point stages follow the same arithmetic in the same order on both sides: float32 runs must
+be bitwise equal; float64 runs may differ by a few ulps, because two library transcendentals
+(the normal scale's pow, samples.py:75-79, and the splat depths' log, density.py:32-35) can
+differ in their last bit between CUDA and glibc.
 """
 import numpy as np
 import pytest
@@ -15,7 +16,7 @@ from kat_util import KATS, inputs, iso_tolerance, options, sha
 pytestmark = pytest.mark.gpu
 
 # Relative tolerances of floating-point stage parity (oracle vs CUDA, same precision).
-STAGE_RTOL = {"float": 2e-6, "double": 1e-13}
+STAGE_RTOL = {"float": 0.0, "double": 1e-13}
 
 
 def _close(a, b, rtol, what):
