@@ -14,6 +14,8 @@ Prints one JSON line (rank 0).  ``--impl reference`` times the CPU restatement o
 reference algorithm (the oracle) on the host cores instead.
 """
 import argparse
+import ctypes
+import gc
 import json
 import os
 import statistics
@@ -105,6 +107,35 @@ class Clocks:
                 "samples": len(sm)}
 
 
+class Pool:
+    """The device's default stream-ordered memory pool, from which the library takes every
+    buffer (cudaMallocAsync): bytes in use now and the high-water mark since a reset."""
+
+    USED_CURRENT, USED_HIGH = 7, 8  # cudaMemPoolAttrUsedMemCurrent / UsedMemHigh
+
+    def __init__(self, device_index):
+        from warp_psr_b200 import _lib
+        _lib.load()  # brings in the CUDA runtime the library links against
+        self.rt = ctypes.CDLL("libcudart.so.12")
+        self.pool = ctypes.c_void_p()
+        assert self.rt.cudaDeviceGetDefaultMemPool(ctypes.byref(self.pool), device_index) == 0
+
+    def _get(self, attr):
+        v = ctypes.c_uint64()
+        assert self.rt.cudaMemPoolGetAttribute(self.pool, attr, ctypes.byref(v)) == 0
+        return int(v.value)
+
+    def used(self):
+        return self._get(self.USED_CURRENT)
+
+    def high(self):
+        return self._get(self.USED_HIGH)
+
+    def reset_high(self):
+        zero = ctypes.c_uint64(0)
+        assert self.rt.cudaMemPoolSetAttribute(self.pool, self.USED_HIGH, ctypes.byref(zero)) == 0
+
+
 def field_error(result, reference, queries):
     """Max |f - f64| at the queries, raw and normalised by max |f64| (both evaluated in float64)."""
     import torch
@@ -145,13 +176,13 @@ def run_ours(args, rank, world):
     q_host = lo + (hi - lo) * rng.uniform(size=(32, 3))
     seed_host = rng.normal(size=32)
 
-    def step(p_in=None, n_in=None):
+    def step(p_in=None, n_in=None, precision=None):
         """One solve+adjoint: differentiable reconstruction, loss, reverse pass onto the inputs."""
         P = (p_dev if p_in is None else p_in).detach().requires_grad_(True)
         N = (n_dev if n_in is None else n_in).detach().requires_grad_(True)
         e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         e[0].record(stream)
-        res = reconstruct_differentiable(P, N, precision=args.precision, **CONFIG)
+        res = reconstruct_differentiable(P, N, precision=precision or args.precision, **CONFIG)
         dtype = res.result.field.coefficients.dtype
         q = torch.as_tensor(q_host, dtype=dtype, device=device)
         seed = torch.as_tensor(seed_host, dtype=dtype, device=device)
@@ -208,6 +239,9 @@ def run_ours(args, rank, world):
     bw_stage_ms = {k: round(statistics.mean(b[k] for b in bw_stages), 3) for k in bw_stages[0]} if bw_stages else {}
     fwd_ms = statistics.mean(x[0] for x in split)
     bwd_ms = statistics.mean(x[1] for x in split)
+    # the finest level's relaxation launch over the timed steps (the roofline's kernel)
+    finest_s = statistics.mean(f[0] for f in finest)
+    visits = finest[-1][1]
     torch.cuda.synchronize()
     ms = replicas.max_over_ranks(ms, device)
     replicas.barrier()
@@ -227,7 +261,48 @@ def run_ours(args, rank, world):
     e2e_ms, _ = timed(e2e_step, args.steps)
     e2e_ms = replicas.max_over_ranks(e2e_ms, device)
     # the forward alone, not differentiable (what reconstruct() costs)
-    plain_ms, _ = timed(lambda: reconstruct(p_dev, n_dev, precision=args.precision, **CONFIG), max(1, args.steps // 2))
+    plain_ms, plain = timed(lambda: reconstruct(p_dev, n_dev, precision=args.precision, **CONFIG),
+                            max(1, args.steps // 2))
+    plain_relax = {"finest_ms": round(plain.diagnostics["relax_finest_seconds"] * 1e3, 3),
+                   "all_levels_ms": round(plain.diagnostics["relax_seconds"] * 1e3, 3)}
+    del plain
+
+    # The float64 path's solve+adjoint step on the same workload (the metric's comparison).
+    p64, n64 = p_dev.double(), n_dev.double()
+    split.clear()
+    finest.clear()
+    ms64_step, (res64, _, _) = timed(lambda: step(p64, n64, precision="input"), max(2, args.steps // 4))
+    fp64_step = {"ms": round(ms64_step, 3), "forward_differentiable": round(statistics.mean(x[0] for x in split), 3),
+                 "backward": round(statistics.mean(x[1] for x in split), 3),
+                 "relax_finest_ms": round(statistics.mean(f[0] for f in finest) * 1e3, 3),
+                 "precision": "float64 inputs, input precision (the reference's float64 path)"}
+    del p64, n64, res64
+
+    # Memory of the step: the pool's high-water mark over one solve+adjoint step, and the
+    # reverse-pass tape = pool bytes held by a differentiable forward's result minus those
+    # held by a plain forward's result (same inputs).
+    pool = Pool(device.index)
+    gc.collect()
+    torch.cuda.synchronize()
+    pool.reset_high()
+    base_used = pool.used()
+    torch.cuda.reset_peak_memory_stats(device)
+    step()
+    torch.cuda.synchronize()
+    memory = {"pool_peak_bytes": pool.high() - base_used,
+              "torch_peak_bytes": int(torch.cuda.max_memory_allocated(device))}
+    gc.collect()
+    held = {}
+    for name, differentiable in (("plain", False), ("differentiable", True)):
+        before = pool.used()
+        r = reconstruct(p_dev, n_dev, precision=args.precision, _differentiable=differentiable, **CONFIG)
+        torch.cuda.synchronize()
+        held[name] = pool.used() - before
+        del r
+        gc.collect()
+        torch.cuda.synchronize()
+    memory["result_bytes"] = held["plain"]
+    memory["tape_bytes"] = held["differentiable"] - held["plain"]
 
     out_dtype = "f64" if result["dtype"] == torch.float64 else "f32"
     info = result
@@ -239,8 +314,6 @@ def run_ours(args, rank, world):
     vec = 8 if out_dtype == "f64" else 4
     op = 4 if args.precision == "mixed" else vec
     per_visit = 27 * op + 3 * vec + 4
-    finest_s = statistics.mean(f[0] for f in finest)
-    visits = finest[-1][1]
     algorithmic = visits * per_visit
     achieved = algorithmic / finest_s / 1e9 if finest_s > 0 else None
     peak, peak_kind = peaks()
@@ -277,6 +350,11 @@ def run_ours(args, rank, world):
         "split_ms": {"forward_differentiable": round(fwd_ms, 3), "backward": round(bwd_ms, 3),
                      "adjoint_over_forward": round(bwd_ms / fwd_ms, 3), "forward_plain": round(plain_ms, 3),
                      "backward_stages": bw_stage_ms},
+        "fp64_step": fp64_step,
+        "coefficient_sweeps_per_s": {"step": round(all_visits / (ms / 1e3), 1),
+                                     "relaxation_kernels": round(all_visits / all_s, 1) if all_s > 0 else None,
+                                     "row_visits_per_step": int(all_visits)},
+        "memory": memory,
         "gpu_launches": int(launches),
         "stage_ms": {k: round(v * 1e3, 3) for k, v in result["timings"].items()},
         "clocks": clocks.summary(),
@@ -292,11 +370,21 @@ def run_ours(args, rank, world):
         if args.precision != "input":
             f32 = reconstruct(p_dev, n_dev, **CONFIG)
             line["fp32_error_vs_fp64"] = field_error(f32, fp64, q)
-            ms32, _ = timed(lambda: reconstruct(p_dev, n_dev, **CONFIG), max(1, args.steps // 2))
-            ms64, _ = timed(lambda: reconstruct(p_dev.double(), n_dev.double(), **CONFIG), max(1, args.steps // 2))
-            line["variants_ms"] = {"fp32": round(ms32, 3), "fp64": round(ms64, 3)}
+            ms32, r32 = timed(lambda: reconstruct(p_dev, n_dev, **CONFIG), max(1, args.steps // 2))
+            ms64, r64 = timed(lambda: reconstruct(p_dev.double(), n_dev.double(), **CONFIG), max(1, args.steps // 2))
+            line["variants_ms"] = {"fp32": round(ms32, 3), "fp64": round(ms64, 3), args.precision: round(plain_ms, 3),
+                                   "scope": "plain forward reconstruction"}
+            line["variants_relax_ms"] = {
+                "fp32": {"finest_ms": round(r32.diagnostics["relax_finest_seconds"] * 1e3, 3),
+                         "all_levels_ms": round(r32.diagnostics["relax_seconds"] * 1e3, 3)},
+                "fp64": {"finest_ms": round(r64.diagnostics["relax_finest_seconds"] * 1e3, 3),
+                         "all_levels_ms": round(r64.diagnostics["relax_seconds"] * 1e3, 3)},
+                args.precision: plain_relax}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p_host, n_host, steps=1)
+        # same work on both sides: the CPU restatement has no reverse pass, so set its forward
+        # against the GPU's plain forward
+        line["cpu_baseline"]["over_gpu_forward_plain"] = round(line["cpu_baseline"]["value"] / plain_ms, 1)
     return line
 
 
@@ -360,6 +448,13 @@ def main():
     globals()["POINTS"] = args.points
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "ours" and args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # N independent replicas, one process per GPU, started here when no launcher did
+        from warp_psr_b200 import replicas
+        rc, out, err = replicas.launch(args.gpus, Path(__file__).resolve(), sys.argv[1:])
+        sys.stdout.write(out)
+        sys.stderr.write(err)
+        sys.exit(rc)
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)), flush=True)

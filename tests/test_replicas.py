@@ -50,3 +50,18 @@ def test_single_process_is_identity():
     assert replicas.shard([1, 2, 3]) == [1, 2, 3]
     assert replicas.max_over_ranks(3.5) == 3.5
     assert replicas.gather("x") == ["x"]
+
+
+def test_launch_runs_every_rank_and_prints_rank_zeros_line():
+    """replicas.launch (what ``bench.py --gpus N`` uses when it is not started by torchrun)
+    brings up N ranks; rank 0's line reports all of them and the maximum over ranks."""
+    import json
+    from pathlib import Path
+    from warp_psr_b200 import replicas
+    probe = Path(__file__).resolve().parent / "replica_probe.py"
+    rc, out, err = replicas.launch(3, probe, timeout=240)
+    assert rc == 0, err[-3000:]
+    lines = [line for line in out.splitlines() if line.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["n_gpus"] == 3 and line["value"] == 3.0 and line["local_rank"] == 0

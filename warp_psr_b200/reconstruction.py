@@ -151,14 +151,17 @@ STAGES = ("samples", "density", "normal_field", "tree", "assembly_and_solve", "f
 
 def reconstruct(positions, normals, *, depth=6, full_depth=3, base_depth=None, solve_depth=None, kernel_depth=None,
                 samples_per_node=1.5, scale=1.1, point_weight=2.0, exact_interpolation=False, iters=8,
-                base_v_cycles=1, cg_accuracy=1e-3, precision="input", keep_stages=False, _differentiable=False):
+                base_v_cycles=1, cg_accuracy=1e-3, precision="input", keep_stages=False, error_vs_fp64=False,
+                _differentiable=False):
     """Reconstruct oriented CUDA float32/float64 vectors; point_weight=0 selects PSR.
 
     Degree one, Neumann boundaries, confidence disabled.  The return value evaluates the
     implicit function and its model-space gradient; the surface is
     ``value == result.iso_value``.  ``precision="input"`` solves in the input precision
     exactly like the reference; ``precision="mixed"`` solves in float64 with float32
-    storage of the relaxation operators (float64 coefficients).
+    storage of the relaxation operators (float64 coefficients).  ``error_vs_fp64=True``
+    also runs the float64 path on the same inputs and records in
+    ``metadata["error_vs_fp64"]`` the field's error against it (see ``field_error``).
     """
     if base_depth is None:
         base_depth = full_depth
@@ -248,7 +251,39 @@ def reconstruct(positions, normals, *, depth=6, full_depth=3, base_depth=None, s
                    "relax_finest_seconds": info.relax_finest_ms / 1000.0,
                    "relax_finest_row_visits": int(info.relax_finest_row_visits),
                    "normalization": tuple(info.normalization)}
-    return Reconstruction(field, metadata, diagnostics)
+    result = Reconstruction(field, metadata, diagnostics)
+    if error_vs_fp64:
+        options = dict(depth=depth, full_depth=full_depth, base_depth=base_depth, solve_depth=solve_depth,
+                       kernel_depth=kernel_depth, samples_per_node=samples_per_node, scale=scale,
+                       point_weight=point_weight, exact_interpolation=exact_interpolation, iters=iters,
+                       base_v_cycles=base_v_cycles, cg_accuracy=cg_accuracy)
+        if out_dtype == torch.float64 and p.dtype == torch.float64 and precision == "input":
+            reference = result
+        else:
+            reference = reconstruct(p.double(), n.double(), **options)
+        metadata["error_vs_fp64"] = field_error(result, reference, p)
+    return result
+
+
+def field_error(result, reference, points, extra=20_000, seed=2027):
+    """Error of ``result``'s field against ``reference`` (a float64 reconstruction of the same
+    inputs), both evaluated in float64 at the input points and at ``extra`` points uniform
+    in their bounding box: max |f - f64|, that maximum normalised by max |f64|, the
+    isovalue difference, and the number of valid queries."""
+    pts = points.detach().to(torch.float64).reshape(-1, 3)
+    lo, hi = pts.min(0).values, pts.max(0).values
+    gen = torch.Generator(device=pts.device).manual_seed(seed)
+    box = lo + (hi - lo) * torch.rand((extra, 3), dtype=torch.float64, device=pts.device, generator=gen)
+    q = torch.cat([pts, box])
+    ref_v, _, ok = reference.evaluate(q)
+    dtype = result.field.coefficients.dtype
+    v, _, _ = result.evaluate(q.to(dtype))
+    m = ok.bool()
+    diff = (v.double()[m] - ref_v[m]).abs().max().item()
+    scale = ref_v[m].abs().max().item()
+    return {"max_abs": diff, "normalised": diff / scale if scale > 0 else diff,
+            "iso_abs": abs(result.iso_value - reference.iso_value), "queries": int(m.sum().item()),
+            "reference": "float64 path, same inputs"}
 
 
 # ---------------------------------------------------------------- differentiable reconstruction

@@ -7,6 +7,12 @@ finite-difference check), one per rank.  No collective is on the data path; rank
 to agree on timings (the maximum over ranks) and to gather small per-reconstruction results.
 Works with any torch.distributed backend (nccl on GPUs, gloo on CPUs).
 """
+import os
+import signal
+import socket
+import subprocess
+import sys
+
 import torch
 import torch.distributed as dist
 
@@ -63,3 +69,27 @@ def reconstruct_many(clouds, **options):
         local.append((index, result.iso_value, int(result.field.keys.numel())))
     merged = [item for part in gather(local) for item in part]
     return sorted(merged)
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def launch(nprocs, script, args=(), timeout=3600, env=None):
+    """Runs ``script`` as ``nprocs`` ranks of one node (torch.distributed.run, rendezvous on
+    127.0.0.1; RANK, LOCAL_RANK, WORLD_SIZE and MASTER_* set for each rank) and returns
+    (exit code, stdout, stderr).  The launcher's whole process group is killed if it runs
+    past ``timeout`` seconds."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={int(nprocs)}",
+           "--master-addr=127.0.0.1", f"--master-port={free_port()}", str(script), *map(str, args)]
+    proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, start_new_session=True,
+                            env=env)
+    try:
+        out, err = proc.communicate(timeout=timeout)
+    except subprocess.TimeoutExpired:
+        os.killpg(proc.pid, signal.SIGKILL)
+        out, err = proc.communicate()
+        return -signal.SIGKILL, out, err + f"\nreplicas.launch: killed after {timeout} s"
+    return proc.returncode, out, err
