@@ -20,6 +20,8 @@
  *   psr_isovalue          <- reconstruction._compute_isovalue src/warp_psr/reconstruction.py:101-116
  *   psr_backward          <- reconstruct_differentiable backward  src/warp_psr/reconstruction_adjoint.py:99-172
  *   psr_evaluate_backward <- DifferentiableField.evaluate VJP  field_adjoint.py:34-45,246-288; field.py:214-284
+ *   psr_mc_*, psr_mesh_*  <- extract_isosurface (sparse/dense) meshing.py:150-281, Warp's marching cubes
+ *   psr_extract_mesh      <- extract_mesh                     meshing.py:284-346
  */
 #ifndef PSR_B200_H
 #define PSR_B200_H
@@ -150,15 +152,16 @@ int psr_isovalue_static(int32_t dtype, const void* values, const void* weights, 
 /* Reverse pass of a reconstruction made with params.differentiable (warp-psr
  * reconstruction_adjoint.py:99-172): the vector-Jacobian product of the finite algorithm
  * the forward ran, with its discrete choices fixed (groups, tree, bins, schedules, CG
- * stopping points).  Seeds (result dtype; NULL = zero): g_coefficients and g_cumulative
- * (total values each), g_iso, g_normalization (5, the adjoint of psr_info.normalization).
+ * stopping points).  Seeds (device pointers, result dtype; NULL = zero): g_coefficients and
+ * g_cumulative (total values each), g_iso (one value), g_normalization (5, the adjoint of
+ * psr_info.normalization).
  * positions/normals are the forward's inputs (unchanged since), n points of input dtype
  * `dtype`; g_positions and g_normals (n x 3, input dtype) are written, stream-ordered on
  * `stream` (the call returns without waiting for the device; psr_result_info waits for the
  * pass when it reports backward_ms).  The tape stays, so the pass can be repeated with other
  * seeds. */
 int psr_backward(psr_result* result, const void* positions, const void* normals, int64_t n, int32_t dtype,
-                 const void* g_coefficients, const void* g_cumulative, double g_iso, const void* g_normalization,
+                 const void* g_coefficients, const void* g_cumulative, const void* g_iso, const void* g_normalization,
                  void* g_positions, void* g_normals, void* stream);
 
 /* psr_evaluate reversed: seeds g_values (nq) and g_gradients (nq x 3, NULL = zero), result
@@ -168,6 +171,47 @@ int psr_backward(psr_result* result, const void* positions, const void* normals,
 int psr_evaluate_backward(const psr_result* result, const void* queries, int64_t nq, const void* g_values,
                           const void* g_gradients, void* g_coefficients, void* g_cumulative, void* g_queries,
                           void* g_normalization, void* stream);
+
+/* ---- Sparse marching cubes: the field's mesh consumer (warp-psr meshing.py:150-346) ----
+ * Grid: shape[0..2] >= 2 nodes per axis spanning [lower, upper] in model space, the spacing
+ * step = (upper - lower) / (shape - 1) computed in float32 as the reference does; node
+ * (i, j, k) sits at min(max(lower + step * (i, j, k), lower), upper), node index
+ * (i * ny + j) * nz + k, cell index (i * (ny - 1) + j) * (nz - 1) + k.  Values are centred
+ * (field - isovalue) in dtype; a node is inside when its value is >= 0 and a cell is kept when
+ * its corners are neither all inside nor all outside.  Triangles are oriented with normals
+ * pointing from inside to outside; one vertex per crossing grid edge, at pa + t (pb - pa),
+ * t = fa / (fa - fb), on the edge's lower node a and upper node b. */
+typedef struct psr_mesh psr_mesh;
+
+/* Model positions (count x 3, dtype) of the nodes of x-planes start.. (cells == NULL: count =
+ * (planes) * ny * nz) or of the eight corners of each listed cell (count = 8 * cells). */
+int psr_mc_points(int32_t dtype, const int64_t shape[3], const double lower[3], const double upper[3],
+                  const int64_t* cells, int64_t start, int64_t count, void* points, void* stream);
+/* Sets the mask bit (uint32 words over all cells) of every crossing cell of the x-slab
+ * [start, start + width) from the values of its (width + 1) * ny * nz nodes; status[0] |= 1
+ * if a value is not finite (meshing.py:45-60). */
+int psr_mc_mark(int32_t dtype, const void* values, const int64_t shape[3], int64_t start, int64_t width,
+                uint32_t* mask, int32_t* status, void* stream);
+/* Number of marked cells (*count, a host read) and, when cells != NULL, their indices in
+ * ascending order (meshing.py:63-85). */
+int psr_mc_cells(const uint32_t* mask, int64_t words, int64_t* cells, int64_t capacity, int64_t* count, void* stream);
+/* Triangles of the listed cells from their corner values (count x 8, corner order 000, 100,
+ * 110, 010, 001, 101, 111, 011). */
+int psr_mc_triangulate(int32_t dtype, const int64_t shape[3], const double lower[3], const double upper[3],
+                       const int64_t* cells, const void* corner_values, int64_t count, psr_mesh** out, void* stream);
+/* The whole extraction on a reconstruction's own field (extract_mesh, meshing.py:284-346):
+ * slabs of `slab` x-planes classified with the library's evaluator, then the kept cells'
+ * corners evaluated and triangulated; *retained = kept cells.  PSR_EDATA if a grid node lies
+ * outside the reconstruction cube (nonfinite field value). */
+int psr_extract_mesh(const psr_result* result, const int64_t shape[3], const double lower[3], const double upper[3],
+                     double iso, int64_t slab, int64_t* retained, psr_mesh** out, void* stream);
+int psr_mesh_info(const psr_mesh* mesh, int32_t* dtype, int64_t* vertices, int64_t* triangles, int64_t* cells);
+/* vertices (x 3, dtype), indices (triangles x 3, int32), the crossing edge of each vertex
+ * ((lower node index) * 3 + axis), its two corner values (cell * 8 + corner, flat indices
+ * into the corner values), and the kept cells (psr_extract_mesh; NULL otherwise). */
+int psr_mesh_arrays(const psr_mesh* mesh, const void** vertices, const int32_t** indices, const int64_t** edges,
+                    const int64_t** ends, const int64_t** cells);
+int psr_mesh_free(psr_mesh* mesh);
 
 #ifdef __cplusplus
 }

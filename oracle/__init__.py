@@ -43,6 +43,8 @@ def lib():
         vp, i64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32
         L.oracle_reconstruct.restype = vp
         L.oracle_reconstruct.argtypes = [vp, vp, i64, i32, ctypes.POINTER(_Params)]
+        L.oracle_tree.restype = vp
+        L.oracle_tree.argtypes = [vp, vp, i64, i32, ctypes.POINTER(_Params)]
         L.oracle_last_error.restype = ctypes.c_char_p
         L.oracle_free.argtypes = [vp]
         L.oracle_level_count.restype = i64
@@ -85,7 +87,7 @@ def params(depth=6, full_depth=3, base_depth=None, solve_depth=None, kernel_dept
 class OracleResult:
     """Owns one oracle reconstruction; arrays are copied out as numpy."""
 
-    def __init__(self, positions, normals, **options):
+    def __init__(self, positions, normals, tree_only=False, **options):
         positions = np.ascontiguousarray(positions)
         normals = np.ascontiguousarray(normals, dtype=positions.dtype)
         if positions.dtype not in (np.float32, np.float64):
@@ -95,8 +97,10 @@ class OracleResult:
         self.options = p
         self._p = _Params(**p)
         L = lib()
-        self._h = L.oracle_reconstruct(positions.ctypes.data, normals.ctypes.data, len(positions),
-                                       int(self.dtype == np.float64), ctypes.byref(self._p))
+        # tree_only: the stages up to the tree (keys and their stages), no solve
+        run = L.oracle_tree if tree_only else L.oracle_reconstruct
+        self._h = run(positions.ctypes.data, normals.ctypes.data, len(positions), int(self.dtype == np.float64),
+                      ctypes.byref(self._p))
         if not self._h:
             raise ValueError(L.oracle_last_error().decode())
         self.depth = p["depth"]

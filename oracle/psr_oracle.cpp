@@ -1407,8 +1407,9 @@ void blocked_isovalue(const std::vector<T>& values, const std::vector<T>& weight
 }
 
 // ---------------------------------------------------------------- driver (reconstruction.py:137-349, solver.py:320-466)
+// tree_only: stop after the tree (stages up to A4, basis and support keys; no solve).
 template <class T>
-Result<T>* reconstruct(const T* pos, const T* nrm, int64_t count, const Params& prm) {
+Result<T>* reconstruct(const T* pos, const T* nrm, int64_t count, const Params& prm, bool tree_only = false) {
   auto R = std::make_unique<Result<T>>();
   R->dtype = sizeof(T) == 8 ? 1 : 0;
   R->depth = prm.depth;
@@ -1436,6 +1437,14 @@ Result<T>* reconstruct(const T* pos, const T* nrm, int64_t count, const Params& 
   Tree tree = build_tree(N, prm.depth, prm.full_depth, prm.base_depth);
   R->basis = tree.basis;
   R->support = tree.support;
+  if (tree_only) {
+    for (int d = 0; d <= prm.depth; ++d) {
+      R->level_offsets.push_back(int64_t(R->all_keys.size()));
+      R->all_keys.insert(R->all_keys.end(), tree.basis[d].begin(), tree.basis[d].end());
+    }
+    R->level_offsets.push_back(int64_t(R->all_keys.size()));
+    return R.release();
+  }
   int finest = prm.depth;
   const auto& keys = tree.basis;
   std::vector<Csr<T>> transfers(finest);
@@ -1548,6 +1557,19 @@ void* oracle_reconstruct(const void* pos, const void* nrm, int64_t n, int32_t dt
   try {
     if (dtype == 1) return reconstruct<double>((const double*)pos, (const double*)nrm, n, prm);
     return reconstruct<float>((const float*)pos, (const float*)nrm, n, prm);
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return nullptr;
+  }
+}
+
+// The stages up to the tree only (samples, density, normal field, tree): keys, no solve.
+void* oracle_tree(const void* pos, const void* nrm, int64_t n, int32_t dtype, const oracle_params* p) {
+  Params prm{p->depth, p->full_depth, p->base_depth, p->solve_depth, p->kernel_depth, p->samples_per_node,
+             p->scale, p->point_weight, p->cg_accuracy, p->exact, p->iters, p->base_v_cycles};
+  try {
+    if (dtype == 1) return reconstruct<double>((const double*)pos, (const double*)nrm, n, prm, true);
+    return reconstruct<float>((const float*)pos, (const float*)nrm, n, prm, true);
   } catch (const std::exception& e) {
     g_error = e.what();
     return nullptr;

@@ -229,3 +229,34 @@ def test_adjoint_depth7_float32_against_float64(torus100k):
             d32, d64 = float((a * direction).sum()), float((b * direction).sum())
             print(f"  directional {name}: float32 {d32:.6e} float64 {d64:.6e}")
             assert abs(d32 - d64) <= 2e-2 * abs(d64), name
+
+
+def test_three_tori_depth10_tree_matches_oracle():
+    """The scale configuration: 3,500,000 points on three tori (1% outliers, 2% flipped
+    normals), float32 inputs, depth 10, full depth 5, point weight 4.  The float32 path's
+    sample groups, normal records and basis and support keys of every depth are exact against
+    the oracle's float32 stages up to the tree (it stops before the solve, which takes minutes
+    on the host); the mixed precision (a float64 pipeline over the float32 inputs) has exactly
+    the float64 oracle's tree, a finite solution and a field error against the float64 path
+    within 1e-6."""
+    cfg = clouds.CONFIGS[5]
+    p, n = cfg["cloud"]()
+    p, n = p.astype(np.float32), n.astype(np.float32)
+    opts = dict(depth=cfg["depth"], full_depth=cfg["full_depth"], point_weight=cfg["point_weight"])
+    P, N = torch.from_numpy(p).cuda(), torch.from_numpy(n).cuda()
+    g = reconstruct(P, N, keep_stages=True, **opts)
+    ref = oracle.OracleResult(p, n, tree_only=True, **opts)
+    stage = g.diagnostics["stage"]
+    assert np.array_equal(stage("group_keys", torch.int64).cpu().numpy(), ref.stage("group_keys", np.int64))
+    assert np.array_equal(stage("normal_keys", torch.int64).cpu().numpy(), ref.stage("normal_keys", np.int64))
+    for d in range(opts["depth"] + 1):
+        assert np.array_equal(g.diagnostics["support_keys"][d].cpu().numpy(), ref.support(d)), d
+    assert np.array_equal(g.field.keys.cpu().numpy(), ref.keys)
+    del g, ref
+    mixed = reconstruct(P, N, precision="mixed", error_vs_fp64=True, **opts)
+    ref64 = oracle.OracleResult(p.astype(np.float64), n.astype(np.float64), tree_only=True, **opts)
+    assert np.array_equal(mixed.field.keys.cpu().numpy(), ref64.keys)
+    assert np.isfinite(mixed.field.coefficients.cpu().numpy()).all()
+    err = mixed.metadata["error_vs_fp64"]
+    print(f"three tori depth 10: {len(ref64.keys)} coefficients, mixed field error vs float64 {err}")
+    assert err["normalised"] <= 1e-6

@@ -56,7 +56,9 @@ class FieldHandle(ctypes.Structure):
 
 EXPORTS = ("psr_reconstruct", "psr_result_info", "psr_result_arrays", "psr_evaluate", "psr_device_field",
            "psr_free", "psr_last_error", "psr_relax_sliced", "psr_isovalue", "psr_result_stage",
-           "psr_kernel_launches", "psr_isovalue_static", "psr_backward", "psr_evaluate_backward")
+           "psr_kernel_launches", "psr_isovalue_static", "psr_backward", "psr_evaluate_backward",
+           "psr_mc_points", "psr_mc_mark", "psr_mc_cells", "psr_mc_triangulate", "psr_extract_mesh",
+           "psr_mesh_info", "psr_mesh_arrays", "psr_mesh_free")
 
 _lib = None
 
@@ -88,8 +90,19 @@ def load():
     L.psr_result_stage.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(vp), ctypes.POINTER(i64), ctypes.POINTER(i32)]
     L.psr_kernel_launches.argtypes = [ctypes.POINTER(i64)]
     L.psr_isovalue_static.argtypes = [i32, vp, vp, i64, vp, vp]
-    L.psr_backward.argtypes = [vp, vp, vp, i64, i32, vp, vp, ctypes.c_double, vp, vp, vp, vp]
+    L.psr_backward.argtypes = [vp, vp, vp, i64, i32, vp, vp, vp, vp, vp, vp, vp]
     L.psr_evaluate_backward.argtypes = [vp, vp, i64, vp, vp, vp, vp, vp, vp, vp]
+    shape3, real3 = ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_double)
+    L.psr_mc_points.argtypes = [i32, shape3, real3, real3, vp, i64, i64, vp, vp]
+    L.psr_mc_mark.argtypes = [i32, vp, shape3, i64, i64, vp, vp, vp]
+    L.psr_mc_cells.argtypes = [vp, i64, vp, i64, ctypes.POINTER(i64), vp]
+    L.psr_mc_triangulate.argtypes = [i32, shape3, real3, real3, vp, vp, i64, ctypes.POINTER(vp), vp]
+    L.psr_extract_mesh.argtypes = [vp, shape3, real3, real3, ctypes.c_double, i64, ctypes.POINTER(i64),
+                                   ctypes.POINTER(vp), vp]
+    L.psr_mesh_info.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i64), ctypes.POINTER(i64),
+                                ctypes.POINTER(i64)]
+    L.psr_mesh_arrays.argtypes = [vp] + [ctypes.POINTER(vp)] * 5
+    L.psr_mesh_free.argtypes = [vp]
     for name in EXPORTS:
         getattr(L, name).restype = i32
     _lib = L

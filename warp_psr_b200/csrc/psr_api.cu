@@ -264,7 +264,7 @@ __global__ void cast_kernel_t(const void* in, int in_double, int64_t n, T* out) 
 // Reverse pass: field (isovalue, cumulative) -> solve -> splats, density -> inputs.
 template <class T>
 void backward(psr_result* R, const T* pos, const T* nrm, int64_t n, const T* g_coef_in, const T* g_cum_in,
-              double g_iso, const T* g_norm, T* g_pos, T* g_nrm, cudaStream_t s) {
+              const T* g_iso, const T* g_norm, T* g_pos, T* g_nrm, cudaStream_t s) {
   Tape<T>& tp = *static_cast<Tape<T>*>(R->tape.get());
   const Params& prm = R->params;
   const int64_t total = R->level_offsets.back();
@@ -468,21 +468,20 @@ int psr_evaluate(const psr_result* R, const void* queries, int64_t nq, void* val
 }
 
 int psr_backward(psr_result* R, const void* positions, const void* normals, int64_t n, int32_t dtype,
-                 const void* g_coefficients, const void* g_cumulative, double g_iso, const void* g_normalization,
+                 const void* g_coefficients, const void* g_cumulative, const void* g_iso, const void* g_normalization,
                  void* g_positions, void* g_normals, void* stream) {
   try {
     if (!R) throw Error(PSR_EINVAL, "result must not be NULL");
     if (!R->tape) throw Error(PSR_EINVAL, "the reconstruction was not made differentiable (params.differentiable)");
     if (dtype != PSR_FLOAT32 && dtype != PSR_FLOAT64) throw Error(PSR_EINVAL, "dtype must be float32 or float64");
     if (!positions || !normals || !g_positions || !g_normals) throw Error(PSR_EINVAL, "inputs and outputs are required");
-    if (!std::isfinite(g_iso)) throw Error(PSR_EINVAL, "g_iso must be finite");
     cudaStream_t s = (cudaStream_t)stream;
     if (R->dtype == PSR_FLOAT64) {
       const int64_t want = static_cast<Tape<double>*>(R->tape.get())->n_input;
       if (n != want) throw Error(PSR_EINVAL, "n differs from the forward's point count");
       if (dtype == PSR_FLOAT64) {
         backward<double>(R, (const double*)positions, (const double*)normals, n, (const double*)g_coefficients,
-                         (const double*)g_cumulative, g_iso, (const double*)g_normalization, (double*)g_positions,
+                         (const double*)g_cumulative, (const double*)g_iso, (const double*)g_normalization, (double*)g_positions,
                          (double*)g_normals, s);
       } else {
         DBuf<double> p64(3 * n, s), n64(3 * n, s), gp(3 * n, s), gn(3 * n, s);
@@ -490,7 +489,7 @@ int psr_backward(psr_result* R, const void* positions, const void* normals, int6
         PSR_LAUNCH_CHECK();
         cast_kernel_t<double><<<blocks_for(3 * n), kThreads, 0, s>>>(normals, 0, 3 * n, n64.p);
         PSR_LAUNCH_CHECK();
-        backward<double>(R, p64.p, n64.p, n, (const double*)g_coefficients, (const double*)g_cumulative, g_iso,
+        backward<double>(R, p64.p, n64.p, n, (const double*)g_coefficients, (const double*)g_cumulative, (const double*)g_iso,
                          (const double*)g_normalization, gp.p, gn.p, s);
         cast_kernel_t<float><<<blocks_for(3 * n), kThreads, 0, s>>>(gp.p, 1, 3 * n, (float*)g_positions);
         PSR_LAUNCH_CHECK();
@@ -502,10 +501,9 @@ int psr_backward(psr_result* R, const void* positions, const void* normals, int6
       const int64_t want = static_cast<Tape<float>*>(R->tape.get())->n_input;
       if (n != want) throw Error(PSR_EINVAL, "n differs from the forward's point count");
       backward<float>(R, (const float*)positions, (const float*)normals, n, (const float*)g_coefficients,
-                      (const float*)g_cumulative, g_iso, (const float*)g_normalization, (float*)g_positions,
+                      (const float*)g_cumulative, (const float*)g_iso, (const float*)g_normalization, (float*)g_positions,
                       (float*)g_normals, s);
     }
-    PSR_CUDA(cudaStreamSynchronize(s));
     return PSR_OK;
   } catch (const Error& e) {
     return fail(e);

@@ -372,11 +372,11 @@ __global__ void evaluate_reverse_kernel(const HashView h, const T* coeff, const 
 }
 
 // Isovalue reversed (field_adjoint.py:144-152): each centroid value's adjoint is
-// T(g_iso / total weight) * w.
+// T(g_iso / total weight) * w, the seed g_iso read from device memory (no host round trip).
 template <class T>
-__global__ void isovalue_reverse_kernel(const T* weights, int64_t n, double g_iso, const double* mass, T* g_values) {
+__global__ void isovalue_reverse_kernel(const T* weights, int64_t n, const T* g_iso, const double* mass, T* g_values) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i < n) g_values[i] = T(g_iso / mass[0]) * weights[i];
+  if (i < n) g_values[i] = T(double(g_iso[0]) / mass[0]) * weights[i];
 }
 
 // Total sample weight (float64), block sums added atomically (mass must start at zero).
@@ -419,9 +419,9 @@ __global__ void cumulative_reverse_kernel(const int64_t* keys, int64_t begin, in
 
 template <class T>
 void field_backward(const int64_t* keys, const std::vector<int64_t>& offsets, const HashView& h, const T* coeff,
-                    const T* cumulative, int depth, const T* gsums, const T* gweights, int64_t groups, double g_iso,
+                    const T* cumulative, int depth, const T* gsums, const T* gweights, int64_t groups, const T* g_iso,
                     T* g_coeff, T* g_cum, T* g_sums, cudaStream_t s) {
-  if (g_iso != 0.0 && groups > 0) {
+  if (g_iso && groups > 0) {
     DBuf<double> mass(1, s);
     mass.zero();
     mass_kernel<T><<<std::min<int64_t>(blocks_for(groups), 592), 256, 0, s>>>(gweights, groups, mass.p);
@@ -456,7 +456,7 @@ void evaluate_backward(const HashView& h, const T* coeff, const T* cumulative, c
 
 #define INSTANTIATE(T)                                                                                               \
   template void field_backward<T>(const int64_t*, const std::vector<int64_t>&, const HashView&, const T*, const T*, \
-                                  int, const T*, const T*, int64_t, double, T*, T*, T*, cudaStream_t);               \
+                                  int, const T*, const T*, int64_t, const T*, T*, T*, T*, cudaStream_t);             \
   template void evaluate_backward<T>(const HashView&, const T*, const T*, const T*, int64_t, const T*, const T*,     \
                                      int, const T*, const T*, T*, T*, T*, double*, cudaStream_t);                    \
   template void cumulative_coefficients<T>(const int64_t*, const std::vector<int64_t>&, const HashView&, const T*,  \

@@ -190,6 +190,53 @@ __host__ __device__ __forceinline__ void write_inv_diag(I* row, V inv) {
   memcpy(reinterpret_cast<char*>(row + 28), &inv, sizeof(V));
 }
 
+// Stored index rows keep their 16-byte chunks permuted by schedule position: logical chunk q
+// of row p sits at chunk q ^ idx_swizzle<I>(p).  Any eight consecutive rows then hold a given
+// logical chunk in eight different groups of four shared-memory banks (64-byte rows of 16-bit
+// indices: two rows per 128 bytes, four chunks; 128-byte rows of 32-bit indices: eight
+// chunks), so a warp reading one chunk of 32 consecutive staged rows takes the minimum of four
+// wavefronts instead of sixteen (thirty-two for 32-bit rows), at any offset of the rows in
+// shared memory.  Rows are written and read whole through store_idx_row / load_idx_row.
+template <class I>
+__host__ __device__ constexpr int idx_chunks() {
+  return 32 * int(sizeof(I)) / 16;
+}
+template <class I>
+__host__ __device__ __forceinline__ int idx_swizzle(int64_t p) {
+  return int(p / (8 / idx_chunks<I>())) & (idx_chunks<I>() - 1);
+}
+// Position of logical slot k in the stored row of schedule position p.
+template <class I>
+__host__ __device__ __forceinline__ int idx_slot(int64_t p, int k) {
+  constexpr int E = 16 / int(sizeof(I));
+  return ((k / E) ^ idx_swizzle<I>(p)) * E + k % E;
+}
+// Logical row (32 slots, 16-byte aligned) of schedule position p from its stored row.
+template <class I>
+__device__ __forceinline__ void load_idx_row(const I* stored, int64_t p, I* out) {
+  const int g = idx_swizzle<I>(p);
+  const int4* src = reinterpret_cast<const int4*>(stored);
+  int4* dst = reinterpret_cast<int4*>(out);
+#pragma unroll
+  for (int q = 0; q < idx_chunks<I>(); ++q) dst[q] = src[q ^ g];
+}
+template <class I>
+__device__ __forceinline__ void load_idx_row_ldg(const I* stored, int64_t p, I* out) {
+  const int g = idx_swizzle<I>(p);
+  const int4* src = reinterpret_cast<const int4*>(stored);
+  int4* dst = reinterpret_cast<int4*>(out);
+#pragma unroll
+  for (int q = 0; q < idx_chunks<I>(); ++q) dst[q] = __ldg(src + (q ^ g));
+}
+template <class I>
+__device__ __forceinline__ void store_idx_row(I* stored, int64_t p, const I* in) {
+  const int g = idx_swizzle<I>(p);
+  int4* dst = reinterpret_cast<int4*>(stored);
+  const int4* src = reinterpret_cast<const int4*>(in);
+#pragma unroll
+  for (int q = 0; q < idx_chunks<I>(); ++q) dst[q ^ g] = src[q];
+}
+
 // Schedule order of a sliced level: rows sorted by (slice, colour), key order inside a group.
 struct StripSchedule {
   int64_t rows = 0;
@@ -240,7 +287,7 @@ void evaluation_transforms(const T* normalization, T* transforms /* 32 */, cudaS
 // group, accumulated) receives the centroids' share.
 template <class T>
 void field_backward(const int64_t* keys, const std::vector<int64_t>& offsets, const HashView& h, const T* coeff,
-                    const T* cumulative, int depth, const T* gsums, const T* gweights, int64_t groups, double g_iso,
+                    const T* cumulative, int depth, const T* gsums, const T* gweights, int64_t groups, const T* g_iso,
                     T* g_coeff, T* g_cum, T* g_sums, cudaStream_t s);
 // Model-frame query evaluation reversed: g_coeff, g_cum accumulate; g_queries is written;
 // g_ltr (12 float64: L row-major, then tr) accumulates.

@@ -30,6 +30,8 @@
 // flight, and every CTA exits.
 #include "psr_internal.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -53,8 +55,32 @@ __host__ __device__ __forceinline__ V get_inv_diag(const I* row) {
   memcpy(&inv, reinterpret_cast<const char*>(row + 28), sizeof(V));
   return inv;
 }
-constexpr int kPad = 32;       // one 128-byte line per slice counter
+constexpr int kFlagPad = 8;    // one 32-byte sector per strip flag
+constexpr int kTraceSlots = 16;
 constexpr int kRelaxThreads = 512;
+// Resident CTAs per SM.  Measured at depth 9 (mixed, 16 strips): one 512-thread CTA per SM
+// 3.01 ms, two 256-thread CTAs per SM with half the shared memory each 5.2 ms (tasks that no
+// longer fit shared memory read their rows from global memory).
+constexpr int kRelaxCtasPerSm = 1;
+constexpr int kMetaInts = 96;
+
+// One task description per (logical slice z, strip s), shared by the iters visits of that
+// strip; built once per launch by strip_meta_kernel.  Footprint range r = 4j + c is colour
+// c of logical slice z - 1 + j, x within 4 of the strip.
+struct StripMeta {
+  int lo[12], hi[12];        // schedule positions [lo, hi) of each footprint range
+  int base[13];              // footprint offset of each range; base[12] = footprint size
+  int delta[12];             // footprint index of a group-relative neighbour index i: i + delta[r]
+  int p0[4], p1[4];          // rows updated in colour phase c: own rows plus a halo of width 3 - c
+  int rbase[5];              // staged row offset of each colour's rows; rbase[4] = staged rows
+  int bshift[4];             // staged right-hand-side offset of each colour's first row
+  int o0[4], o1[4];          // own rows (x in [x0, x1)): published and recorded
+  int staged;                // rows and right-hand sides fit shared memory (bulk copies)
+  uint32_t bytes;            // bytes of those copies
+  int dep_lo[3], dep_hi[3];  // strips of slices z-1, z, z+1 whose x range meets the footprint window
+  int pad[14];
+};
+static_assert(sizeof(StripMeta) == kMetaInts * 4, "StripMeta is loaded as kMetaInts ints");
 
 struct StripLevel {
   int n;                 // 2^depth (slices 0..n)
@@ -63,19 +89,19 @@ struct StripLevel {
   int cap;               // footprint capacity (elements) per CTA
   int row_cap;           // staged update rows per task
   int b_cap;             // staged right-hand-side elements per task
-  const int32_t* bounds;     // [(n+1)*(strips+1)] x boundaries of the strips of each slice
-  const int32_t* group_off;  // [4(n+1)+1] schedule position of each (slice, colour) group
+  const StripMeta* meta;     // [(n+1) * strips] by logical slice, then strip
   const void* vals;          // T[rows*28]   schedule order
   const void* nidx;          // I[rows*32]   neighbour index within its group, -1 absent; [27] = own
   const void* b;             // V[rows + slack]
   void* xb0;                 // V[rows]  even visits
   void* xb1;                 // V[rows]  odd visits (holds the initial x)
-  const int32_t* xstart;     // [(n+1)*4][n+2]: first position of group (z,c) with x >= X
   const int2* visits;        // slice-visits (z, t) in wave order
-  int* done;                 // completed strip tasks of slice z at done[z * kPad]
+  int* done;                 // visits completed by strip s of logical slice z at done[(z*strips + s) * kFlagPad]
   int* counter;
   int* error;
-  long long* trace;          // optional: 8 timestamps per task
+  long long* trace;          // optional, kTraceSlots per task: [0] start (globaltimer ns); [1..11] SM cycles from
+                             // the start to: copies issued, own-slice wait done, first barrier, newest-slice wait
+                             // done, second barrier, phases start, end of phase 0, 1, 2, 3, published; [15] CTA
   void* hist;                // optional V[rows * iters]: row p's record of visit t at p * iters + t
   int64_t rows;              // rows of the level
   int iters;                 // visits per slice
@@ -104,6 +130,15 @@ __device__ __forceinline__ bool wait_at_least(const int* p, int v, const int* er
     __nanosleep(it < 512 ? 32 : 256);
   }
   return false;
+}
+
+// The lanes of one warp wait together until strips [slo, shi] of logical slice zz have
+// completed v visits (one strip per lane); false if any wait gave up.
+__device__ __forceinline__ bool wait_strips(const StripLevel& L, int zz, int slo, int shi, int v, int lane) {
+  bool ok = true;
+  for (int sp = slo + lane; sp <= shi; sp += 32)
+    ok = ok && wait_at_least(L.done + (int64_t(zz) * L.strips + sp) * kFlagPad, v, L.error, L.poll_log2);
+  return __all_sync(0xffffffffu, ok);
 }
 
 // ---- mbarrier and 1-D bulk copy (global -> shared), no multicast
@@ -151,13 +186,6 @@ __device__ __forceinline__ void load_vals(const T* src, T out[kSlotsR]) {
 #pragma unroll
   for (int q = 0; q < kSlotsR * int(sizeof(T)) / 16; ++q) d[q] = s[q];
 }
-template <class I>
-__device__ __forceinline__ void load_idx(const I* src, I out[kIdxSlots]) {
-  const int4* s = reinterpret_cast<const int4*>(src);
-  int4* d = reinterpret_cast<int4*>(out);
-#pragma unroll
-  for (int q = 0; q < kIdxSlots * int(sizeof(I)) / 16; ++q) d[q] = s[q];
-}
 
 // One row of colour C: r = b - sum_k x_k A_k in slot order; x_self += r / A_self.
 // Every slot takes part in the sum: an absent slot (value +0, index idx_absent) reads the +0
@@ -165,12 +193,14 @@ __device__ __forceinline__ void load_idx(const I* src, I out[kIdxSlots]) {
 // skipping it.  A present slot holds its k-th neighbour (checked where the rows are built),
 // which lies in the footprint by construction; the unsigned clamp keeps every read inside
 // the footprint whatever the rows hold.  Measured ~2x fewer instructions per slot than
-// testing each slot's presence and range.
+// testing each slot's presence and range.  An own row (out != nullptr) is published to
+// global memory as soon as it is computed: later phases of the strip do not change it.
 template <int C, bool M, class T, class V, class I>
-__device__ __forceinline__ void update_row(const I* nrow, const T* arow, V bv, V* foot, const int* delta,
-                                           unsigned total, int* error, V* rec, bool record_increment) {
-  __align__(16) I n[kIdxSlots];  // filled with 16-byte vector loads
-  load_idx(nrow, n);
+__device__ __forceinline__ void update_row(const I* nrow, int p, const T* arow, V bv, V* foot, const int* delta,
+                                           unsigned total, int* error, V* rec, bool record_increment, V* out,
+                                           V* out2 = nullptr) {
+  __align__(16) I n[kIdxSlots];  // filled with 16-byte vector loads (stored row of position p)
+  load_idx_row(nrow, p, n);
   __align__(16) T a[kSlotsR];
   load_vals(arow, a);
   V xs[27];
@@ -185,37 +215,44 @@ __device__ __forceinline__ void update_row(const I* nrow, const T* arow, V bv, V
     atomicExch(error, 3);
     return;
   }
-  V inc = V(0);
+  V inc = V(0), xn;
   if (n[13] >= 0 && a[13] != T(0)) {
     inc = r * get_inv_diag<V>(n);
-    foot[self] = xs[13] + inc;
+    xn = xs[13] + inc;
+    foot[self] = xn;
+  } else {
+    xn = foot[self];
   }
-  if (rec) *rec = record_increment ? inc : foot[self];
+  if (out) __stcg(out, xn);
+  if (out2) *out2 = xn;
+  if (rec) *rec = record_increment ? inc : xn;
 }
 
 // `hist` (optional) points at this visit's record column (row p records at hist[p * iters]);
-// only the strip's own rows [o0, o1) write it (halo rows are recomputed by the neighbouring
-// strip, which owns them).
+// only the strip's own rows [o0, o1) write it and are published to `out` (halo rows are
+// recomputed by the neighbouring strip, which owns them).
 template <int C, bool M, class T, class V, class I>
-__device__ __forceinline__ void phase(const StripLevel& L, bool staged, int p0, int p1, int rbase, int bshift,
-                                      const I* s_idx, const T* s_vals, const V* s_b, V* foot, const int* delta,
-                                      unsigned total, V* hist, int o0, int o1) {
+__device__ __forceinline__ void phase(const StripLevel& L, const StripMeta& m, bool staged, const I* s_idx,
+                                      const T* s_vals, const V* s_b, V* foot, V* hist, V* out) {
   const I* gidx = reinterpret_cast<const I*>(L.nidx);
   const T* gvals = reinterpret_cast<const T*>(L.vals);
   const V* gb = reinterpret_cast<const V*>(L.b);
   const bool inc = L.record_increment != 0;
+  const int p0 = m.p0[C], p1 = m.p1[C], o0 = m.o0[C], o1 = m.o1[C], rbase = m.rbase[C], bshift = m.bshift[C];
+  const unsigned total = unsigned(m.base[12]);
   int dreg[12];  // footprint offsets in registers (measured ~1% faster than shared-memory reads)
 #pragma unroll
-  for (int r = 0; r < 12; ++r) dreg[r] = delta[r];
+  for (int r = 0; r < 12; ++r) dreg[r] = m.delta[r];
   for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
-    V* rec = (hist && p >= o0 && p < o1) ? hist + int64_t(p) * L.iters : nullptr;
+    const bool own = p >= o0 && p < o1;
+    V* rec = (hist && own) ? hist + int64_t(p) * L.iters : nullptr;
     if (staged) {
       int i = rbase + (p - p0);
-      update_row<C, M>(s_idx + int64_t(i) * kIdxSlots, s_vals + int64_t(i) * kSlotsR, s_b[bshift + (p - p0)], foot,
-                       dreg, total, L.error, rec, inc);
+      update_row<C, M>(s_idx + int64_t(i) * kIdxSlots, p, s_vals + int64_t(i) * kSlotsR, s_b[bshift + (p - p0)],
+                       foot, dreg, total, L.error, rec, inc, own ? out + p : nullptr);
     } else {
-      update_row<C, M>(gidx + int64_t(p) * kIdxSlots, gvals + int64_t(p) * kSlotsR, gb[p], foot, dreg, total,
-                       L.error, rec, inc);
+      update_row<C, M>(gidx + int64_t(p) * kIdxSlots, p, gvals + int64_t(p) * kSlotsR, gb[p], foot, dreg, total,
+                       L.error, rec, inc, own ? out + p : nullptr);
     }
   }
 }
@@ -224,13 +261,22 @@ __device__ __forceinline__ void phase(const StripLevel& L, bool staged, int p0, 
 // reverse of that sweep on the same layout -- logical slice z is stored slice n - z (so slot
 // k's neighbour lies in logical slice z + 1 - k % 3) and the colours run 3..0.  One
 // instantiation per order keeps each kernel's body to its own four phases.
+//
+// Task (z, t, s) -- visit t of strip s of logical slice z -- waits for the strips whose x
+// range meets its footprint window: of slice z after visit t-1 (early, while its operator
+// rows are copied), then of slice z+1 after visit t and of slice z-1 after visit t-1.  Those
+// waits also order every earlier reader of the x buffer it overwrites (visit t-2 of slice z,
+// read by tasks (z, t-1), (z+1, t-1) and (z-1, t-2) of strips within 4 of its rows) before
+// its first write: each of them is, or was waited for by, a strip this task waits for.  A
+// strip publishes the number of its completed visits with a release (atomicMax, so the count
+// only grows).
 template <class T, class V, class I, bool REV>
-__global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L) {
+__global__ void __launch_bounds__(kRelaxThreads, kRelaxCtasPerSm) strip_gs_kernel(StripLevel L) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t s_bar;
-  __shared__ int s_task, s_fail, s_total, s_rows, s_staged;
-  __shared__ int s_lo[12], s_hi[12], s_base[13], s_delta[12];
-  __shared__ int s_p0[4], s_p1[4], s_rbase[5], s_bshift[4], s_o0[4], s_o1[4];
+  __shared__ int s_task[2], s_fail;
+  __shared__ int2 s_zt[2];
+  __shared__ StripMeta s_meta[2];
   // Shared layout (each part 16-byte aligned): footprint V[cap + 1] | values T[row_cap*28] |
   // neighbour indices I[row_cap*32] | right-hand side V[b_cap].
   V* foot = reinterpret_cast<V*>(smem_raw);
@@ -244,144 +290,106 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
   const V* gb = reinterpret_cast<const V*>(L.b);
   V* xb0 = reinterpret_cast<V*>(L.xb0);
   V* xb1 = reinterpret_cast<V*>(L.xb1);
-  const int nx = L.n + 2;
   const int total_tasks = L.nvisits * L.strips;
-  constexpr int per16 = 16 / int(sizeof(V));  // right-hand-side elements per 16 bytes
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   uint32_t parity = 0;
+  // Takes the next task and loads its description into s_task[b], s_meta[b] (one warp).
+  auto fetch = [&](int b) {
+    int task = 0;
+    if (lane == 0) task = atomicAdd(L.counter, 1);
+    task = __shfl_sync(0xffffffffu, task, 0);
+    if (lane == 0) s_task[b] = task;
+    if (task < total_tasks) {
+      const int2 zt = L.visits[task / L.strips];
+      if (lane == 0) s_zt[b] = zt;
+      const int* src = reinterpret_cast<const int*>(L.meta + int64_t(zt.x) * L.strips + task % L.strips);
+      int* dst = reinterpret_cast<int*>(&s_meta[b]);
+      for (int i = lane; i < kMetaInts; i += 32) dst[i] = src[i];
+    }
+  };
   if (threadIdx.x == 0) mbar_init(&s_bar);
+  if (warp == 0) fetch(0);
   __syncthreads();
-  while (true) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      s_task = atomicAdd(L.counter, 1);
-      s_fail = 0;
-    }
-    __syncthreads();
-    const int task = s_task;
+  for (int buf = 0;; buf ^= 1) {
+    const int task = s_task[buf];
     if (task >= total_tasks) return;
-    long long* tr = (L.trace && threadIdx.x == 0) ? L.trace + int64_t(task) * 8 : nullptr;
+    const StripMeta& m = s_meta[buf];
+    long long* tr = (L.trace && threadIdx.x == 0) ? L.trace + int64_t(task) * kTraceSlots : nullptr;
+    long long* trc = (L.trace && threadIdx.x == 32) ? L.trace + int64_t(task) * kTraceSlots : nullptr;
+    const long long g0 = tr ? globaltimer() : 0;
+    const long long c0 = (tr || trc) ? clock64() : 0;
     if (tr) {
-      tr[0] = globaltimer();
-      tr[7] = blockIdx.x;
+      tr[0] = g0;
+      tr[15] = blockIdx.x;
     }
-    const int2 zt = L.visits[task / L.strips];
+    const int2 zt = s_zt[buf];
     const int z = zt.x, t = zt.y, s = task % L.strips;
-    // stored slice of a logical slice (the mirrored sweep reads the forward layout)
-    auto phys = [&](int zz) { return REV ? L.n - zz : zz; };
-    const int x0 = L.bounds[phys(z) * (L.strips + 1) + s], x1 = L.bounds[phys(z) * (L.strips + 1) + s + 1];
-    // All range lookups in one round: 24 footprint bounds, 8 update bounds, 8 own bounds.
-    if (threadIdx.x < 40) {
-      int i = threadIdx.x;
-      if (i < 24) {
-        int r = i >> 1, j = r >> 2, c = r & 3, zz = z + j - 1;
-        int v = 0;
-        if (zz >= 0 && zz <= L.n) {
-          int X = (i & 1) ? min(x1 + 4, L.n + 1) : max(x0 - 4, 0);
-          v = L.xstart[int64_t(phys(zz) * 4 + c) * nx + X];
-        }
-        if (i & 1)
-          s_hi[r] = v;
-        else
-          s_lo[r] = v;
-      } else {
-        int k = i - 24, c = (k >> 1) & 3, own = k >= 8, h = own ? 0 : (REV ? c : 3 - c);
-        int X = (k & 1) ? min(x1 + h, L.n + 1) : max(min(x0 - h, L.n + 1), 0);
-        int v = L.xstart[int64_t(phys(z) * 4 + c) * nx + X];
-        if (own) {
-          if (k & 1)
-            s_o1[c] = v;
-          else
-            s_o0[c] = v;
-        } else {
-          if (k & 1)
-            s_p1[c] = v;
-          else
-            s_p0[c] = v;
+    const bool staged = m.staged != 0;
+    const int total = m.base[12];
+    if (warp == 0) {
+      if (lane == 0) {
+        s_fail = 0;
+        if (total > L.cap) {
+          atomicExch(L.error, 2);
+          s_fail = 1;
         }
       }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int total = 0;
-      for (int r = 0; r < 12; ++r) {
-        s_base[r] = total;
-        total += s_hi[r] - s_lo[r];
-        int j = r >> 2, c = r & 3, zz = z + j - 1;
-        int gstart = (zz >= 0 && zz <= L.n) ? L.group_off[phys(zz) * 4 + c] : 0;
-        s_delta[r] = s_base[r] + gstart - s_lo[r];
-      }
-      s_base[12] = total;
-      s_total = total;
-      int rows = 0, bsum = 0;
-      for (int c = 0; c < 4; ++c) {
-        s_rbase[c] = rows;
-        rows += s_p1[c] - s_p0[c];
-        int a0 = s_p0[c] - s_p0[c] % per16, a1 = (s_p1[c] + per16 - 1) / per16 * per16;
-        s_bshift[c] = bsum + (s_p0[c] - a0);
-        bsum += s_p1[c] > s_p0[c] ? a1 - a0 : 0;
-      }
-      s_rbase[4] = rows;
-      s_rows = rows;
-      if (total > L.cap) {
-        atomicExch(L.error, 2);
-        s_fail = 1;
-      }
-      s_staged = !s_fail && rows <= L.row_cap && bsum <= L.b_cap;
-      if (s_staged) {
-        // Operator rows do not depend on x: copy them while the dependencies are pending.
-        fence_proxy_async();
-        uint32_t bytes = 0;
-        for (int c = 0; c < 4; ++c) {
-          int cnt = s_p1[c] - s_p0[c];
-          if (cnt <= 0) continue;
-          bytes += uint32_t(cnt) * (kSlotsR * sizeof(T) + kIdxSlots * sizeof(I));
-          int a0 = s_p0[c] - s_p0[c] % per16, a1 = (s_p1[c] + per16 - 1) / per16 * per16;
-          bytes += uint32_t(a1 - a0) * sizeof(V);
-        }
-        mbar_expect_tx(&s_bar, bytes);
-        int bpos = 0;
-        for (int c = 0; c < 4; ++c) {
-          int cnt = s_p1[c] - s_p0[c];
-          if (cnt <= 0) continue;
-          int p0 = s_p0[c];
-          bulk_copy(s_vals + int64_t(s_rbase[c]) * kSlotsR, gvals + int64_t(p0) * kSlotsR,
-                    uint32_t(cnt) * kSlotsR * sizeof(T), &s_bar);
-          bulk_copy(s_idx + int64_t(s_rbase[c]) * kIdxSlots, gidx + int64_t(p0) * kIdxSlots,
-                    uint32_t(cnt) * kIdxSlots * sizeof(I), &s_bar);
-          int a0 = p0 - p0 % per16, a1 = (s_p1[c] + per16 - 1) / per16 * per16;
-          bulk_copy(s_b + bpos, gb + a0, uint32_t(a1 - a0) * sizeof(V), &s_bar);
-          bpos += a1 - a0;
-        }
-      }
-      if (tr) tr[1] = globaltimer();
+      __syncwarp();
       // slice z after visit t-1 (two waves back); the newer dependencies are awaited below
       // while this slice is staged
-      bool ok = !s_fail;
-      if (ok) ok = wait_at_least(L.done + z * kPad, t * L.strips, L.error, L.poll_log2);
-      if (!ok) {
+      if (!s_fail && !wait_strips(L, z, m.dep_lo[1], m.dep_hi[1], t, lane) && lane == 0) {
         atomicCAS(L.error, 0, 1);
         s_fail = 1;
       }
-      if (tr) tr[2] = globaltimer();
+      if (tr && threadIdx.x == 0) tr[2] = clock64() - c0;
+    } else if (warp == 1) {
+      // Operator rows do not depend on x: one bulk copy per lane (values, indices and
+      // right-hand side of each colour's rows) lands them while warp 0 waits for the
+      // dependencies.  Issuing the copies takes ~0.8 us, so they are not on warp 0's path.
+      if (staged && total <= L.cap) {
+        if (lane == 0) mbar_expect_tx(&s_bar, m.bytes);
+        __syncwarp();
+        if (lane < 12) {
+          constexpr int per16 = 16 / int(sizeof(V));
+          const int c = lane / 3, kind = lane % 3;
+          const int p0 = m.p0[c], cnt = m.p1[c] - p0;
+          if (cnt > 0) {
+            fence_proxy_async();
+            if (kind == 0) {
+              bulk_copy(s_vals + int64_t(m.rbase[c]) * kSlotsR, gvals + int64_t(p0) * kSlotsR,
+                        uint32_t(cnt) * kSlotsR * sizeof(T), &s_bar);
+            } else if (kind == 1) {
+              bulk_copy(s_idx + int64_t(m.rbase[c]) * kIdxSlots, gidx + int64_t(p0) * kIdxSlots,
+                        uint32_t(cnt) * kIdxSlots * sizeof(I), &s_bar);
+            } else {
+              const int a0 = p0 - p0 % per16, a1 = (m.p1[c] + per16 - 1) / per16 * per16;
+              bulk_copy(s_b + (m.bshift[c] - p0 % per16), gb + a0, uint32_t(a1 - a0) * sizeof(V), &s_bar);
+            }
+          }
+        }
+      }
+      if (trc) trc[1] = clock64() - c0;
+    } else if (warp == nwarps - 1) {
+      // The last warp takes the next task and loads its description meanwhile (the other
+      // warps are idle until the barrier below).
+      fetch(buf ^ 1);
     }
     __syncthreads();
-    const bool staged = s_staged;
     if (s_fail) {
-      if (staged) mbar_wait(&s_bar, parity);  // never leave with copies in flight
+      if (staged && total <= L.cap) mbar_wait(&s_bar, parity);  // never leave with copies in flight
       return;
     }
-    if (tr) tr[3] = globaltimer();
+    if (tr && threadIdx.x == 0) tr[3] = clock64() - c0;
     // Stage the footprint: slice z+1 after visit t, slices z and z-1 after visit t-1.  Warp 0
     // waits for slices z+1 and z-1 while the other warps stage slice z, then all stage the rest.
     {
       const V* cur = (t & 1) ? xb1 : xb0;
       const V* prev = (t & 1) ? xb0 : xb1;
-      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
       // range r staged by `parts` warps, part `part` of them (4 loads in flight per lane)
       auto stage_range = [&](int r, int part, int parts) {
-        const V* src = ((r >> 2) == 2 ? cur : prev) + s_lo[r];
-        V* dst = foot + s_base[r];
-        const int cnt = s_hi[r] - s_lo[r];
+        const V* src = ((r >> 2) == 2 ? cur : prev) + m.lo[r];
+        V* dst = foot + m.base[r];
+        const int cnt = m.hi[r] - m.lo[r];
         for (int i0 = part * 128 + lane; i0 < cnt; i0 += 128 * parts) {
           V v[4];
 #pragma unroll
@@ -393,24 +401,22 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
         }
       };
       if (warp == 0) {
-        if (lane == 0) {
-          bool ok = true;
-          if (z + 1 <= L.n)
-            ok = wait_at_least(L.done + (z + 1) * kPad, (t + 1) * L.strips + (L.stall ? (1 << 30) : 0), L.error,
-                               L.poll_log2);
-          if (ok && z > 0) ok = wait_at_least(L.done + (z - 1) * kPad, t * L.strips, L.error, L.poll_log2);
-          if (!ok) {
-            atomicCAS(L.error, 0, 1);
-            s_fail = 1;
-          }
+        bool ok = true;
+        if (z + 1 <= L.n)
+          ok = wait_strips(L, z + 1, m.dep_lo[2], m.dep_hi[2], t + 1 + (L.stall ? (1 << 30) : 0), lane);
+        if (ok && z > 0) ok = wait_strips(L, z - 1, m.dep_lo[0], m.dep_hi[0], t, lane);
+        if (!ok && lane == 0) {
+          atomicCAS(L.error, 0, 1);
+          s_fail = 1;
         }
-        __syncwarp();
+        if (tr && threadIdx.x == 0) tr[4] = clock64() - c0;
       } else {
         // slice z: 4 ranges over the other warps
         const int parts = max(1, (nwarps - 1) / 4);
         for (int q = warp - 1; q < 4 * parts; q += nwarps - 1) stage_range(4 + q / parts, q % parts, parts);
       }
       __syncthreads();
+      if (tr && threadIdx.x == 0) tr[5] = clock64() - c0;
       if (s_fail) {
         if (staged) mbar_wait(&s_bar, parity);
         return;
@@ -423,43 +429,413 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) strip_gs_kernel(StripLevel L
         }
       }
     }
-    if (threadIdx.x == 0) foot[s_total] = V(0);  // the entry absent slots read
+    if (threadIdx.x == 0) foot[total] = V(0);  // the entry absent slots read
     if (staged && !mbar_wait(&s_bar, parity)) {
       if (threadIdx.x == 0) atomicExch(L.error, 4);
       return;
     }
     if (staged) parity ^= 1;
     __syncthreads();
-    if (tr) tr[4] = globaltimer();
+    if (tr && threadIdx.x == 0) tr[6] = clock64() - c0;
     {
       V* hv = L.hist ? reinterpret_cast<V*>(L.hist) + t : nullptr;
-#define PSR_PHASE(C, M)                                                                                          \
-  phase<C, M, T, V, I>(L, staged, s_p0[C], s_p1[C], s_rbase[C], s_bshift[C], s_idx, s_vals, s_b, foot, s_delta, \
-                       unsigned(s_total), hv, s_o0[C], s_o1[C]);                                               \
-  __syncthreads();
+      V* out = (t & 1) ? xb1 : xb0;
+#define PSR_PHASE(C, M, K)                                                \
+  phase<C, M, T, V, I>(L, m, staged, s_idx, s_vals, s_b, foot, hv, out); \
+  __syncthreads();                                                        \
+  if (tr && threadIdx.x == 0) tr[7 + K] = clock64() - c0;
       if (!REV) {
-        PSR_PHASE(0, false) PSR_PHASE(1, false) PSR_PHASE(2, false) PSR_PHASE(3, false)
+        PSR_PHASE(0, false, 0) PSR_PHASE(1, false, 1) PSR_PHASE(2, false, 2) PSR_PHASE(3, false, 3)
       } else {
-        PSR_PHASE(3, true) PSR_PHASE(2, true) PSR_PHASE(1, true) PSR_PHASE(0, true)
+        PSR_PHASE(3, true, 0) PSR_PHASE(2, true, 1) PSR_PHASE(1, true, 2) PSR_PHASE(0, true, 3)
       }
 #undef PSR_PHASE
     }
-    if (tr) tr[5] = globaltimer();
-    // Publish the strip's own rows (x in [x0, x1)) as visit t.
-    {
-      V* out = (t & 1) ? xb1 : xb0;
-      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-      for (int c = warp; c < 4; c += nwarps) {
-        const int o0 = s_o0[c], o1 = s_o1[c], base = s_base[4 + c] - s_lo[4 + c];
-        for (int p = o0 + lane; p < o1; p += 32) __stcg(out + p, foot[base + p]);
-      }
-    }
-    __syncthreads();
+    // The strip's own rows were published in their phases: release visit t.  (Measured: from
+    // another warp, overlapping the next task's bulk copies, the release takes longer and the
+    // launch is ~7% slower.)
     if (threadIdx.x == 0) {
       __threadfence();
-      atomicAdd(L.done + z * kPad, 1);
-      if (tr) tr[6] = globaltimer();
+      atomicMax(L.done + (int64_t(z) * L.strips + s) * kFlagPad, t + 1);
+      if (tr) tr[11] = clock64() - c0;
     }
+  }
+}
+
+// Task descriptions of one launch: one thread per (logical slice z, strip s).  Error 2: a
+// footprint exceeds the capacity (the kernel then stops before staging it).
+template <bool REV>
+__global__ void strip_meta_kernel(const int32_t* xstart, const int32_t* bounds, const int32_t* group_off, int n,
+                                  int strips, int per16, int cap, int row_cap, int b_cap, int row_bytes,
+                                  int vbytes, StripMeta* meta) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (n + 1) * strips) return;
+  const int z = idx / strips, s = idx % strips, nx = n + 2;
+  auto phys = [&](int zz) { return REV ? n - zz : zz; };
+  const int32_t* bz = bounds + int64_t(phys(z)) * (strips + 1);
+  const int x0 = bz[s], x1 = bz[s + 1];
+  const int xa = max(x0 - 4, 0), xb = min(x1 + 4, n + 1);
+  StripMeta m;
+  int total = 0;
+  for (int r = 0; r < 12; ++r) {
+    const int j = r >> 2, c = r & 3, zz = z + j - 1;
+    int lo = 0, hi = 0, gstart = 0;
+    if (zz >= 0 && zz <= n) {
+      const int32_t* xs = xstart + int64_t(phys(zz) * 4 + c) * nx;
+      lo = xs[xa];
+      hi = xs[xb];
+      gstart = group_off[phys(zz) * 4 + c];
+    }
+    m.lo[r] = lo;
+    m.hi[r] = hi;
+    m.base[r] = total;
+    m.delta[r] = total + gstart - lo;
+    total += hi - lo;
+  }
+  m.base[12] = total;
+  int rows = 0, bsum = 0;
+  uint32_t bytes = 0;
+  for (int c = 0; c < 4; ++c) {
+    const int32_t* xs = xstart + int64_t(phys(z) * 4 + c) * nx;
+    const int h = REV ? c : 3 - c;
+    const int p0 = xs[max(min(x0 - h, n + 1), 0)], p1 = xs[min(x1 + h, n + 1)];
+    m.p0[c] = p0;
+    m.p1[c] = p1;
+    m.o0[c] = xs[x0];
+    m.o1[c] = xs[min(x1, n + 1)];
+    m.rbase[c] = rows;
+    rows += p1 - p0;
+    const int a0 = p0 - p0 % per16, a1 = (p1 + per16 - 1) / per16 * per16;
+    m.bshift[c] = bsum + (p0 - a0);
+    if (p1 > p0) {
+      bsum += a1 - a0;
+      bytes += uint32_t(p1 - p0) * uint32_t(row_bytes) + uint32_t(a1 - a0) * uint32_t(vbytes);
+    }
+  }
+  m.rbase[4] = rows;
+  m.staged = total <= cap && rows <= row_cap && bsum <= b_cap;
+  m.bytes = bytes;
+  for (int j = 0; j < 3; ++j) {
+    const int zz = z + j - 1;
+    int lo = strips, hi = -1;
+    if (zz >= 0 && zz <= n) {
+      const int32_t* bb = bounds + int64_t(phys(zz)) * (strips + 1);
+      for (int sp = 0; sp < strips; ++sp)
+        if (bb[sp] < bb[sp + 1] && bb[sp] < xb && bb[sp + 1] > xa) {
+          lo = min(lo, sp);
+          hi = max(hi, sp);
+        }
+    }
+    m.dep_lo[j] = lo;
+    m.dep_hi[j] = hi;
+  }
+  for (int i = 0; i < 14; ++i) m.pad[i] = 0;
+  meta[idx] = m;
+}
+
+// ------------------------------------------------------------------ cluster pipelines
+// The same order run as one pipeline per visit.  Visit t's pipeline is one cluster of
+// kPipeCtas CTAs (strip s = rank) that relaxes slices z = 2^d .. 0 in turn (step = 2^d - z),
+// which is the order in which the sequential sweep gives visit t to the slices.  Visit t of
+// slice z needs:
+//  * slice z+1 after visit t -- the previous step of the same pipeline: each CTA keeps its
+//    own rows' new values of every step in an export buffer in shared memory, and the CTAs
+//    read their neighbours' through distributed shared memory after a cluster barrier;
+//  * slices z and z-1 after visit t-1 -- pipeline t-1, one and two steps earlier: through
+//    global memory (x buffer of visit parity t-1) and per-strip completion counts, as in the
+//    dynamic scheduler above, staged by helper warps during the previous step.
+// So a step costs its four colour phases, one cluster barrier and the neighbour exchange in
+// shared memory; the global-memory hand-off between pipelines is paid once per visit (the
+// pipelines run staggered), not once per slice.  Operator rows are brought in per colour phase
+// by bulk copies into three rotating regions, issued three phases ahead.
+//
+// Warps 0..11 update rows; warp 12 loads the next step's task description and issues the bulk
+// copies and the release of each step; warps 13..15 stage the next step's global ranges.  Every
+// wait is bounded; after an error the CTAs keep taking part in the barriers (skipping the work)
+// until the loop ends, so no barrier is left waiting, and drain their copies before exiting.
+constexpr int kPipeCtas = 8;
+constexpr int kPipeRowThreads = 384;
+constexpr int kPipeRegions = 3;
+constexpr int kMaxPeerSegs = 40;
+
+struct PeerSeg {
+  int rank, src, dst, count;  // values [src, src+count) of CTA `rank`'s export -> footprint [dst, dst+count)
+};
+struct PipeMeta {
+  StripMeta m;
+  int ebase[5];  // export offset of each colour's own rows (colour-major); ebase[4] = own rows
+  int nseg, overflow, pad;
+  PeerSeg seg[kMaxPeerSegs];  // the slice z+1 footprint ranges, by owner
+};
+constexpr int kPipeMetaInts = int(sizeof(PipeMeta) / 4);
+static_assert(sizeof(PipeMeta) % 16 == 0, "PipeMeta is copied as ints into 16-byte aligned shared memory");
+
+struct PipeLevel {
+  StripLevel L;  // n, strips (= kPipeCtas), vals, nidx, b, xb0, xb1, done, error, hist, iters, ...
+  const PipeMeta* meta;
+  int cap;       // footprint elements
+  int rcap;      // rows per region
+  int bcap;      // right-hand-side elements per region
+  int ecap;      // exported values per step
+  int64_t off_foot[2], off_vals[kPipeRegions], off_idx[kPipeRegions], off_b[kPipeRegions], off_exp[2], off_meta[2];
+};
+
+__device__ __forceinline__ void bar_named(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+template <int C, bool M, class T, class V, class I>
+__device__ __forceinline__ void pipe_phase(const StripLevel& L, const StripMeta& m, const int* ebase, const I* r_idx,
+                                           const T* r_vals, const V* r_b, V* foot, V* hist, V* out, V* expo) {
+  constexpr int per16 = 16 / int(sizeof(V));
+  const bool inc = L.record_increment != 0;
+  const int p0 = m.p0[C], p1 = m.p1[C], o0 = m.o0[C], o1 = m.o1[C], bshift = p0 % per16;
+  const unsigned total = unsigned(m.base[12]);
+  int dreg[12];
+#pragma unroll
+  for (int r = 0; r < 12; ++r) dreg[r] = m.delta[r];
+  for (int p = p0 + int(threadIdx.x); p < p1; p += kPipeRowThreads) {
+    const bool own = p >= o0 && p < o1;
+    V* rec = (hist && own) ? hist + int64_t(p) * L.iters : nullptr;
+    const int i = p - p0;
+    update_row<C, M>(r_idx + int64_t(i) * kIdxSlots, p, r_vals + int64_t(i) * kSlotsR, r_b[bshift + i], foot, dreg,
+                     total, L.error, rec, inc, own ? out + p : nullptr, own ? expo + ebase[C] + (p - o0) : nullptr);
+  }
+}
+
+template <class T, class V, class I, bool REV>
+__global__ void __launch_bounds__(kRelaxThreads, 1) pipeline_gs_kernel(PipeLevel P) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t s_full[kPipeRegions];   // rows of the region's phase have landed
+  __shared__ uint64_t s_empty[kPipeRegions];  // the region's phase is done with them
+  __shared__ int s_err;
+  const StripLevel& L = P.L;
+  const int t = int(blockIdx.x) / kPipeCtas;
+  const int s = int(cluster.block_rank());
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nsteps = L.n + 1, nphases = 4 * nsteps;
+  V* foot[2] = {reinterpret_cast<V*>(smem_raw + P.off_foot[0]), reinterpret_cast<V*>(smem_raw + P.off_foot[1])};
+  V* expo[2] = {reinterpret_cast<V*>(smem_raw + P.off_exp[0]), reinterpret_cast<V*>(smem_raw + P.off_exp[1])};
+  PipeMeta* sm[2] = {reinterpret_cast<PipeMeta*>(smem_raw + P.off_meta[0]),
+                     reinterpret_cast<PipeMeta*>(smem_raw + P.off_meta[1])};
+  const T* gvals = reinterpret_cast<const T*>(L.vals);
+  const I* gidx = reinterpret_cast<const I*>(L.nidx);
+  const V* gb = reinterpret_cast<const V*>(L.b);
+  V* xout = reinterpret_cast<V*>((t & 1) ? L.xb1 : L.xb0);         // x after visit t
+  const V* xprev = reinterpret_cast<const V*>((t & 1) ? L.xb0 : L.xb1);  // after visit t-1 (t = 0: initial x)
+  V* hv = L.hist ? reinterpret_cast<V*>(L.hist) + t : nullptr;
+  if (threadIdx.x == 0) {
+    for (int r = 0; r < kPipeRegions; ++r) {
+      mbar_init(&s_full[r]);
+      mbar_init(&s_empty[r]);
+    }
+    s_err = 0;
+  }
+  auto fail = [&](int code) {
+    atomicCAS(L.error, 0, code);
+    s_err = 1;
+  };
+  // warp 12: the task description of a step into sm[step & 1]
+  auto load_meta = [&](int step) {
+    const int z = L.n - step;
+    const int* src = reinterpret_cast<const int*>(P.meta + (int64_t(z) * kPipeCtas + s));
+    int* dst = reinterpret_cast<int*>(sm[step & 1]);
+    for (int i = lane; i < kPipeMetaInts; i += 32) dst[i] = src[i];
+  };
+  int last_issued[kPipeRegions] = {-1, -1, -1};  // thread 384: the last phase issued into each region
+  // thread 384: bulk copies of phase k's rows into region k % 3 (empty phases only arrive)
+  auto issue = [&](int k) {
+    last_issued[k % kPipeRegions] = k;
+    constexpr int per16 = 16 / int(sizeof(V));
+    const int step = k / 4, col = REV ? 3 - k % 4 : k % 4, r = k % kPipeRegions;
+    const StripMeta& m = sm[step & 1]->m;
+    const int p0 = m.p0[col], cnt = m.p1[col] - p0;
+    const int a0 = p0 - p0 % per16, a1 = (m.p1[col] + per16 - 1) / per16 * per16;
+    const bool ok = cnt > 0 && cnt <= P.rcap && a1 - a0 <= P.bcap;
+    if (cnt > 0 && !ok) fail(2);
+    const uint32_t bytes =
+        ok ? uint32_t(cnt) * (kSlotsR * sizeof(T) + kIdxSlots * sizeof(I)) + uint32_t(a1 - a0) * sizeof(V) : 0;
+    fence_proxy_async();
+    mbar_expect_tx(&s_full[r], bytes);
+    if (ok) {
+      bulk_copy(smem_raw + P.off_vals[r], gvals + int64_t(p0) * kSlotsR, uint32_t(cnt) * kSlotsR * sizeof(T),
+                &s_full[r]);
+      bulk_copy(smem_raw + P.off_idx[r], gidx + int64_t(p0) * kIdxSlots, uint32_t(cnt) * kIdxSlots * sizeof(I),
+                &s_full[r]);
+      bulk_copy(smem_raw + P.off_b[r], gb + a0, uint32_t(a1 - a0) * sizeof(V), &s_full[r]);
+    }
+  };
+  // warps 13..15: footprint ranges of slices z and z-1 after visit t-1 for a step, into
+  // foot[step & 1], once pipeline t-1 has published them
+  auto stage_global = [&](int step) {
+    const StripMeta& m = sm[step & 1]->m;
+    const int z = L.n - step;
+    const int ht = threadIdx.x - 13 * 32;  // 0..95
+    if (warp == 13) {
+      bool ok = !s_err;
+      if (ok) ok = wait_strips(L, z, m.dep_lo[1], m.dep_hi[1], t, lane);
+      if (ok && z > 0) ok = wait_strips(L, z - 1, m.dep_lo[0], m.dep_hi[0], t, lane);
+      if (!ok && lane == 0 && !s_err) fail(1);
+    }
+    bar_named(3, 96);
+    if (s_err) return;
+    V* f = foot[step & 1];
+    for (int r = 0; r < 8; ++r) {
+      const V* src = xprev + m.lo[r];
+      V* dst = f + m.base[r];
+      const int cnt = m.hi[r] - m.lo[r];
+      for (int i0 = ht; i0 < cnt; i0 += 4 * 96) {
+        V v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (i0 + 96 * u < cnt) v[u] = __ldcg(src + i0 + 96 * u);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (i0 + 96 * u < cnt) dst[i0 + 96 * u] = v[u];
+      }
+    }
+  };
+  __syncthreads();
+  // prologue: step 0's description, its first three phases' rows, its global ranges
+  if (warp == 12) load_meta(0);
+  __syncthreads();
+  if (threadIdx.x == 12 * 32)
+    for (int k = 0; k < kPipeRegions && k < nphases; ++k) issue(k);
+  if (warp >= 13) stage_global(0);
+  __syncthreads();
+  cluster.sync();  // every CTA of the cluster has initialised its shared memory
+  for (int step = 0; step < nsteps; ++step) {
+    const int z = L.n - step, fb = step & 1;
+    const PipeMeta& pm = *sm[fb];
+    const StripMeta& m = pm.m;
+    // slice z+1 after visit t: the peers' exports of the previous step
+    if (warp < 12 && step > 0 && !s_err) {
+      for (int g = 0; g < pm.nseg; ++g) {
+        const PeerSeg sg = pm.seg[g];
+        const V* remote = cluster.map_shared_rank(expo[(step - 1) & 1], sg.rank);
+        for (int i = threadIdx.x; i < sg.count; i += kPipeRowThreads) foot[fb][sg.dst + i] = remote[sg.src + i];
+      }
+    }
+    if (threadIdx.x == 0) foot[fb][m.base[12]] = V(0);
+    __syncthreads();
+    if (warp < 12) {
+#define PSR_PIPE_PHASE(CI)                                                                                         \
+  {                                                                                                                \
+    const int k = 4 * step + CI;                                                                                   \
+    constexpr int col = REV ? 3 - CI : CI;                                                                         \
+    const int r = k % kPipeRegions;                                                                                \
+    if (!s_err && !mbar_wait(&s_full[r], uint32_t(k / kPipeRegions) & 1)) fail(4);                              \
+    if (!s_err)                                                                                                    \
+      pipe_phase<col, REV, T, V, I>(L, m, pm.ebase, reinterpret_cast<const I*>(smem_raw + P.off_idx[r]),          \
+                                    reinterpret_cast<const T*>(smem_raw + P.off_vals[r]),                          \
+                                    reinterpret_cast<const V*>(smem_raw + P.off_b[r]), foot[fb], hv, xout,         \
+                                    expo[fb]);                                                                     \
+    bar_named(1, kPipeRowThreads);                                                                                 \
+    if (threadIdx.x == 0) mbar_arrive(&s_empty[r]);                                                                \
+  }
+      PSR_PIPE_PHASE(0) PSR_PIPE_PHASE(1) PSR_PIPE_PHASE(2) PSR_PIPE_PHASE(3)
+#undef PSR_PIPE_PHASE
+    } else if (warp == 12) {
+      if (step + 1 < nsteps) load_meta(step + 1);
+      __syncwarp();
+      bar_named(2, 128);  // the next step's description is in place for warps 13..15
+      if (lane == 0) {
+        for (int ci = 0; ci < 4; ++ci) {
+          // region k % 3 is free once phase k is done; then the copies of phase k + 3 go in.
+          // (One full and one empty barrier per region: neither can run a phase ahead of the
+          // other, so a parity wait never confuses two phases.)
+          const int k = 4 * step + ci;
+          if (!mbar_wait(&s_empty[k % kPipeRegions], uint32_t(k / kPipeRegions) & 1) && !s_err) fail(4);
+          if (k + kPipeRegions < nphases && !s_err) issue(k + kPipeRegions);
+        }
+        if (!s_err) {  // release slice z after visit t to pipeline t+1
+          __threadfence();
+          atomicMax(L.done + (int64_t(z) * L.strips + s) * kFlagPad, t + 1);
+        }
+      }
+      __syncwarp();
+    } else {
+      bar_named(2, 128);
+      if (step + 1 < nsteps) stage_global(step + 1);
+    }
+    cluster.sync();
+  }
+  // never leave with copies in flight (after an error some were not consumed)
+  if (threadIdx.x == 12 * 32)
+    for (int r = 0; r < kPipeRegions; ++r)
+      if (last_issued[r] >= 0) mbar_wait(&s_full[r], uint32_t(last_issued[r] / kPipeRegions) & 1);
+  __syncthreads();
+}
+
+// Peer segments and export offsets of the cluster pipelines, one thread per (logical slice z,
+// strip s); meta holds the StripMeta of the same tasks.
+template <bool REV>
+__global__ void pipe_meta_kernel(const StripMeta* strip_meta, const int32_t* xstart, const int32_t* bounds, int n,
+                                 PipeMeta* meta, int* caps) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (n + 1) * kPipeCtas) return;
+  const int z = idx / kPipeCtas, nx = n + 2;
+  auto phys = [&](int zz) { return REV ? n - zz : zz; };
+  PipeMeta pm;
+  pm.m = strip_meta[idx];
+  const StripMeta& m = pm.m;
+  int e = 0;
+  for (int c = 0; c < 4; ++c) {
+    pm.ebase[c] = e;
+    e += m.o1[c] - m.o0[c];
+  }
+  pm.ebase[4] = e;
+  pm.nseg = 0;
+  pm.overflow = 0;
+  pm.pad = 0;
+  const int zz = z + 1;
+  if (zz <= n) {
+    const int32_t* bb = bounds + int64_t(phys(zz)) * (kPipeCtas + 1);
+    for (int sp = m.dep_lo[2]; sp <= m.dep_hi[2]; ++sp) {
+      int ob[5], o0s[4], o1s[4], acc = 0;
+      for (int c = 0; c < 4; ++c) {
+        const int32_t* xs = xstart + int64_t(phys(zz) * 4 + c) * nx;
+        o0s[c] = xs[bb[sp]];
+        o1s[c] = xs[bb[sp + 1]];
+        ob[c] = acc;
+        acc += o1s[c] - o0s[c];
+      }
+      for (int c = 0; c < 4; ++c) {
+        const int r = 8 + c;
+        const int a = max(m.lo[r], o0s[c]), b = min(m.hi[r], o1s[c]);
+        if (a >= b) continue;
+        if (pm.nseg < kMaxPeerSegs) {
+          pm.seg[pm.nseg] = PeerSeg{sp, ob[c] + (a - o0s[c]), m.base[r] + (a - m.lo[r]), b - a};
+          ++pm.nseg;
+        } else {
+          pm.overflow = 1;
+        }
+      }
+    }
+  }
+  for (int g = pm.nseg; g < kMaxPeerSegs; ++g) pm.seg[g] = PeerSeg{0, 0, 0, 0};
+  meta[idx] = pm;
+  // capacities: footprint, rows per colour, exported values, overflow (right-hand-side spans:
+  // pipe_bspan_kernel)
+  atomicMax(caps + 0, m.base[12]);
+  for (int c = 0; c < 4; ++c) atomicMax(caps + 1, m.p1[c] - m.p0[c]);
+  atomicMax(caps + 3, e);
+  if (pm.overflow) atomicMax(caps + 4, 1);
+}
+
+__global__ void pipe_bspan_kernel(const PipeMeta* meta, int count, int per16, int* caps) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= count) return;
+  const StripMeta& m = meta[idx].m;
+  for (int c = 0; c < 4; ++c) {
+    if (m.p1[c] <= m.p0[c]) continue;
+    const int a0 = m.p0[c] - m.p0[c] % per16, a1 = (m.p1[c] + per16 - 1) / per16 * per16;
+    atomicMax(caps + 2, a1 - a0);
   }
 }
 
@@ -548,6 +924,25 @@ __global__ void footprint_kernel(const int32_t* xstart, const int32_t* bounds, i
   atomicMax(caps, total);
 }
 
+// Tasks whose update rows or right-hand sides exceed the staging capacity (they read their
+// rows from global memory), added to *count.
+__global__ void unstaged_kernel(const int32_t* xstart, const int32_t* bounds, int n, int strips, int per16, int rev,
+                                int row_cap, int b_cap, int* count) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (n + 1) * strips) return;
+  int z = idx / strips, s = idx % strips, nx = n + 2;
+  int x0 = bounds[z * (strips + 1) + s], x1 = bounds[z * (strips + 1) + s + 1];
+  int rows = 0, bspan = 0;
+  for (int c = 0; c < 4; ++c) {
+    const int32_t* xs = xstart + int64_t(z * 4 + c) * nx;
+    int h = rev ? c : 3 - c;
+    int p0 = xs[max(min(x0 - h, n + 1), 0)], p1 = xs[min(x1 + h, n + 1)];
+    rows += p1 - p0;
+    if (p1 > p0) bspan += (p1 + per16 - 1) / per16 * per16 - (p0 - p0 % per16);
+  }
+  if (rows > row_cap || bspan > b_cap) atomicAdd(count, 1);
+}
+
 __global__ void inverse_kernel(const int32_t* perm, int64_t n, int32_t* inv) {
   int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (p < n) inv[perm[p]] = int32_t(p);
@@ -568,17 +963,18 @@ __global__ void reorder_kernel(const int32_t* perm, const int32_t* inv, const in
   int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (p >= n) return;
   int64_t row = perm[p];
+  __align__(16) I idx[kIdxSlots];
   for (int k = 0; k < kSlotsR; ++k) {
     int32_t c = k < 27 ? cols[row * kSlotsR + k] : -1;
-    I idx = idx_absent<I>();
-    if (c >= 0) idx = I(inv[c] - group_off[group_of(keys[c])]);
+    idx[k] = idx_absent<I>();
+    if (c >= 0) idx[k] = I(inv[c] - group_off[group_of(keys[c])]);
     svals[p * kSlotsR + k] = k < 27 ? vals[row * kSlotsR + k] : T(0);
-    sidx[p * kIdxSlots + k] = idx;
   }
-  sidx[p * kIdxSlots + 27] = I(p - group_off[group_of(keys[row])]);
-  for (int k = 28; k < kIdxSlots; ++k) sidx[p * kIdxSlots + k] = I(-1);
+  idx[27] = I(p - group_off[group_of(keys[row])]);
+  for (int k = 28; k < kIdxSlots; ++k) idx[k] = I(-1);
   const T diag = vals[row * kSlotsR + 13];
-  put_inv_diag<V>(sidx + p * kIdxSlots, diag != T(0) ? V(1.0) / V(diag) : V(0));
+  put_inv_diag<V>(idx, diag != T(0) ? V(1.0) / V(diag) : V(0));
+  store_idx_row(sidx + p * kIdxSlots, p, idx);
   sb[p] = b[row];
   sx[p] = x[row];
   skeys[p] = keys[row];
@@ -641,10 +1037,156 @@ static int device_smem_optin() {
   return bytes;
 }
 
+static int device_smem_per_sm() {
+  static int bytes = 0;
+  if (!bytes) {
+    int dev = 0;
+    PSR_CUDA(cudaGetDevice(&dev));
+    PSR_CUDA(cudaDeviceGetAttribute(&bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  }
+  return bytes;
+}
+
 template <class V>
 __global__ void gather_x_kernel(const int32_t* perm, int64_t n, const V* x, V* sx) {
   int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (p < n) sx[p] = x[perm[p]];
+}
+
+// The cluster pipelines for one level, when they apply: every task's rows fit a region and
+// its footprint, peer segments and exports fit shared memory, and `iters` clusters of
+// kPipeCtas CTAs can be resident at once.  Returns false (nothing launched) otherwise.
+// PSR_RELAX_KERNEL=strip keeps the dynamic scheduler; =pipeline asks for the pipelines even
+// when a test override of the dynamic scheduler is set.
+template <class T, class V, class I>
+static bool relax_pipeline(const StripSchedule& S, const T* svals, const I* sidx, const V* sb, const int32_t* xstart,
+                           V* xb0, V* xb1, int iters, cudaStream_t s, float* ms, V* hist, bool rev,
+                           bool record_increment) {
+  const char* mode = std::getenv("PSR_RELAX_KERNEL");
+  const bool forced = mode && std::string(mode) == "pipeline";
+  if (!forced) return false;  // opt-in until validated on hardware
+  if (!forced && (std::getenv("PSR_RELAX_STRIPS") || std::getenv("PSR_RELAX_ROW_CAP") ||
+                  std::getenv("PSR_RELAX_FOOTPRINT_LIMIT") || std::getenv("PSR_RELAX_STALL_TEST")))
+    return false;
+  const int depth = S.depth, n = 1 << depth, strips = kPipeCtas;
+  const int per16 = 16 / int(sizeof(V));
+  if (int64_t(iters) * kPipeCtas > device_sms()) return false;
+  const int ntasks = (n + 1) * strips;
+  DBuf<int32_t> bounds(int64_t(n + 1) * (strips + 1), s);
+  strip_bounds_kernel<<<blocks_for(int64_t(n + 1) * (strips + 1)), kThreads, 0, s>>>(xstart, n, strips, bounds.p);
+  PSR_LAUNCH_CHECK();
+  DBuf<int> caps(8, s);
+  caps.zero();
+  footprint_kernel<<<blocks_for(ntasks), kThreads, 0, s>>>(xstart, bounds.p, n, strips, per16, rev ? 1 : 0, caps.p);
+  PSR_LAUNCH_CHECK();
+  std::vector<int> fcap = read_vector(caps.p, 3, s);
+  if (sizeof(I) == 2 && fcap[0] > 32767) return false;
+  const int big = 1 << 30;
+  DBuf<StripMeta> smeta(ntasks, s);
+  auto mk = rev ? strip_meta_kernel<true> : strip_meta_kernel<false>;
+  mk<<<blocks_for(ntasks, 128), 128, 0, s>>>(xstart, bounds.p, S.off.p, n, strips, per16, big, big, big,
+                                             kSlotsR * int(sizeof(T)) + kIdxSlots * int(sizeof(I)), int(sizeof(V)),
+                                             smeta.p);
+  PSR_LAUNCH_CHECK();
+  DBuf<PipeMeta> meta(ntasks, s);
+  caps.zero();
+  auto pk = rev ? pipe_meta_kernel<true> : pipe_meta_kernel<false>;
+  pk<<<blocks_for(ntasks, 64), 64, 0, s>>>(smeta.p, xstart, bounds.p, n, meta.p, caps.p);
+  PSR_LAUNCH_CHECK();
+  pipe_bspan_kernel<<<blocks_for(ntasks), kThreads, 0, s>>>(meta.p, ntasks, per16, caps.p);
+  PSR_LAUNCH_CHECK();
+  std::vector<int> c = read_vector(caps.p, 5, s);
+  if (c[4]) return false;  // more peer segments than a task description holds
+  PipeLevel P{};
+  P.cap = std::max(c[0], 1);
+  P.rcap = std::max(c[1], 1);
+  P.bcap = std::max(c[2], per16);
+  P.ecap = std::max(c[3], 1);
+  auto al = [](int64_t b) { return (b + 127) & ~int64_t(127); };
+  int64_t off = 0;
+  for (int f = 0; f < 2; ++f) {
+    P.off_foot[f] = off;
+    off += al(int64_t(P.cap + 1) * int64_t(sizeof(V)));
+  }
+  for (int r = 0; r < kPipeRegions; ++r) {
+    P.off_vals[r] = off;
+    off += al(int64_t(P.rcap) * kSlotsR * int64_t(sizeof(T)));
+    P.off_idx[r] = off;
+    off += al(int64_t(P.rcap) * kIdxSlots * int64_t(sizeof(I)));
+    P.off_b[r] = off;
+    off += al(int64_t(P.bcap) * int64_t(sizeof(V)));
+  }
+  for (int f = 0; f < 2; ++f) {
+    P.off_exp[f] = off;
+    off += al(int64_t(P.ecap) * int64_t(sizeof(V)));
+  }
+  for (int f = 0; f < 2; ++f) {
+    P.off_meta[f] = off;
+    off += al(int64_t(sizeof(PipeMeta)));
+  }
+  const int64_t budget = int64_t(device_smem_optin()) - 2048;  // static shared memory of the kernel
+  if (off > budget) return false;
+  auto kernel = rev ? pipeline_gs_kernel<T, V, I, true> : pipeline_gs_kernel<T, V, I, false>;
+  PSR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(off)));
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kPipeCtas;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(unsigned(iters * kPipeCtas));
+  cfg.blockDim = dim3(kRelaxThreads);
+  cfg.dynamicSmemBytes = size_t(off);
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (clusters < iters) return false;
+  DBuf<int> ctrl(64, s);  // error word
+  ctrl.zero();
+  DBuf<int> done(int64_t(ntasks) * kFlagPad, s);
+  done.zero();
+  StripLevel& L = P.L;
+  L.n = n;
+  L.strips = strips;
+  L.vals = svals;
+  L.nidx = sidx;
+  L.b = sb;
+  L.xb0 = xb0;
+  L.xb1 = xb1;
+  L.done = done.p;
+  L.error = ctrl.p;
+  L.hist = hist;
+  L.rows = S.rows;
+  L.iters = iters;
+  L.record_increment = record_increment ? 1 : 0;
+  L.poll_log2 = 26;
+  L.cap = P.cap;
+  P.meta = meta.p;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ms) {
+    PSR_CUDA(cudaEventCreate(&e0));
+    PSR_CUDA(cudaEventCreate(&e1));
+    PSR_CUDA(cudaEventRecord(e0, s));
+  }
+  PSR_CUDA(cudaLaunchKernelEx(&cfg, kernel, P));
+  PSR_LAUNCH_CHECK();
+  if (ms) PSR_CUDA(cudaEventRecord(e1, s));
+  const int err = read_scalar(L.error, s);
+  if (ms) {
+    PSR_CUDA(cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  if (err == 2) throw Error(4, "ordered relaxation: a task's rows exceed their region");
+  if (err == 3) throw Error(1, "ordered relaxation: an operator column is not its slot's neighbour");
+  if (err == 4) throw Error(4, "ordered relaxation: a bulk copy or a phase did not complete");
+  if (err) throw Error(4, "ordered relaxation: a dependency wait timed out");
+  return true;
 }
 
 template <class T, class V, class I>
@@ -665,23 +1207,35 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
   DBuf<int32_t> xstart(int64_t(n + 1) * 4 * nx, s);
   xstart_kernel<<<blocks_for(int64_t(n + 1) * 4 * nx), kThreads, 0, s>>>(skeys_p, off, n, xstart.p);
   PSR_LAUNCH_CHECK();
-  // Strips per slice: a wave (iters x strips tasks) fills about two thirds of the persistent
+  if (relax_pipeline<T, V, I>(S, svals, sidx, sb, xstart.p, x0.p, x1.p, iters, s, ms, hist, rev, record_increment)) {
+    scatter_back_kernel<V><<<blocks_for(rows), kThreads, 0, s>>>(perm, rows, ((iters - 1) & 1) ? x1.p : x0.p, x);
+    PSR_LAUNCH_CHECK();
+    return;
+  }
+  // Strips per slice: a wave (iters x strips tasks) fills about seven eighths of the persistent
   // grid, leaving CTAs that take the next wave's tasks early and prefetch their operator rows;
-  // at least ~128 rows per strip.  (Measured at depth 9, 8 sweeps, 148 SMs: 12 strips 4.4 ms,
-  // 9 strips 7.0 ms, 18 strips 4.6 ms, 24 strips 5.9 ms.)
+  // at least ~128 rows per strip.  More strips are taken (up to twice as many) while more than
+  // 5% of the tasks would not fit their rows in shared memory.  Measured at depth 9, 8 sweeps,
+  // 148 SMs (finest level, ms): mixed 12/14/16/18/20/24 strips 3.28/3.04/3.01/3.15/3.40/3.99;
+  // float64 (wider rows) 12/16/20/24 strips 9.40/5.83/4.38/4.48.
   const int sms = device_sms();
+  const int ctas = kRelaxCtasPerSm * sms;
   int strips = int(std::max<int64_t>(
-      1, std::min<int64_t>(std::max(1, (2 * sms) / (3 * iters)), rows / (int64_t(n + 1) * 128))));
+      1, std::min<int64_t>(std::max(1, (7 * ctas) / (8 * iters)), rows / (int64_t(n + 1) * 128))));
   // Tuning override of the strips per slice (sweeps; the default above is the measured choice).
+  bool forced_strips = false;
   if (const char* env = std::getenv("PSR_RELAX_STRIPS")) {
     const int forced = std::atoi(env);
-    if (forced >= 1 && forced <= 256) strips = forced;
+    if (forced >= 1 && forced <= 256) {
+      strips = forced;
+      forced_strips = true;
+    }
   }
-  const int64_t pad_end = int64_t(n + 1) * kPad;
-  DBuf<int> flags(pad_end + 4 * kPad, s);
-  int* counter = flags.p + pad_end;
-  int* error = flags.p + pad_end + kPad;
-  int* caps_dev = flags.p + pad_end + 2 * kPad;
+  const int base_strips = strips;
+  DBuf<int> ctrl(3 * 32, s);  // task counter, error word, capacities: one 128-byte line each
+  int* counter = ctrl.p;
+  int* error = ctrl.p + 32;
+  int* caps_dev = ctrl.p + 64;
   DBuf<int32_t> bounds;
   std::vector<int> caps;
   // 16-bit index rows reach the footprint through offsets below 2^15 (idx_absent).
@@ -692,19 +1246,44 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
     const int forced = std::atoi(env);
     if (forced >= 1 && forced < fp_limit) fp_limit = forced;
   }
+  // Shared memory of one CTA: the footprint (and its +0 entry), the staged rows and their
+  // right-hand sides.
+  const int64_t budget = std::min<int64_t>(device_smem_optin(), device_smem_per_sm() / kRelaxCtasPerSm) - 4096;
+  const int64_t row_bytes = kSlotsR * int64_t(sizeof(T)) + kIdxSlots * int64_t(sizeof(I));
+  auto fp_bytes_of = [&](int fp) { return (int64_t(std::max(fp, 1) + 1) * int64_t(sizeof(V)) + 15) & ~int64_t(15); };
+  // staged rows and right-hand-side elements that fit beside a footprint of fp elements
+  auto row_capacity = [&](int fp, int maxrows, int maxb) {
+    int64_t rc = std::max<int64_t>(0, std::min<int64_t>(maxrows, (budget - fp_bytes_of(fp) - 4 * 16) /
+                                                                       (row_bytes + int64_t(sizeof(V)))));
+    return std::make_pair(rc, std::min<int64_t>(maxb, rc + 4 * per16) / per16 * per16);
+  };
   while (true) {
     bounds.alloc(int64_t(n + 1) * (strips + 1), s);
     strip_bounds_kernel<<<blocks_for(int64_t(n + 1) * (strips + 1)), kThreads, 0, s>>>(xstart.p, n, strips,
                                                                                         bounds.p);
     PSR_LAUNCH_CHECK();
-    flags.zero();
+    ctrl.zero();
     footprint_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, bounds.p, n, strips, per16,
                                                                         rev ? 1 : 0, caps_dev);
     PSR_LAUNCH_CHECK();
     caps = read_vector(caps_dev, 3, s);
+    const auto cap = row_capacity(caps[0], caps[1], caps[2]);
+    unstaged_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, bounds.p, n, strips, per16,
+                                                                       rev ? 1 : 0, int(cap.first), int(cap.second),
+                                                                       caps_dev + 3);
+    PSR_LAUNCH_CHECK();
+    caps.push_back(read_scalar(caps_dev + 3, s));
     // narrow the strips until the largest footprint fits the 16-bit offsets
-    if (sizeof(I) == 4 || caps[0] <= fp_limit || strips >= 256) break;
-    strips = std::min(256, 2 * strips);
+    if (!(sizeof(I) == 4 || caps[0] <= fp_limit) && strips < 256) {
+      strips = std::min(256, 2 * strips);
+      continue;
+    }
+    // then while more than 5% of the tasks would run unstaged (wide rows: float64 values)
+    if (!forced_strips && int64_t(caps[3]) * 20 > int64_t(n + 1) * strips && strips < std::min(256, 2 * base_strips)) {
+      strips = std::min({256, 2 * base_strips, strips + std::max(1, strips / 4)});
+      continue;
+    }
+    break;
   }
   if (sizeof(I) == 2 && caps[0] > fp_limit)
     throw Error(4, "ordered relaxation: a strip footprint exceeds the 16-bit index range");
@@ -723,16 +1302,15 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
   L.n = n;
   L.strips = strips;
   L.nvisits = int(visits.size());
-  L.bounds = bounds.p;
-  L.group_off = off;
   L.vals = svals;
   L.nidx = sidx;
   L.b = sb;
   L.xb0 = x0.p;
   L.xb1 = x1.p;
-  L.xstart = xstart.p;
   L.visits = dvisits.p;
-  L.done = flags.p;
+  DBuf<int> done(int64_t(n + 1) * strips * kFlagPad, s);
+  done.zero();
+  L.done = done.p;
   L.counter = counter;
   L.error = error;
   L.hist = hist;
@@ -749,14 +1327,10 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
       L.poll_log2 = 12;
     }
   // Shared memory: the footprint, plus the staged rows of tasks that fit.
-  const int64_t budget = std::min<int64_t>(device_smem_optin() - 4096, 220 * 1024);
-  // the footprint plus its +0 entry at index `total`
-  const int64_t fp_bytes = (int64_t(std::max(maxfp, 1) + 1) * int64_t(sizeof(V)) + 15) & ~int64_t(15);
+  const int64_t fp_bytes = fp_bytes_of(maxfp);
   if (fp_bytes > budget) throw Error(4, "ordered relaxation: a strip footprint exceeds shared memory");
-  const int64_t per_row = kSlotsR * int64_t(sizeof(T)) + kIdxSlots * int64_t(sizeof(I)) + int64_t(sizeof(V));
   L.cap = std::max(maxfp, 1);
-  int64_t rc = std::min<int64_t>(maxrows, (budget - fp_bytes - 4 * 16) / per_row);
-  rc = std::max<int64_t>(rc, 0);
+  int64_t rc = row_capacity(maxfp, maxrows, maxb).first;
   // PSR_RELAX_ROW_CAP caps the staged rows per task (test override: 0 sends every task down
   // the global-memory row path that only tasks too large for shared memory take).
   if (const char* env = std::getenv("PSR_RELAX_ROW_CAP")) {
@@ -768,14 +1342,23 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
   int64_t smem = fp_bytes + rc * (kSlotsR * int64_t(sizeof(T)) + kIdxSlots * int64_t(sizeof(I))) +
                  ((int64_t(L.b_cap) * int64_t(sizeof(V)) + 15) & ~int64_t(15));
   smem = std::max<int64_t>(smem, 16);
+  DBuf<StripMeta> meta(int64_t(n + 1) * strips, s);
+  {
+    auto mk = rev ? strip_meta_kernel<true> : strip_meta_kernel<false>;
+    mk<<<blocks_for(int64_t(n + 1) * strips, 128), 128, 0, s>>>(xstart.p, bounds.p, off, n, strips, per16, L.cap,
+                                                                 L.row_cap, L.b_cap, int(row_bytes), int(sizeof(V)),
+                                                                 meta.p);
+    PSR_LAUNCH_CHECK();
+  }
+  L.meta = meta.p;
   auto kernel = rev ? strip_gs_kernel<T, V, I, true> : strip_gs_kernel<T, V, I, false>;
   PSR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   const int64_t total_tasks = int64_t(visits.size()) * strips;
-  const int grid = int(std::min<int64_t>(total_tasks, sms));
+  const int grid = int(std::min<int64_t>(total_tasks, ctas));
   const char* trace_file = std::getenv("PSR_RELAX_TRACE_FILE");
   DBuf<long long> trace;
   if (trace_file) {
-    trace.alloc(total_tasks * 8, s);
+    trace.alloc(total_tasks * kTraceSlots, s);
     trace.zero();
     L.trace = trace.p;
   }
@@ -797,9 +1380,9 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
     cudaEventDestroy(e1);
   }
   if (trace_file) {
-    std::vector<long long> h = read_vector(trace.p, total_tasks * 8, s);
+    std::vector<long long> h = read_vector(trace.p, total_tasks * kTraceSlots, s);
     if (FILE* f = std::fopen(trace_file, "ab")) {
-      long long header[6] = {depth, n, strips, L.row_cap, grid, total_tasks};
+      long long header[8] = {depth, n, strips, L.row_cap, grid, total_tasks, caps[3], kTraceSlots};
       std::fwrite(header, sizeof(header), 1, f);
       std::fwrite(visits.data(), sizeof(int2), visits.size(), f);
       std::fwrite(h.data(), sizeof(long long), h.size(), f);

@@ -633,9 +633,7 @@ __global__ void __launch_bounds__(128, 12) assemble_sliced_kernel(const int64_t*
   int4* vd = reinterpret_cast<int4*>(svals + p * 28);
   const int4* vs = reinterpret_cast<const int4*>(v);
   for (int q = 0; q < 28 * int(sizeof(S)) / 16; ++q) vd[q] = vs[q];
-  int4* id = reinterpret_cast<int4*>(sidx + p * 32);
-  const int4* is = reinterpret_cast<const int4*>(idx);
-  for (int q = 0; q < 32 * int(sizeof(I)) / 16; ++q) id[q] = is[q];
+  store_idx_row(sidx + p * 32, p, idx);
   sb[p] = T(load[i]) + T(0.5) * T(pl);
 }
 

@@ -68,7 +68,7 @@ __global__ void transpose_values_kernel(int64_t n, const int64_t* skeys, const i
   const I* row = sidx + p * kIdxSlots;
   __align__(16) S v[kSlots];
   for (int k = 0; k < 27; ++k) {
-    const I idx = row[k];
+    const I idx = row[idx_slot<I>(p, k)];
     S a = S(0);
     if (idx >= 0) {
       int q[3] = {c[0] + k / 9 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k % 3 - 1};
@@ -143,12 +143,7 @@ __global__ void level_reverse_kernel(LevelReverse<T, S, I> L) {
     const int own = (c[0] & 1) + 2 * (c[1] & 1);
     // the row's index record (vector loads) and its increments of every visit, loaded once
     __align__(16) I row[kIdxSlots];
-    {
-      const int4* src = reinterpret_cast<const int4*>(L.sidx + p * kIdxSlots);
-      int4* dst = reinterpret_cast<int4*>(row);
-#pragma unroll
-      for (int q = 0; q < kIdxSlots * int(sizeof(I)) / 16; ++q) dst[q] = __ldg(src + q);
-    }
+    load_idx_row_ldg(L.sidx + p * kIdxSlots, p, row);
     const int iters = ITERS > 0 ? ITERS : L.iters;
     const T* mrow = L.mu + p * iters;
     // fixed visit count (the common 8): records in registers, vector loads
@@ -318,12 +313,7 @@ __global__ void __launch_bounds__(128) level_rows_reverse_kernel(const int64_t* 
   const int64_t i = perm[p];
   const int own = (c[0] & 1) + 2 * (c[1] & 1);
   __align__(16) I row[kIdxSlots];
-  {
-    const int4* src = reinterpret_cast<const int4*>(sidx + p * kIdxSlots);
-    int4* dst = reinterpret_cast<int4*>(row);
-#pragma unroll
-    for (int q = 0; q < kIdxSlots * int(sizeof(I)) / 16; ++q) dst[q] = __ldg(src + q);
-  }
+  load_idx_row_ldg(sidx + p * kIdxSlots, p, row);
   // visit records as 16-byte vector loads (a row's ITERS values are contiguous and aligned)
   static_assert(ITERS * sizeof(T) % 16 == 0, "visit records in 16-byte vectors");
   __align__(16) T mu[ITERS];  // reverse visit u

@@ -352,12 +352,12 @@ class _ReconstructFunction(torch.autograd.Function):
         def ptr(t):
             return 0 if t is None else t.to(dtype).contiguous().data_ptr()
 
-        keep = [t.to(dtype).contiguous() if t is not None else None for t in (g_coef, g_cum, g_norm)]
+        keep = [t.to(dtype).contiguous() if t is not None else None for t in (g_coef, g_cum, g_norm, g_iso)]
         dtype_code = _lib.PSR_FLOAT64 if p.dtype == torch.float64 else _lib.PSR_FLOAT32
         with torch.cuda.device(p.device):
             _lib.check(_lib.load().psr_backward(
                 result.field._handle.ptr, p.data_ptr(), n.data_ptr(), p.shape[0], dtype_code,
-                ptr(keep[0]), ptr(keep[1]), float(g_iso) if g_iso is not None else 0.0, ptr(keep[2]),
+                ptr(keep[0]), ptr(keep[1]), ptr(keep[3]), ptr(keep[2]),
                 g_p.data_ptr(), g_n.data_ptr(), _stream(p.device)))
         ctx.box.reverse_pass_done(result)
         return (g_p if ctx.needs_input_grad[0] else None), (g_n if ctx.needs_input_grad[1] else None), None, None
