@@ -245,6 +245,7 @@ def run_ours(args, rank, world):
     bw_stage_ms = {k: round(statistics.mean(b[k] for b in bw_stages), 3) for k in bw_stages[0]} if bw_stages else {}
     fwd_ms = statistics.mean(x[0] for x in split)
     bwd_ms = statistics.mean(x[1] for x in split)
+    split_steps = list(split)  # (forward, backward) ms of each timed step
     # the finest level's relaxation launch over the timed steps (the roofline's kernel)
     finest_s = statistics.mean(f[0] for f in finest)
     visits = finest[-1][1]
@@ -358,7 +359,8 @@ def run_ours(args, rank, world):
                 "d2h_bytes_per_step": int(p_pin.numel() * 4 * 2)},
         "split_ms": {"forward_differentiable": round(fwd_ms, 3), "backward": round(bwd_ms, 3),
                      "adjoint_over_forward": round(bwd_ms / fwd_ms, 3), "forward_plain": round(plain_ms, 3),
-                     "backward_stages": bw_stage_ms},
+                     "backward_stages": bw_stage_ms,
+                     "per_step": [[round(a, 2), round(b, 2)] for a, b in split_steps]},
         "fp64_step": fp64_step,
         "coefficient_sweeps_per_s": {"step": round(all_visits / (ms / 1e3), 1),
                                      "relaxation_kernels": round(all_visits / all_s, 1) if all_s > 0 else None,

@@ -7,7 +7,9 @@ the default path:
 * PSR_RELAX_FOOTPRINT_LIMIT -- a strip whose footprint exceeds the 16-bit index range makes
   the launch narrow its strips (doubling their count) until every footprint fits.  On the
   torus fixture's depth-6 level the default 4 strips have a 912-entry footprint, 8 strips
-  740, 16 strips 596 and 32 strips 504, so a limit of 600 narrows the strips 4 -> 16 (or 32).
+  740, 16 strips 596 and 32 strips 504, so a limit of 600 narrows the strips 4 -> 16 (or 32);
+* PSR_RELAX_KERNEL=pipeline -- the cluster pipelines (one 8-CTA cluster per visit), which the
+  library leaves off by default (slower than the dynamic scheduler on the benchmark level).
 """
 import numpy as np
 import pytest
@@ -20,11 +22,13 @@ from test_gpu_relaxation import gpu_relax
 
 pytestmark = pytest.mark.gpu
 
-OVERRIDES = [("PSR_RELAX_ROW_CAP", "0"), ("PSR_RELAX_FOOTPRINT_LIMIT", "600"), ("PSR_RELAX_FOOTPRINT_LIMIT", "1")]
+OVERRIDES = [("PSR_RELAX_ROW_CAP", "0"), ("PSR_RELAX_FOOTPRINT_LIMIT", "600"), ("PSR_RELAX_KERNEL", "pipeline"),
+             ("PSR_RELAX_FOOTPRINT_LIMIT", "1")]
+FORCED = OVERRIDES[:3]
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
-@pytest.mark.parametrize("name,value", OVERRIDES[:2])
+@pytest.mark.parametrize("name,value", FORCED)
 @pytest.mark.parametrize("pattern,size,depth,iters", [("full", 9, 3, 3), ("random", 33, 5, 8)])
 def test_forced_relaxation_paths_match_oracle(monkeypatch, dtype, name, value, pattern, size, depth, iters):
     monkeypatch.setenv(name, value)
@@ -36,14 +40,14 @@ def test_forced_relaxation_paths_match_oracle(monkeypatch, dtype, name, value, p
 def test_footprint_beyond_every_strip_count_is_an_error(monkeypatch):
     """A footprint that no strip count brings under the limit raises (never a wrong answer)."""
     from warp_psr_b200 import _lib
-    monkeypatch.setenv("PSR_RELAX_FOOTPRINT_LIMIT", "1")
+    monkeypatch.setenv(*OVERRIDES[3])
     keys, offsets, columns, values, b, x = local_system("full", dtype=np.float64)
     with pytest.raises(_lib.PSRError, match="16-bit index range"):
         gpu_relax(keys, offsets, columns, values, b, x, 3, 2)
 
 
 @pytest.mark.parametrize("precision", ["double", "float", "mixed"])
-@pytest.mark.parametrize("name,value", OVERRIDES[:2])
+@pytest.mark.parametrize("name,value", FORCED)
 def test_forced_paths_reconstruct_identically(monkeypatch, precision, name, value):
     from warp_psr_b200 import reconstruct
     kat = BY_NAME["torus"]

@@ -112,16 +112,27 @@ __global__ void isovalue_blocks_kernel(const T* values, const T* weights, int64_
   tv[l] = v;
   tw[l] = w;
   __syncthreads();
-  for (int stride = 128; stride >= 1; stride >>= 1) {
+  // pairwise tree, stride 128 .. 1: element l takes l + stride.  Strides 128..32 in shared
+  // memory, 16..1 inside warp 0 with shuffles (the same additions in the same order).
+  for (int stride = 128; stride >= 32; stride >>= 1) {
     if (l < stride) {
       tv[l] = tv[l] + tv[l + stride];
       tw[l] = tw[l] + tw[l + stride];
     }
     __syncthreads();
   }
-  if (l == 0) {
-    partial[2 * blockIdx.x] = tv[0];
-    partial[2 * blockIdx.x + 1] = tw[0];
+  if (l < 32) {
+    v = tv[l];
+    w = tw[l];
+#pragma unroll
+    for (int stride = 16; stride >= 1; stride >>= 1) {
+      v = v + __shfl_down_sync(0xffffffffu, v, stride);
+      w = w + __shfl_down_sync(0xffffffffu, w, stride);
+    }
+    if (l == 0) {
+      partial[2 * blockIdx.x] = v;
+      partial[2 * blockIdx.x + 1] = w;
+    }
   }
 }
 

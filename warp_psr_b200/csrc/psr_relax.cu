@@ -67,7 +67,7 @@ constexpr int kMetaInts = 96;
 // One task description per (logical slice z, strip s), shared by the iters visits of that
 // strip; built once per launch by strip_meta_kernel.  Footprint range r = 4j + c is colour
 // c of logical slice z - 1 + j, x within 4 of the strip.
-struct StripMeta {
+struct __align__(16) StripMeta {
   int lo[12], hi[12];        // schedule positions [lo, hi) of each footprint range
   int base[13];              // footprint offset of each range; base[12] = footprint size
   int delta[12];             // footprint index of a group-relative neighbour index i: i + delta[r]
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(kRelaxThreads, kRelaxCtasPerSm) strip_gs_kerne
   __shared__ uint64_t s_bar;
   __shared__ int s_task[2], s_fail;
   __shared__ int2 s_zt[2];
-  __shared__ StripMeta s_meta[2];
+  __shared__ __align__(16) StripMeta s_meta[2];
   // Shared layout (each part 16-byte aligned): footprint V[cap + 1] | values T[row_cap*28] |
   // neighbour indices I[row_cap*32] | right-hand side V[b_cap].
   V* foot = reinterpret_cast<V*>(smem_raw);
@@ -302,9 +302,9 @@ __global__ void __launch_bounds__(kRelaxThreads, kRelaxCtasPerSm) strip_gs_kerne
     if (task < total_tasks) {
       const int2 zt = L.visits[task / L.strips];
       if (lane == 0) s_zt[b] = zt;
-      const int* src = reinterpret_cast<const int*>(L.meta + int64_t(zt.x) * L.strips + task % L.strips);
-      int* dst = reinterpret_cast<int*>(&s_meta[b]);
-      for (int i = lane; i < kMetaInts; i += 32) dst[i] = src[i];
+      static_assert(kMetaInts / 4 <= 32, "one 16-byte load per lane");
+      const int4* src = reinterpret_cast<const int4*>(L.meta + int64_t(zt.x) * L.strips + task % L.strips);
+      if (lane < kMetaInts / 4) reinterpret_cast<int4*>(&s_meta[b])[lane] = __ldg(src + lane);
     }
   };
   if (threadIdx.x == 0) mbar_init(&s_bar);
@@ -547,7 +547,8 @@ __global__ void strip_meta_kernel(const int32_t* xstart, const int32_t* bounds, 
 // So a step costs its four colour phases, one cluster barrier and the neighbour exchange in
 // shared memory; the global-memory hand-off between pipelines is paid once per visit (the
 // pipelines run staggered), not once per slice.  Operator rows are brought in per colour phase
-// by bulk copies into three rotating regions, issued three phases ahead.
+// by bulk copies into two alternating regions, issued two phases ahead; a phase with more rows
+// than a region holds (polar slices: the few largest tasks) reads its rows from global memory.
 //
 // Warps 0..11 update rows; warp 12 loads the next step's task description and issues the bulk
 // copies and the release of each step; warps 13..15 stage the next step's global ranges.  Every
@@ -555,17 +556,21 @@ __global__ void strip_meta_kernel(const int32_t* xstart, const int32_t* bounds, 
 // until the loop ends, so no barrier is left waiting, and drain their copies before exiting.
 constexpr int kPipeCtas = 8;
 constexpr int kPipeRowThreads = 384;
-constexpr int kPipeRegions = 3;
+constexpr int kPipeRegions = 2;
 constexpr int kMaxPeerSegs = 40;
 
 struct PeerSeg {
   int rank, src, dst, count;  // values [src, src+count) of CTA `rank`'s export -> footprint [dst, dst+count)
 };
 struct PipeMeta {
-  StripMeta m;
+  StripMeta m;   // footprint layout padded: every range starts where its first element's
+                 // offset from a 16-byte boundary matches the x buffers' (bulk copies)
   int ebase[5];  // export offset of each colour's own rows (colour-major); ebase[4] = own rows
-  int nseg, overflow, pad;
-  PeerSeg seg[kMaxPeerSegs];  // the slice z+1 footprint ranges, by owner
+  int nseg, overflow, npush;
+  PeerSeg seg[kMaxPeerSegs];      // the slice z+1 footprint ranges, by owner (pulled: rank = owner)
+  PeerSeg push[kMaxPeerSegs];     // this task's exports pushed into the next step's footprints
+                                  // (rank = receiving CTA, dst = its footprint offset)
+  int pushoff[kMaxPeerSegs + 4];  // values before each push segment; pushoff[npush] = all of them
 };
 constexpr int kPipeMetaInts = int(sizeof(PipeMeta) / 4);
 static_assert(sizeof(PipeMeta) % 16 == 0, "PipeMeta is copied as ints into 16-byte aligned shared memory");
@@ -583,16 +588,35 @@ struct PipeLevel {
 __device__ __forceinline__ void bar_named(int id, int count) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
+// Cluster barrier in two halves (each warp, converged): arrive releases this thread's writes
+// (shared memory of any CTA of the cluster, global memory); wait acquires the others'.
+__device__ __forceinline__ void cluster_arrive() {
+  __syncwarp();
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+  __syncwarp();
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
 template <int C, bool M, class T, class V, class I>
 __device__ __forceinline__ void pipe_phase(const StripLevel& L, const StripMeta& m, const int* ebase, const I* r_idx,
-                                           const T* r_vals, const V* r_b, V* foot, V* hist, V* out, V* expo) {
+                                           const T* r_vals, const V* r_b, V* foot, V* hist, V* out, V* expo,
+                                           int rcap, int bcap) {
   constexpr int per16 = 16 / int(sizeof(V));
   const bool inc = L.record_increment != 0;
-  const int p0 = m.p0[C], p1 = m.p1[C], o0 = m.o0[C], o1 = m.o1[C], bshift = p0 % per16;
+  const int p0 = m.p0[C], p1 = m.p1[C], o0 = m.o0[C], o1 = m.o1[C];
+  int bshift = p0 % per16;
+  const int a1 = (p1 + per16 - 1) / per16 * per16;
+  if (p1 - p0 > rcap || a1 - (p0 - bshift) > bcap) {  // not staged: the rows in global memory
+    r_idx = reinterpret_cast<const I*>(L.nidx) + int64_t(p0) * kIdxSlots;
+    r_vals = reinterpret_cast<const T*>(L.vals) + int64_t(p0) * kSlotsR;
+    r_b = reinterpret_cast<const V*>(L.b) + p0;
+    bshift = 0;
+  }
   const unsigned total = unsigned(m.base[12]);
   int dreg[12];
 #pragma unroll
@@ -613,6 +637,7 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) pipeline_gs_kernel(PipeLevel
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t s_full[kPipeRegions];   // rows of the region's phase have landed
   __shared__ uint64_t s_empty[kPipeRegions];  // the region's phase is done with them
+  __shared__ uint64_t s_gfull[2];             // foot[b]'s slices from the previous visit have landed
   __shared__ int s_err;
   const StripLevel& L = P.L;
   const int t = int(blockIdx.x) / kPipeCtas;
@@ -634,21 +659,33 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) pipeline_gs_kernel(PipeLevel
       mbar_init(&s_full[r]);
       mbar_init(&s_empty[r]);
     }
+    mbar_init(&s_gfull[0]);
+    mbar_init(&s_gfull[1]);
     s_err = 0;
   }
   auto fail = [&](int code) {
     atomicCAS(L.error, 0, code);
     s_err = 1;
   };
-  // warp 12: the task description of a step into sm[step & 1]
+  // warp 12: the task description of a step into sm[step & 1] -- every 16-byte load issued
+  // before the first store (a load/store loop serialises on the loads' latency)
   auto load_meta = [&](int step) {
+    constexpr int kVecs = int(sizeof(PipeMeta) / 16), kPer = (kVecs + 31) / 32;
     const int z = L.n - step;
-    const int* src = reinterpret_cast<const int*>(P.meta + (int64_t(z) * kPipeCtas + s));
-    int* dst = reinterpret_cast<int*>(sm[step & 1]);
-    for (int i = lane; i < kPipeMetaInts; i += 32) dst[i] = src[i];
+    const int4* src = reinterpret_cast<const int4*>(P.meta + (int64_t(z) * kPipeCtas + s));
+    int4* dst = reinterpret_cast<int4*>(sm[step & 1]);
+    int4 v[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u)
+      if (lane + 32 * u < kVecs) v[u] = __ldg(src + lane + 32 * u);
+#pragma unroll
+    for (int u = 0; u < kPer; ++u)
+      if (lane + 32 * u < kVecs) dst[lane + 32 * u] = v[u];
   };
-  int last_issued[kPipeRegions] = {-1, -1, -1};  // thread 384: the last phase issued into each region
-  // thread 384: bulk copies of phase k's rows into region k % 3 (empty phases only arrive)
+  int last_issued[kPipeRegions];  // thread 384: the last phase issued into each region
+  for (int r = 0; r < kPipeRegions; ++r) last_issued[r] = -1;
+  // thread 384: bulk copies of phase k's rows into region k % kPipeRegions (phases with no rows,
+  // or more than a region holds, only arrive)
   auto issue = [&](int k) {
     last_issued[k % kPipeRegions] = k;
     constexpr int per16 = 16 / int(sizeof(V));
@@ -656,8 +693,7 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) pipeline_gs_kernel(PipeLevel
     const StripMeta& m = sm[step & 1]->m;
     const int p0 = m.p0[col], cnt = m.p1[col] - p0;
     const int a0 = p0 - p0 % per16, a1 = (m.p1[col] + per16 - 1) / per16 * per16;
-    const bool ok = cnt > 0 && cnt <= P.rcap && a1 - a0 <= P.bcap;
-    if (cnt > 0 && !ok) fail(2);
+    const bool ok = cnt > 0 && cnt <= P.rcap && a1 - a0 <= P.bcap;  // else the phase reads global rows
     const uint32_t bytes =
         ok ? uint32_t(cnt) * (kSlotsR * sizeof(T) + kIdxSlots * sizeof(I)) + uint32_t(a1 - a0) * sizeof(V) : 0;
     fence_proxy_async();
@@ -670,59 +706,67 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) pipeline_gs_kernel(PipeLevel
       bulk_copy(smem_raw + P.off_b[r], gb + a0, uint32_t(a1 - a0) * sizeof(V), &s_full[r]);
     }
   };
-  // warps 13..15: footprint ranges of slices z and z-1 after visit t-1 for a step, into
-  // foot[step & 1], once pipeline t-1 has published them
+  // warp 13: footprint ranges of slices z and z-1 after visit t-1 for a step, into
+  // foot[step & 1] by bulk copies (completion on s_gfull[step & 1]), once pipeline t-1 has
+  // published them.  The flag reads are generic-proxy acquires; the proxy fence orders the
+  // copies' async-proxy reads of the released values after them.
+  int gissued[2] = {-1, -1};  // warp 13 lane 0: the last step whose copies went into each buffer
   auto stage_global = [&](int step) {
     const StripMeta& m = sm[step & 1]->m;
     const int z = L.n - step;
-    const int ht = threadIdx.x - 13 * 32;  // 0..95
-    if (warp == 13) {
-      bool ok = !s_err;
-      if (ok) ok = wait_strips(L, z, m.dep_lo[1], m.dep_hi[1], t, lane);
-      if (ok && z > 0) ok = wait_strips(L, z - 1, m.dep_lo[0], m.dep_hi[0], t, lane);
-      if (!ok && lane == 0 && !s_err) fail(1);
-    }
-    bar_named(3, 96);
-    if (s_err) return;
-    V* f = foot[step & 1];
-    for (int r = 0; r < 8; ++r) {
-      const V* src = xprev + m.lo[r];
-      V* dst = f + m.base[r];
-      const int cnt = m.hi[r] - m.lo[r];
-      for (int i0 = ht; i0 < cnt; i0 += 4 * 96) {
-        V v[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (i0 + 96 * u < cnt) v[u] = __ldcg(src + i0 + 96 * u);
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (i0 + 96 * u < cnt) dst[i0 + 96 * u] = v[u];
+    bool ok = !s_err;
+    if (ok) ok = wait_strips(L, z, m.dep_lo[1], m.dep_hi[1], t, lane);
+    if (ok && z > 0) ok = wait_strips(L, z - 1, m.dep_lo[0], m.dep_hi[0], t, lane);
+    if (!ok && lane == 0 && !s_err) fail(1);
+    if (lane == 0) {
+      constexpr int per16 = 16 / int(sizeof(V));
+      uint32_t bytes = 0;
+      if (ok)
+        for (int r = 0; r < 8; ++r)
+          if (m.hi[r] > m.lo[r])
+            bytes += uint32_t((m.hi[r] + per16 - 1) / per16 * per16 - (m.lo[r] - m.lo[r] % per16)) * sizeof(V);
+      asm volatile("fence.proxy.async.global;" ::: "memory");
+      fence_proxy_async();
+      gissued[step & 1] = step;
+      mbar_expect_tx(&s_gfull[step & 1], bytes);
+      if (ok) {
+        V* f = foot[step & 1];
+        for (int r = 0; r < 8; ++r) {
+          if (m.hi[r] <= m.lo[r]) continue;
+          const int lo = m.lo[r] - m.lo[r] % per16, hi = (m.hi[r] + per16 - 1) / per16 * per16;
+          bulk_copy(f + (m.base[r] - m.lo[r] % per16), xprev + lo, uint32_t(hi - lo) * sizeof(V), &s_gfull[step & 1]);
+        }
       }
     }
+    __syncwarp();
   };
   __syncthreads();
-  // prologue: step 0's description, its first three phases' rows, its global ranges
+  // prologue: step 0's description, its first phases' rows, its global ranges
   if (warp == 12) load_meta(0);
   __syncthreads();
   if (threadIdx.x == 12 * 32)
     for (int k = 0; k < kPipeRegions && k < nphases; ++k) issue(k);
-  if (warp >= 13) stage_global(0);
+  if (warp == 13) stage_global(0);
   __syncthreads();
   cluster.sync();  // every CTA of the cluster has initialised its shared memory
   for (int step = 0; step < nsteps; ++step) {
     const int z = L.n - step, fb = step & 1;
     const PipeMeta& pm = *sm[fb];
     const StripMeta& m = pm.m;
-    // slice z+1 after visit t: the peers' exports of the previous step
-    if (warp < 12 && step > 0 && !s_err) {
-      for (int g = 0; g < pm.nseg; ++g) {
-        const PeerSeg sg = pm.seg[g];
-        const V* remote = cluster.map_shared_rank(expo[(step - 1) & 1], sg.rank);
-        for (int i = threadIdx.x; i < sg.count; i += kPipeRowThreads) foot[fb][sg.dst + i] = remote[sg.src + i];
-      }
-    }
+    // trace (optional): per (visit, strip, step) 16 values: [0] step start (globaltimer ns);
+    // [1..6] SM cycles from then to the phases' start, the end of phase 0..3 and the cluster
+    // barrier's end; [7] the global ranges of the next step staged (globaltimer ns); [8..11]
+    // SM cycles to each phase's rows being in place; [12..15] (copy thread) SM cycles to the
+    // copies of phase k + 2 being issued
+    long long* tr = L.trace ? L.trace + ((int64_t(t) * kPipeCtas + s) * nsteps + step) * 16 : nullptr;
+    const long long c0 = (tr && (threadIdx.x == 0 || threadIdx.x == 12 * 32)) ? clock64() : 0;
+    if (tr && threadIdx.x == 0) tr[0] = globaltimer();
+    // slices z and z-1 after visit t-1 (copied in during the previous step); slice z+1 after
+    // visit t was pushed into foot[fb] by the peers before the cluster barrier
+    if (warp < 12 && !s_err && !mbar_wait(&s_gfull[fb], uint32_t(step >> 1) & 1)) fail(4);
     if (threadIdx.x == 0) foot[fb][m.base[12]] = V(0);
     __syncthreads();
+    if (tr && threadIdx.x == 0) tr[1] = clock64() - c0;
     if (warp < 12) {
 #define PSR_PIPE_PHASE(CI)                                                                                         \
   {                                                                                                                \
@@ -730,60 +774,96 @@ __global__ void __launch_bounds__(kRelaxThreads, 1) pipeline_gs_kernel(PipeLevel
     constexpr int col = REV ? 3 - CI : CI;                                                                         \
     const int r = k % kPipeRegions;                                                                                \
     if (!s_err && !mbar_wait(&s_full[r], uint32_t(k / kPipeRegions) & 1)) fail(4);                              \
+    if (tr && threadIdx.x == 0) tr[8 + CI] = clock64() - c0;                                                       \
     if (!s_err)                                                                                                    \
       pipe_phase<col, REV, T, V, I>(L, m, pm.ebase, reinterpret_cast<const I*>(smem_raw + P.off_idx[r]),          \
                                     reinterpret_cast<const T*>(smem_raw + P.off_vals[r]),                          \
                                     reinterpret_cast<const V*>(smem_raw + P.off_b[r]), foot[fb], hv, xout,         \
-                                    expo[fb]);                                                                     \
+                                    expo[fb], P.rcap, P.bcap);                                                     \
     bar_named(1, kPipeRowThreads);                                                                                 \
     if (threadIdx.x == 0) mbar_arrive(&s_empty[r]);                                                                \
+    if (tr && threadIdx.x == 0) tr[2 + CI] = clock64() - c0;                                                       \
   }
       PSR_PIPE_PHASE(0) PSR_PIPE_PHASE(1) PSR_PIPE_PHASE(2) PSR_PIPE_PHASE(3)
 #undef PSR_PIPE_PHASE
+      // push this step's new values of slice z into the peers' next footprints (remote
+      // stores; the cluster barrier makes them visible)
+      if (step + 1 < nsteps && !s_err) {
+        const int total = pm.pushoff[min(pm.npush, kMaxPeerSegs)];
+        int g = 0;
+        for (int e = threadIdx.x; e < total; e += kPipeRowThreads) {
+          while (pm.pushoff[g + 1] <= e) ++g;
+          const PeerSeg& sg = pm.push[g];
+          V* remote = cluster.map_shared_rank(foot[(step + 1) & 1], sg.rank);
+          remote[sg.dst + (e - pm.pushoff[g])] = expo[fb][sg.src + (e - pm.pushoff[g])];
+        }
+      }
+      cluster_arrive();
     } else if (warp == 12) {
       if (step + 1 < nsteps) load_meta(step + 1);
       __syncwarp();
       bar_named(2, 128);  // the next step's description is in place for warps 13..15
       if (lane == 0) {
         for (int ci = 0; ci < 4; ++ci) {
-          // region k % 3 is free once phase k is done; then the copies of phase k + 3 go in.
-          // (One full and one empty barrier per region: neither can run a phase ahead of the
-          // other, so a parity wait never confuses two phases.)
+          // the region of phase k is free once phase k is done; then the copies of phase
+          // k + kPipeRegions go in.  (One full and one empty barrier per region: neither can run
+          // a phase ahead of the other, so a parity wait never confuses two phases.)
           const int k = 4 * step + ci;
           if (!mbar_wait(&s_empty[k % kPipeRegions], uint32_t(k / kPipeRegions) & 1) && !s_err) fail(4);
           if (k + kPipeRegions < nphases && !s_err) issue(k + kPipeRegions);
+          if (tr) tr[12 + ci] = clock64() - c0;  // copies of phase k + 2 issued (cycles from this thread's step start)
         }
-        if (!s_err) {  // release slice z after visit t to pipeline t+1
-          __threadfence();
-          atomicMax(L.done + (int64_t(z) * L.strips + s) * kFlagPad, t + 1);
-        }
+      }
+      __syncwarp();
+      cluster_arrive();  // this warp's part of the step is done; the release below overlaps the barrier
+      if (lane == 0 && !s_err) {  // release slice z after visit t to pipeline t+1
+        __threadfence();
+        atomicMax(L.done + (int64_t(z) * L.strips + s) * kFlagPad, t + 1);
       }
       __syncwarp();
     } else {
       bar_named(2, 128);
-      if (step + 1 < nsteps) stage_global(step + 1);
+      cluster_arrive();  // the next step's staging (bulk copies) overlaps the barrier
+      if (warp == 13 && step + 1 < nsteps) stage_global(step + 1);
+      if (tr && threadIdx.x == 13 * 32) tr[7] = globaltimer();
     }
-    cluster.sync();
+    cluster_wait();
+    if (tr && threadIdx.x == 0) tr[6] = clock64() - c0;
   }
   // never leave with copies in flight (after an error some were not consumed)
   if (threadIdx.x == 12 * 32)
     for (int r = 0; r < kPipeRegions; ++r)
       if (last_issued[r] >= 0) mbar_wait(&s_full[r], uint32_t(last_issued[r] / kPipeRegions) & 1);
+  if (threadIdx.x == 13 * 32)
+    for (int b = 0; b < 2; ++b)
+      if (gissued[b] >= 0) mbar_wait(&s_gfull[b], uint32_t(gissued[b] >> 1) & 1);
   __syncthreads();
 }
 
-// Peer segments and export offsets of the cluster pipelines, one thread per (logical slice z,
-// strip s); meta holds the StripMeta of the same tasks.
+// Padded footprint layout, peer segments and export offsets of the cluster pipelines, one
+// thread per (logical slice z, strip s); strip_meta holds the StripMeta of the same tasks.
 template <bool REV>
-__global__ void pipe_meta_kernel(const StripMeta* strip_meta, const int32_t* xstart, const int32_t* bounds, int n,
-                                 PipeMeta* meta, int* caps) {
+__global__ void pipe_meta_kernel(const StripMeta* strip_meta, const int32_t* xstart, const int32_t* bounds,
+                                 const int32_t* group_off, int n, int per16, PipeMeta* meta, int* caps) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (n + 1) * kPipeCtas) return;
   const int z = idx / kPipeCtas, nx = n + 2;
   auto phys = [&](int zz) { return REV ? n - zz : zz; };
   PipeMeta pm;
   pm.m = strip_meta[idx];
-  const StripMeta& m = pm.m;
+  StripMeta& m = pm.m;
+  // range r starts at base[r] with base[r] = lo[r] (mod per16), after the previous range's
+  // 16-byte-rounded end, so that a bulk copy of [lo rounded down, hi rounded up) lands in place
+  int tot = 0;
+  for (int r = 0; r < 12; ++r) {
+    const int j = r >> 2, c = r & 3, zz = z + j - 1;
+    const int gstart = (zz >= 0 && zz <= n) ? group_off[phys(zz) * 4 + c] : 0;
+    const int start = (tot + per16 - 1) / per16 * per16;
+    m.base[r] = start + m.lo[r] % per16;
+    m.delta[r] = m.base[r] + gstart - m.lo[r];
+    tot = m.base[r] + (m.hi[r] - m.lo[r]) + ((m.hi[r] + per16 - 1) / per16 * per16 - m.hi[r]);
+  }
+  m.base[12] = tot;
   int e = 0;
   for (int c = 0; c < 4; ++c) {
     pm.ebase[c] = e;
@@ -792,12 +872,12 @@ __global__ void pipe_meta_kernel(const StripMeta* strip_meta, const int32_t* xst
   pm.ebase[4] = e;
   pm.nseg = 0;
   pm.overflow = 0;
-  pm.pad = 0;
+  pm.npush = 0;
   const int zz = z + 1;
   if (zz <= n) {
     const int32_t* bb = bounds + int64_t(phys(zz)) * (kPipeCtas + 1);
     for (int sp = m.dep_lo[2]; sp <= m.dep_hi[2]; ++sp) {
-      int ob[5], o0s[4], o1s[4], acc = 0;
+      int ob[4], o0s[4], o1s[4], acc = 0;
       for (int c = 0; c < 4; ++c) {
         const int32_t* xs = xstart + int64_t(phys(zz) * 4 + c) * nx;
         o0s[c] = xs[bb[sp]];
@@ -819,13 +899,45 @@ __global__ void pipe_meta_kernel(const StripMeta* strip_meta, const int32_t* xst
     }
   }
   for (int g = pm.nseg; g < kMaxPeerSegs; ++g) pm.seg[g] = PeerSeg{0, 0, 0, 0};
+  for (int g = 0; g < kMaxPeerSegs; ++g) pm.push[g] = PeerSeg{0, 0, 0, 0};
+  for (int g = 0; g < kMaxPeerSegs + 4; ++g) pm.pushoff[g] = 0;
   meta[idx] = pm;
   // capacities: footprint, rows per colour, exported values, overflow (right-hand-side spans:
   // pipe_bspan_kernel)
-  atomicMax(caps + 0, m.base[12]);
+  atomicMax(caps + 0, tot + per16);
   for (int c = 0; c < 4; ++c) atomicMax(caps + 1, m.p1[c] - m.p0[c]);
   atomicMax(caps + 3, e);
   if (pm.overflow) atomicMax(caps + 4, 1);
+}
+
+// Inverts the pull segments: the segment of consumer (z, s') reading owner rank s of slice
+// z+1 becomes a push segment of task (z+1, s), with the consumer's rank and footprint offset.
+__global__ void pipe_push_kernel(PipeMeta* meta, int n, int* caps) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * kPipeCtas) return;  // consumers z = 0 .. n-1
+  const int z = idx / kPipeCtas, sc = idx % kPipeCtas;
+  const PipeMeta& cm = meta[idx];
+  for (int g = 0; g < cm.nseg; ++g) {
+    const PeerSeg sg = cm.seg[g];
+    PipeMeta& pr = meta[(z + 1) * kPipeCtas + sg.rank];
+    const int slot = atomicAdd(&pr.npush, 1);
+    if (slot < kMaxPeerSegs)
+      pr.push[slot] = PeerSeg{sc, sg.src, sg.dst, sg.count};
+    else
+      atomicMax(caps + 4, 1);
+  }
+}
+
+__global__ void pipe_pushoff_kernel(PipeMeta* meta, int count) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= count) return;
+  PipeMeta& pm = meta[idx];
+  const int np = min(pm.npush, kMaxPeerSegs);
+  int acc = 0;
+  for (int g = 0; g < kMaxPeerSegs + 4; ++g) {
+    pm.pushoff[g] = acc;
+    if (g < np) acc += pm.push[g].count;
+  }
 }
 
 __global__ void pipe_bspan_kernel(const PipeMeta* meta, int count, int per16, int* caps) {
@@ -1091,7 +1203,11 @@ static bool relax_pipeline(const StripSchedule& S, const T* svals, const I* sidx
   DBuf<PipeMeta> meta(ntasks, s);
   caps.zero();
   auto pk = rev ? pipe_meta_kernel<true> : pipe_meta_kernel<false>;
-  pk<<<blocks_for(ntasks, 64), 64, 0, s>>>(smeta.p, xstart, bounds.p, n, meta.p, caps.p);
+  pk<<<blocks_for(ntasks, 64), 64, 0, s>>>(smeta.p, xstart, bounds.p, S.off.p, n, per16, meta.p, caps.p);
+  PSR_LAUNCH_CHECK();
+  pipe_push_kernel<<<blocks_for(int64_t(n) * kPipeCtas, 64), 64, 0, s>>>(meta.p, n, caps.p);
+  PSR_LAUNCH_CHECK();
+  pipe_pushoff_kernel<<<blocks_for(ntasks, 64), 64, 0, s>>>(meta.p, ntasks);
   PSR_LAUNCH_CHECK();
   pipe_bspan_kernel<<<blocks_for(ntasks), kThreads, 0, s>>>(meta.p, ntasks, per16, caps.p);
   PSR_LAUNCH_CHECK();
@@ -1099,10 +1215,19 @@ static bool relax_pipeline(const StripSchedule& S, const T* svals, const I* sidx
   if (c[4]) return false;  // more peer segments than a task description holds
   PipeLevel P{};
   P.cap = std::max(c[0], 1);
-  P.rcap = std::max(c[1], 1);
-  P.bcap = std::max(c[2], per16);
   P.ecap = std::max(c[3], 1);
   auto al = [](int64_t b) { return (b + 127) & ~int64_t(127); };
+  const int64_t budget = int64_t(device_smem_optin()) - 2048;  // static shared memory of the kernel
+  {  // rows per region: all of them if they fit, else as many as fit beside the rest
+    const int64_t fixed = 2 * al(int64_t(P.cap + 1) * int64_t(sizeof(V))) + 2 * al(int64_t(P.ecap) * int64_t(sizeof(V))) +
+                          2 * al(int64_t(sizeof(PipeMeta))) + kPipeRegions * 3 * 128;
+    const int64_t per_row = kSlotsR * int64_t(sizeof(T)) + kIdxSlots * int64_t(sizeof(I)) + int64_t(sizeof(V));
+    const int64_t fit = (budget - fixed - kPipeRegions * 2 * per16 * int64_t(sizeof(V))) / (kPipeRegions * per_row);
+    P.rcap = int(std::min<int64_t>(std::max(c[1], 1), fit));
+    P.bcap = std::min(std::max(c[2], per16), (P.rcap + 2 * per16) / per16 * per16);
+    // below a quarter of the median task's rows the pipelines would read most rows from global memory
+    if (P.rcap < 64) return false;
+  }
   int64_t off = 0;
   for (int f = 0; f < 2; ++f) {
     P.off_foot[f] = off;
@@ -1124,7 +1249,21 @@ static bool relax_pipeline(const StripSchedule& S, const T* svals, const I* sidx
     P.off_meta[f] = off;
     off += al(int64_t(sizeof(PipeMeta)));
   }
-  const int64_t budget = int64_t(device_smem_optin()) - 2048;  // static shared memory of the kernel
+  if (std::getenv("PSR_RELAX_DEBUG")) {
+    std::vector<PipeMeta> hm = read_vector(meta.p, ntasks, s);
+    std::vector<int> rows, fps;
+    for (const PipeMeta& q : hm) {
+      for (int cc = 0; cc < 4; ++cc) rows.push_back(q.m.p1[cc] - q.m.p0[cc]);
+      fps.push_back(q.m.base[12]);
+    }
+    std::sort(rows.begin(), rows.end());
+    std::sort(fps.begin(), fps.end());
+    auto pct = [](const std::vector<int>& v, double f) { return v.empty() ? 0 : v[size_t(f * (v.size() - 1))]; };
+    std::fprintf(stderr, "pipeline depth %d: cap %d rcap %d bcap %d ecap %d smem %lld budget %lld; rows/colour p50 %d "
+                 "p90 %d p99 %d max %d; footprint p50 %d p90 %d p99 %d max %d\n", depth, P.cap, P.rcap, P.bcap, P.ecap,
+                 (long long)off, (long long)budget, pct(rows, .5), pct(rows, .9), pct(rows, .99), pct(rows, 1.0),
+                 pct(fps, .5), pct(fps, .9), pct(fps, .99), pct(fps, 1.0));
+  }
   if (off > budget) return false;
   auto kernel = rev ? pipeline_gs_kernel<T, V, I, true> : pipeline_gs_kernel<T, V, I, false>;
   PSR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(off)));
@@ -1167,6 +1306,14 @@ static bool relax_pipeline(const StripSchedule& S, const T* svals, const I* sidx
   L.poll_log2 = 26;
   L.cap = P.cap;
   P.meta = meta.p;
+  const char* trace_file = std::getenv("PSR_RELAX_TRACE_FILE");
+  DBuf<long long> trace;
+  const int64_t trace_count = int64_t(iters) * kPipeCtas * (n + 1) * 16;
+  if (trace_file) {
+    trace.alloc(trace_count, s);
+    trace.zero();
+    L.trace = trace.p;
+  }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (ms) {
     PSR_CUDA(cudaEventCreate(&e0));
@@ -1181,6 +1328,15 @@ static bool relax_pipeline(const StripSchedule& S, const T* svals, const I* sidx
     PSR_CUDA(cudaEventElapsedTime(ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+  }
+  if (trace_file) {
+    std::vector<long long> h = read_vector(trace.p, trace_count, s);
+    if (FILE* f = std::fopen(trace_file, "ab")) {
+      long long header[8] = {depth, n, kPipeCtas, iters, -1, trace_count, 0, 16};  // -1: pipeline trace
+      std::fwrite(header, sizeof(header), 1, f);
+      std::fwrite(h.data(), sizeof(long long), h.size(), f);
+      std::fclose(f);
+    }
   }
   if (err == 2) throw Error(4, "ordered relaxation: a task's rows exceed their region");
   if (err == 3) throw Error(1, "ordered relaxation: an operator column is not its slot's neighbour");
@@ -1200,7 +1356,7 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
   const int per16 = 16 / int(sizeof(V));
   const int32_t* perm = S.perm.p;
   const int32_t* off = S.off.p;
-  DBuf<V> x0(rows, s), x1(rows, s);
+  DBuf<V> x0(rows + 16, s), x1(rows + 16, s);  // slack: 16-byte copies may read past the last row
   gather_x_kernel<V><<<blocks_for(rows), kThreads, 0, s>>>(perm, rows, x, x1.p);
   PSR_LAUNCH_CHECK();
   const int64_t* skeys_p = S.skeys.p;
