@@ -313,8 +313,27 @@ def run_ours(args, rank, world):
     memory["result_bytes"] = held["plain"]
     memory["tape_bytes"] = held["differentiable"] - held["plain"]
 
+    # Per-kernel roofline: one more solve+adjoint step (after the timed ones) with the
+    # library's kernel clocks on -- CUDA events around each launch of its main kernels, each
+    # with the launch's algorithmic bytes (what it must read and write once).
+    os.environ["PSR_KERNEL_CLOCKS"] = "1"
+    try:
+        _lib.kernel_clocks()  # clears earlier totals
+        step()
+        torch.cuda.synchronize()
+        kernel_clocks = _lib.kernel_clocks()
+    finally:
+        os.environ.pop("PSR_KERNEL_CLOCKS", None)
+
     out_dtype = "f64" if result["dtype"] == torch.float64 else "f32"
     info = result
+    peak_k, _ = peaks()
+    kernel_rows = [{"kernel": c["kernel"], "launches": c["launches"], "ms": round(c["ms"], 3),
+                    "algorithmic_bytes": int(c["bytes"]), "units": int(c["units"]), "unit": c["unit"],
+                    "bytes_per_unit": round(c["bytes"] / c["units"], 1) if c["units"] else None,
+                    "achieved": round(c["bytes"] / (c["ms"] * 1e-3) / 1e9, 1) if c["ms"] > 0 else None,
+                    "frac": round(c["bytes"] / (c["ms"] * 1e-3) / 1e9 / peak_k, 4) if c["ms"] > 0 else None}
+                   for c in sorted(kernel_clocks, key=lambda c: -c["ms"])]
     # Roofline of the dominant kernel: the finest level's ordered-relaxation launch
     # (strip_gs_kernel).  Algorithmic bytes per row visit: 27 operator entries (float32 in the
     # mixed path, else the input precision), b read, x read, x write in the vector precision,
@@ -354,7 +373,11 @@ def run_ours(args, rank, world):
                      "note": "latency-bound: each of the 2^d + 2(iters-1) + 1 waves depends on the previous one",
                      "all_levels": {"launches": info["relax_launches"], "row_visits": all_visits,
                                     "ms": round(all_s * 1e3, 3),
-                                    "achieved": round(all_visits * per_visit / all_s / 1e9, 1) if all_s > 0 else None}},
+                                    "achieved": round(all_visits * per_visit / all_s / 1e9, 1) if all_s > 0 else None},
+                     "kernels": kernel_rows,
+                     "kernels_note": "one extra solve+adjoint step with CUDA events around each launch of the library's "
+                                     "main kernels; algorithmic bytes = what a launch must read and write once "
+                                     "(index structures excluded); frac of the measured HBM copy peak"},
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(p_pin.numel() * 4 * 2),
                 "d2h_bytes_per_step": int(p_pin.numel() * 4 * 2)},
         "split_ms": {"forward_differentiable": round(fwd_ms, 3), "backward": round(bwd_ms, 3),

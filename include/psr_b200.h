@@ -123,6 +123,23 @@ int psr_last_error(char* buffer, size_t length);
  * scans from CUB are not counted). */
 int psr_kernel_launches(int64_t* count);
 
+/* Device time of the library's main kernels for a per-kernel roofline (a diagnostic, no
+ * counterpart in the reference).  Launches issued while the environment variable
+ * PSR_KERNEL_CLOCKS=1 is set are bracketed by CUDA events; this call waits for them and
+ * reports, per kernel, the launches, summed device ms, summed algorithmic bytes (what the
+ * launch must read and write once) and summed units (rows, row visits, points), then clears
+ * the totals.  Up to `capacity` entries are written; *count receives how many kernels have
+ * totals. */
+typedef struct psr_kernel_clock {
+  const char* kernel;
+  const char* unit;
+  int64_t launches;
+  double ms;
+  double bytes;
+  double units;
+} psr_kernel_clock;
+int psr_kernel_clocks(psr_kernel_clock* out, int32_t capacity, int32_t* count);
+
 /* Ordered sliced Gauss-Seidel of one level on a caller-supplied CSR operator (device
  * pointers; rows = basis keys of `depth`).  Result bitwise identical to the reference's
  * sequential slice/colour order. */

@@ -1,8 +1,9 @@
 """Paths that only large inputs take, forced on small cases: the hashed column index (used
 for depths beyond the dense per-depth tables, above 12; PSR_COLUMN_INDEX=hash) and the base
 relaxation with x in global memory (base levels too large for shared memory;
-PSR_BASE_RELAX=global).  Reconstructions, field evaluation and the reverse pass agree with
-the default paths."""
+PSR_BASE_RELAX=global) or with x but not the operator rows in shared memory (base levels
+above ~790 rows; PSR_BASE_RELAX=shared).  Reconstructions, field evaluation and the reverse
+pass agree with the default paths."""
 import numpy as np
 import pytest
 import torch
@@ -48,15 +49,17 @@ def test_reverse_pass_with_hashed_columns_agrees(monkeypatch):
     torch.testing.assert_close(grads[1], grads[0], rtol=1e-10, atol=1e-13)
 
 
+@pytest.mark.parametrize("forced", ["global", "shared"])
 @pytest.mark.parametrize("case", ["spsr_base1_depth4", "psr_base0_constant_mode"])
-def test_base_relaxation_in_global_memory_is_identical(monkeypatch, case):
-    """PSR_BASE_RELAX=global: the base levels' colour relaxation with x in global memory (the
-    path of base levels too large for shared memory) gives the shared-memory path's result."""
+def test_base_relaxation_in_global_memory_is_identical(monkeypatch, case, forced):
+    """PSR_BASE_RELAX=global (x in global memory) and =shared (x in shared memory, operator
+    rows from global memory): the base levels' colour relaxation gives the default path's
+    result (x and the operator rows staged in shared memory) bit for bit."""
     from warp_psr_b200 import reconstruct
     p0, m0 = cloud()
     opts = {k: v for k, v in CASES[case].items()}
     runs = []
-    for mode in (None, "global"):
+    for mode in (None, forced):
         if mode:
             monkeypatch.setenv("PSR_BASE_RELAX", mode)
         r = reconstruct(torch.tensor(p0, device="cuda"), torch.tensor(m0, device="cuda"), **opts)
@@ -65,13 +68,14 @@ def test_base_relaxation_in_global_memory_is_identical(monkeypatch, case):
     assert runs[0][1] == runs[1][1]
 
 
-def test_reverse_base_relaxation_in_global_memory_agrees(monkeypatch):
+@pytest.mark.parametrize("forced", ["global", "shared"])
+def test_reverse_base_relaxation_in_global_memory_agrees(monkeypatch, forced):
     from warp_psr_b200 import reconstruct_differentiable
     p0, m0 = cloud()
     q = torch.tensor(QUERIES, device="cuda", dtype=torch.float64)
     seed = torch.tensor(SEED, device="cuda", dtype=torch.float64)
     grads = []
-    for mode in (None, "global"):
+    for mode in (None, forced):
         if mode:
             monkeypatch.setenv("PSR_BASE_RELAX", mode)
         P = torch.tensor(p0, device="cuda", requires_grad=True)

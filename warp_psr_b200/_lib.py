@@ -54,11 +54,19 @@ class FieldHandle(ctypes.Structure):
     ]
 
 
+class KernelClock(ctypes.Structure):
+    """Mirror of ``psr_kernel_clock``: one kernel's launches, device ms and algorithmic bytes."""
+    _fields_ = [
+        ("kernel", ctypes.c_char_p), ("unit", ctypes.c_char_p), ("launches", ctypes.c_int64),
+        ("ms", ctypes.c_double), ("bytes", ctypes.c_double), ("units", ctypes.c_double),
+    ]
+
+
 EXPORTS = ("psr_reconstruct", "psr_result_info", "psr_result_arrays", "psr_evaluate", "psr_device_field",
            "psr_free", "psr_last_error", "psr_relax_sliced", "psr_isovalue", "psr_result_stage",
            "psr_kernel_launches", "psr_isovalue_static", "psr_backward", "psr_evaluate_backward",
            "psr_mc_points", "psr_mc_mark", "psr_mc_cells", "psr_mc_triangulate", "psr_extract_mesh",
-           "psr_mesh_info", "psr_mesh_arrays", "psr_mesh_free")
+           "psr_mesh_info", "psr_mesh_arrays", "psr_mesh_free", "psr_kernel_clocks")
 
 _lib = None
 
@@ -103,6 +111,7 @@ def load():
                                 ctypes.POINTER(i64)]
     L.psr_mesh_arrays.argtypes = [vp] + [ctypes.POINTER(vp)] * 5
     L.psr_mesh_free.argtypes = [vp]
+    L.psr_kernel_clocks.argtypes = [ctypes.POINTER(KernelClock), i32, ctypes.POINTER(i32)]
     for name in EXPORTS:
         getattr(L, name).restype = i32
     _lib = L
@@ -119,6 +128,17 @@ def kernel_launches():
     count = ctypes.c_int64()
     check(load().psr_kernel_launches(ctypes.byref(count)))
     return count.value
+
+
+def kernel_clocks():
+    """Totals of the kernel clocks (launches made while PSR_KERNEL_CLOCKS=1) since the last
+    call: a list of dicts (kernel, unit, launches, ms, bytes, units); clears the totals."""
+    L = load()
+    count = ctypes.c_int32()
+    out = (KernelClock * 32)()
+    check(L.psr_kernel_clocks(out, 32, ctypes.byref(count)))
+    return [{"kernel": c.kernel.decode(), "unit": c.unit.decode(), "launches": int(c.launches), "ms": c.ms,
+             "bytes": c.bytes, "units": c.units} for c in out[:min(count.value, 32)]]
 
 
 def check(code):

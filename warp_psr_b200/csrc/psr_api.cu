@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 
 using namespace psr;
@@ -17,6 +18,38 @@ namespace psr {
 std::atomic<long long> g_kernel_launches{0};
 
 void set_last_error(const std::string& message) { g_error = message; }
+
+namespace clocks {
+struct ClockTotals {
+  long long launches = 0;
+  double ms = 0, bytes = 0, units = 0;
+};
+struct PendingClock {
+  int kind;
+  double bytes, units;
+  cudaEvent_t a, b;
+};
+std::mutex g_clock_mutex;
+std::vector<PendingClock> g_clock_pending;
+ClockTotals g_clock_totals[kClkKinds];
+const char* const kClockNames[kClkKinds] = {
+    "assemble_sliced_kernel",        "cross_apply_kernel",        "normal_stencil_dense_kernel",
+    "relax_colors_shared_kernel",    "strip_gs_kernel (forward)", "strip_gs_kernel (reverse)",
+    "normal_stencil_reverse_kernel", "level_rows_reverse_kernel", "screening_points_reverse_kernel"};
+const char* const kClockUnits[kClkKinds] = {"row", "row", "row", "row visit", "row visit",
+                                            "row visit", "normal record", "row", "point"};
+}  // namespace clocks
+using namespace clocks;
+
+bool kernel_clocks_on() {
+  const char* v = std::getenv("PSR_KERNEL_CLOCKS");
+  return v && v[0] == '1';
+}
+
+void kernel_clock_push(int kind, double bytes, double units, cudaEvent_t a, cudaEvent_t b) {
+  std::lock_guard<std::mutex> lock(clocks::g_clock_mutex);
+  clocks::g_clock_pending.push_back(PendingClock{kind, bytes, units, a, b});
+}
 
 __global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, longlong2* slots, uint64_t mask,
                                    int32_t value_offset) {
@@ -227,6 +260,7 @@ void run(const T* pos, const T* nrm, int64_t n, const Params& prm, cudaStream_t 
   PSR_CUDA(cudaMemcpyAsync(host_tr, R->transforms.p, 32 * sizeof(T), cudaMemcpyDeviceToHost, s));
   PSR_CUDA(cudaMemcpyAsync(host_norm, G.transform.p, 5 * sizeof(T), cudaMemcpyDeviceToHost, s));
   PSR_CUDA(cudaStreamSynchronize(s));
+  R->stats.finish();
   R->iso = double(host_iso);
   for (int i = 0; i < 32; ++i) R->host_transforms[i] = double(host_tr[i]);
   for (int i = 0; i < 5; ++i) R->normalization[i] = double(host_norm[i]);
@@ -700,6 +734,40 @@ int psr_result_stage(const psr_result* R, const char* name, const void** data, i
   *count = it->second.count;
   *elem = it->second.elem;
   return PSR_OK;
+}
+
+int psr_kernel_clocks(psr_kernel_clock* out, int32_t capacity, int32_t* count) {
+  if (!count || (capacity > 0 && !out)) return PSR_EINVAL;
+  try {
+    using namespace psr::clocks;
+    std::lock_guard<std::mutex> lock(g_clock_mutex);
+    for (PendingClock& c : g_clock_pending) {
+      float ms = 0;
+      PSR_CUDA(cudaEventSynchronize(c.b));
+      PSR_CUDA(cudaEventElapsedTime(&ms, c.a, c.b));
+      ClockTotals& t = g_clock_totals[c.kind];
+      t.launches += 1;
+      t.ms += ms;
+      t.bytes += c.bytes;
+      t.units += c.units;
+      cudaEventDestroy(c.a);
+      cudaEventDestroy(c.b);
+    }
+    g_clock_pending.clear();
+    int n = 0;
+    for (int k = 0; k < kClkKinds; ++k) {
+      const ClockTotals& t = g_clock_totals[k];
+      if (!t.launches) continue;
+      if (n < capacity) out[n] = psr_kernel_clock{kClockNames[k], kClockUnits[k], t.launches, t.ms, t.bytes, t.units};
+      ++n;
+      g_clock_totals[k] = ClockTotals();
+    }
+    *count = n;
+    return PSR_OK;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return PSR_ECUDA;
+  }
 }
 
 int psr_kernel_launches(int64_t* count) {

@@ -78,6 +78,47 @@ struct EventMarks {
     if (start) cudaEventDestroy(start);
   }
 };
+// Process-wide device time of selected kernels, for the per-kernel roofline: a diagnostic,
+// off unless PSR_KERNEL_CLOCKS=1 when the launch is issued.  A KernelClock brackets one
+// launch with events; `bytes` is the launch's algorithmic traffic (what it must read and
+// write once), `units` the rows, points or row visits it processes.  psr_kernel_clocks()
+// waits for the events, reports the totals per kernel and clears them.
+enum ClockKind {
+  kClkAssembleSliced,
+  kClkCrossApply,
+  kClkNormalStencil,
+  kClkBaseRelax,
+  kClkStripForward,
+  kClkStripReverse,
+  kClkNormalStencilReverse,
+  kClkLevelRowsReverse,
+  kClkScreeningReverse,
+  kClkKinds
+};
+bool kernel_clocks_on();
+void kernel_clock_push(int kind, double bytes, double units, cudaEvent_t a, cudaEvent_t b);
+struct KernelClock {
+  int kind;
+  double bytes, units;
+  cudaStream_t s;
+  cudaEvent_t a = nullptr;
+  KernelClock(int kind_, double bytes_, double units_, cudaStream_t s_)
+      : kind(kind_), bytes(bytes_), units(units_), s(s_) {
+    if (kernel_clocks_on() && cudaEventCreate(&a) == cudaSuccess) cudaEventRecord(a, s);
+  }
+  void stop() {  // closes the interval (at scope end if not called)
+    cudaEvent_t b = nullptr;
+    if (a && cudaEventCreate(&b) == cudaSuccess && cudaEventRecord(b, s) == cudaSuccess)
+      kernel_clock_push(kind, bytes, units, a, b);
+    else if (a)
+      cudaEventDestroy(a);
+    a = nullptr;
+  }
+  ~KernelClock() { stop(); }
+  KernelClock(const KernelClock&) = delete;
+  KernelClock& operator=(const KernelClock&) = delete;
+};
+
 enum { kBwField, kBwMirror, kBwSweep, kBwOperator, kBwBase, kBwPoints, kBwNormalLoads, kBwSamples, kBwSlots };
 
 // Sets the message psr_last_error returns on this thread.
@@ -151,12 +192,52 @@ template <class T>
 TreeData build_tree(const NormalData<T>& N, int depth, int full_depth, int base_depth, cudaStream_t s);
 
 // ---------------------------------------------------------------- A5-A10 solver.py
+struct RelaxDeferred {
+  int* error = nullptr;                                                // device word, zeroed before the first launch
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* events = nullptr;  // created by the launch, owned by the caller
+};
+void throw_relax_error(int err);  // nonzero relaxation error code -> Error
+
 struct SolveStats {
   double relax_ms = 0;       // ordered relaxation kernels (sum over levels)
   int64_t row_visits = 0;    // rows x sweeps relaxed by the sliced kernels
   int64_t launches = 0;
   std::vector<double> level_relax_ms;
   int64_t finest_row_visits = 0;  // rows x sweeps of the last (finest) sliced level
+  // Read back once, after the caller's stream synchronisation (finish), not per level.
+  DBuf<int> relax_error;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> relax_events;
+  RelaxDeferred defer(cudaStream_t s) {
+    if (!relax_error.p) {
+      relax_error.alloc(1, s);
+      relax_error.zero();
+    }
+    return RelaxDeferred{relax_error.p, &relax_events};
+  }
+  // The stream has synchronised: throws the first relaxation error, else fills the timings.
+  void finish() {
+    int err = 0;
+    if (relax_error.p) PSR_CUDA(cudaMemcpy(&err, relax_error.p, sizeof(int), cudaMemcpyDeviceToHost));
+    for (auto& e : relax_events) {
+      float ms = 0;
+      if (!err) PSR_CUDA(cudaEventElapsedTime(&ms, e.first, e.second));
+      relax_ms += ms;
+      level_relax_ms.push_back(ms);
+    }
+    release();
+    throw_relax_error(err);
+  }
+  void release() {
+    for (auto& e : relax_events) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+    relax_events.clear();
+  }
+  SolveStats() = default;
+  SolveStats(const SolveStats&) = delete;
+  SolveStats& operator=(const SolveStats&) = delete;
+  ~SolveStats() { release(); }
 };
 // With `tape_out` the solve keeps what its adjoint needs (an opaque SolveTape<T>).
 template <class T>
@@ -257,10 +338,13 @@ void build_strip_schedule(const int64_t* keys, int64_t rows, int depth, StripSch
 // runs the exact reverse of the forward sequential order over the same schedule-order rows:
 // slices 2^d .. 0 (logical slice z is stored slice 2^d - z) and the colours of a slice in the
 // order 3, 2, 1, 0 (used by the adjoint on the transposed operator).
+// With `defer`, a launch merges its error code into defer->error (the first nonzero code wins,
+// on the device) and appends its start/end events to defer->events instead of reading either
+// back, so a stage that relaxes several levels synchronises once rather than once per level.
 template <class T, class V, class I>
 void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sidx, const V* sb, V* x, int iters,
                             cudaStream_t s, float* ms, V* hist = nullptr, bool rev = false,
-                            bool record_increment = false);
+                            bool record_increment = false, RelaxDeferred* defer = nullptr);
 
 // Strip-scheduled ordered relaxation (psr_relax.cu): slot-ELL rows in key order, x in key
 // order holds the initial guess and receives the result.

@@ -1037,11 +1037,18 @@ __global__ void footprint_kernel(const int32_t* xstart, const int32_t* bounds, i
 }
 
 // Tasks whose update rows or right-hand sides exceed the staging capacity (they read their
-// rows from global memory), added to *count.
+// rows from global memory), added to caps[3].  The capacity follows from footprint_kernel's
+// caps[0..2] as the launch computes it: rows of row_bytes + vbytes that fit `budget` beside a
+// footprint of caps[0] elements (and its +0 entry).
 __global__ void unstaged_kernel(const int32_t* xstart, const int32_t* bounds, int n, int strips, int per16, int rev,
-                                int row_cap, int b_cap, int* count) {
+                                int64_t budget, int row_bytes, int vbytes, int* caps) {
   int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (n + 1) * strips) return;
+  const int64_t fp_bytes = (int64_t(max(caps[0], 1) + 1) * vbytes + 15) & ~int64_t(15);
+  const int64_t rc = max(int64_t(0), min(int64_t(caps[1]), (budget - fp_bytes - 4 * 16) / (row_bytes + vbytes)));
+  const int row_cap = int(rc);
+  const int b_cap = int(min(int64_t(caps[2]), rc + 4 * per16) / per16 * per16);
+  int* count = caps + 3;
   int z = idx / strips, s = idx % strips, nx = n + 2;
   int x0 = bounds[z * (strips + 1) + s], x1 = bounds[z * (strips + 1) + s + 1];
   int rows = 0, bspan = 0;
@@ -1165,6 +1172,18 @@ __global__ void gather_x_kernel(const int32_t* perm, int64_t n, const V* x, V* s
   if (p < n) sx[p] = x[perm[p]];
 }
 
+// The first nonzero error word of a launch into the stage's deferred word.
+__global__ void merge_error_kernel(const int* launch_error, int* stage_error) {
+  if (threadIdx.x == 0 && *launch_error) atomicCAS(stage_error, 0, *launch_error);
+}
+
+void throw_relax_error(int err) {
+  if (err == 2) throw Error(4, "ordered relaxation: footprint exceeds its capacity");
+  if (err == 3) throw Error(1, "ordered relaxation: an operator column is not its slot's neighbour");
+  if (err == 4) throw Error(4, "ordered relaxation: a bulk copy or a phase did not complete");
+  if (err) throw Error(4, "ordered relaxation: a dependency wait timed out");
+}
+
 // The cluster pipelines for one level, when they apply: every task's rows fit a region and
 // its footprint, peer segments and exports fit shared memory, and `iters` clusters of
 // kPipeCtas CTAs can be resident at once.  Returns false (nothing launched) otherwise.
@@ -1173,7 +1192,7 @@ __global__ void gather_x_kernel(const int32_t* perm, int64_t n, const V* x, V* s
 template <class T, class V, class I>
 static bool relax_pipeline(const StripSchedule& S, const T* svals, const I* sidx, const V* sb, const int32_t* xstart,
                            V* xb0, V* xb1, int iters, cudaStream_t s, float* ms, V* hist, bool rev,
-                           bool record_increment) {
+                           bool record_increment, RelaxDeferred* defer) {
   const char* mode = std::getenv("PSR_RELAX_KERNEL");
   const bool forced = mode && std::string(mode) == "pipeline";
   if (!forced) return false;  // opt-in until validated on hardware
@@ -1314,20 +1333,31 @@ static bool relax_pipeline(const StripSchedule& S, const T* svals, const I* sidx
     trace.zero();
     L.trace = trace.p;
   }
+  const bool timed = ms || (defer && defer->events);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (ms) {
+  if (timed) {
     PSR_CUDA(cudaEventCreate(&e0));
     PSR_CUDA(cudaEventCreate(&e1));
     PSR_CUDA(cudaEventRecord(e0, s));
   }
   PSR_CUDA(cudaLaunchKernelEx(&cfg, kernel, P));
   PSR_LAUNCH_CHECK();
-  if (ms) PSR_CUDA(cudaEventRecord(e1, s));
+  if (timed) PSR_CUDA(cudaEventRecord(e1, s));
+  if (defer && defer->error && !trace_file) {
+    merge_error_kernel<<<1, 32, 0, s>>>(L.error, defer->error);
+    PSR_LAUNCH_CHECK();
+    if (timed) defer->events->emplace_back(e0, e1);
+    return true;
+  }
   const int err = read_scalar(L.error, s);
-  if (ms) {
-    PSR_CUDA(cudaEventElapsedTime(ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+  if (timed) {
+    if (ms) PSR_CUDA(cudaEventElapsedTime(ms, e0, e1));
+    if (defer && defer->events)
+      defer->events->emplace_back(e0, e1);
+    else {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+    }
   }
   if (trace_file) {
     std::vector<long long> h = read_vector(trace.p, trace_count, s);
@@ -1338,16 +1368,13 @@ static bool relax_pipeline(const StripSchedule& S, const T* svals, const I* sidx
       std::fclose(f);
     }
   }
-  if (err == 2) throw Error(4, "ordered relaxation: a task's rows exceed their region");
-  if (err == 3) throw Error(1, "ordered relaxation: an operator column is not its slot's neighbour");
-  if (err == 4) throw Error(4, "ordered relaxation: a bulk copy or a phase did not complete");
-  if (err) throw Error(4, "ordered relaxation: a dependency wait timed out");
+  throw_relax_error(err);
   return true;
 }
 
 template <class T, class V, class I>
 void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sidx, const V* sb, V* x, int iters,
-                            cudaStream_t s, float* ms, V* hist, bool rev, bool record_increment) {
+                            cudaStream_t s, float* ms, V* hist, bool rev, bool record_increment, RelaxDeferred* defer) {
   const int64_t rows = S.rows;
   if (iters <= 0 || rows <= 0) return;
   const int depth = S.depth;
@@ -1363,7 +1390,8 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
   DBuf<int32_t> xstart(int64_t(n + 1) * 4 * nx, s);
   xstart_kernel<<<blocks_for(int64_t(n + 1) * 4 * nx), kThreads, 0, s>>>(skeys_p, off, n, xstart.p);
   PSR_LAUNCH_CHECK();
-  if (relax_pipeline<T, V, I>(S, svals, sidx, sb, xstart.p, x0.p, x1.p, iters, s, ms, hist, rev, record_increment)) {
+  if (relax_pipeline<T, V, I>(S, svals, sidx, sb, xstart.p, x0.p, x1.p, iters, s, ms, hist, rev, record_increment,
+                              defer)) {
     scatter_back_kernel<V><<<blocks_for(rows), kThreads, 0, s>>>(perm, rows, ((iters - 1) & 1) ? x1.p : x0.p, x);
     PSR_LAUNCH_CHECK();
     return;
@@ -1422,13 +1450,11 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
     footprint_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, bounds.p, n, strips, per16,
                                                                         rev ? 1 : 0, caps_dev);
     PSR_LAUNCH_CHECK();
-    caps = read_vector(caps_dev, 3, s);
-    const auto cap = row_capacity(caps[0], caps[1], caps[2]);
     unstaged_kernel<<<blocks_for((n + 1) * strips), kThreads, 0, s>>>(xstart.p, bounds.p, n, strips, per16,
-                                                                       rev ? 1 : 0, int(cap.first), int(cap.second),
-                                                                       caps_dev + 3);
+                                                                       rev ? 1 : 0, budget, int(row_bytes),
+                                                                       int(sizeof(V)), caps_dev);
     PSR_LAUNCH_CHECK();
-    caps.push_back(read_scalar(caps_dev + 3, s));
+    caps = read_vector(caps_dev, 4, s);  // footprint, rows, right-hand side, unstaged tasks
     // narrow the strips until the largest footprint fits the 16-bit offsets
     if (!(sizeof(I) == 4 || caps[0] <= fp_limit) && strips < 256) {
       strips = std::min(256, 2 * strips);
@@ -1518,22 +1544,39 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
     trace.zero();
     L.trace = trace.p;
   }
+  const bool timed = ms || (defer && defer->events);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (ms) {
+  if (timed) {
     PSR_CUDA(cudaEventCreate(&e0));
     PSR_CUDA(cudaEventCreate(&e1));
     PSR_CUDA(cudaEventRecord(e0, s));
   }
-  kernel<<<grid, kRelaxThreads, size_t(smem), s>>>(L);
-  PSR_LAUNCH_CHECK();
-  if (ms) PSR_CUDA(cudaEventRecord(e1, s));
+  {
+    // per row visit: 27 operator values (S), b, x read and written (V), row id, visit record
+    const double visits = double(rows) * iters;
+    KernelClock clock(rev ? kClkStripReverse : kClkStripForward,
+                      visits * (27.0 * sizeof(T) + 3 * sizeof(V) + 4 + (hist ? sizeof(V) : 0)), visits, s);
+    kernel<<<grid, kRelaxThreads, size_t(smem), s>>>(L);
+    PSR_LAUNCH_CHECK();
+  }
+  if (timed) PSR_CUDA(cudaEventRecord(e1, s));
   scatter_back_kernel<V><<<blocks_for(rows), kThreads, 0, s>>>(perm, rows, ((iters - 1) & 1) ? x1.p : x0.p, x);
   PSR_LAUNCH_CHECK();
+  if (defer && defer->error && !trace_file) {
+    merge_error_kernel<<<1, 32, 0, s>>>(L.error, defer->error);
+    PSR_LAUNCH_CHECK();
+    if (timed) defer->events->emplace_back(e0, e1);
+    return;
+  }
   int err = read_scalar(L.error, s);
-  if (ms) {
-    PSR_CUDA(cudaEventElapsedTime(ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+  if (timed) {
+    if (ms) PSR_CUDA(cudaEventElapsedTime(ms, e0, e1));
+    if (defer && defer->events)
+      defer->events->emplace_back(e0, e1);
+    else {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+    }
   }
   if (trace_file) {
     std::vector<long long> h = read_vector(trace.p, total_tasks * kTraceSlots, s);
@@ -1545,10 +1588,7 @@ void relax_strips_scheduled(const StripSchedule& S, const T* svals, const I* sid
       std::fclose(f);
     }
   }
-  if (err == 2) throw Error(4, "ordered relaxation: footprint exceeds its capacity");
-  if (err == 3) throw Error(1, "ordered relaxation: an operator column is not its slot's neighbour");
-  if (err == 4) throw Error(4, "ordered relaxation: a bulk copy did not complete");
-  if (err) throw Error(4, "ordered relaxation: a dependency wait timed out");
+  throw_relax_error(err);
 }
 
 void build_strip_schedule(const int64_t* keys, int64_t rows, int depth, StripSchedule& S, cudaStream_t s) {
@@ -1626,7 +1666,7 @@ template void relax_sliced_strips<float, double>(const int64_t*, int64_t, int, c
 namespace psr {
 #define PSR_SCHED(T, V, I)                                                                                       \
   template void relax_strips_scheduled<T, V, I>(const StripSchedule&, const T*, const I*, const V*, V*, int,  \
-                                                cudaStream_t, float*, V*, bool, bool);
+                                                cudaStream_t, float*, V*, bool, bool, RelaxDeferred*);
 PSR_SCHED(float, float, int16_t)
 PSR_SCHED(float, float, int32_t)
 PSR_SCHED(double, double, int16_t)

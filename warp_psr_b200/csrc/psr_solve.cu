@@ -833,46 +833,144 @@ __device__ __forceinline__ void gs_row_shared(const int32_t* __restrict__ cols, 
   if (diagonal != T(0)) xs_sh[row] = xi + r * (T(1.0) / T(diagonal));
 }
 
+// The row of schedule position j from a slot-major copy of the operator (slot k of position
+// j at k * stride): 27 values v, 27 columns c already clamped to n (absent -> the +0 entry of
+// x), and b.  Consecutive threads take consecutive positions, so each slot is one coalesced
+// (global) or conflict-free (shared) access per warp.  Same arithmetic and order as
+// gs_row_shared.
 template <class T>
-__global__ void __launch_bounds__(1024) relax_colors_shared_kernel(const int32_t* cols, const T* vals, const T* b, T* x,
+__device__ __forceinline__ void gs_row_slots(const T* v, const uint16_t* c, int64_t stride, T bj, T* xs_sh, int32_t row,
+                                             T* rec) {
+  T xv[27], a[27];
+#pragma unroll
+  for (int k = 0; k < 27; ++k) {
+    a[k] = v[k * stride];
+    xv[k] = xs_sh[c[k * stride]];
+  }
+  T r = bj;
+#pragma unroll
+  for (int k = 0; k < 27; ++k) r = r - xv[k] * a[k];
+  T diagonal = T(0);
+  T xi = T(0);
+  if (c[13 * stride] == unsigned(row)) {
+    diagonal = a[13];
+    xi = xv[13];
+  }
+  if (rec) {
+    rec[0] = xi;
+    rec[1] = r;
+  }
+  if (diagonal != T(0)) xs_sh[row] = xi + r * (T(1.0) / T(diagonal));
+}
+
+// Slot-major copy of a base level's operator in colour order (v[k n + j], c[k n + j] with the
+// column clamped to n, bj[j] = b[rows[j]]) for relax_colors_shared_kernel<T, false>.
+template <class T>
+__global__ void base_slots_kernel(const int32_t* cols, const T* vals, const T* b, const int32_t* rows, int64_t n, T* v,
+                                  uint16_t* c, T* bj) {
+  const int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (e >= 27 * n) return;
+  const int64_t j = e / 27, k = e - 27 * j;
+  const int64_t src = int64_t(rows[j]) * kSlots + k;
+  v[k * n + j] = vals[src];
+  c[k * n + j] = uint16_t(min(unsigned(cols[src]), unsigned(n)));
+  if (k == 0) bj[j] = b[rows[j]];
+}
+
+// Shared-memory layout of relax_colors_shared_kernel<T, STAGED> for n rows.
+template <class T, bool STAGED>
+struct BaseRelaxLayout {
+  static constexpr size_t bytes(int64_t n) {
+    return size_t(n + 1) * sizeof(T) + (STAGED ? size_t(28 * n) * sizeof(T) : 0) + size_t(n + 9) * sizeof(int32_t) +
+           (STAGED ? size_t(27 * n) * sizeof(uint16_t) : 0);
+  }
+};
+
+// One CTA relaxes the whole level for `iters` sweeps over the 8 colours.  Shared memory holds
+// x (n + 1 entries, the last a +0 for absent slots), the colour-ordered row list and the 9
+// group offsets, so a colour phase starts with one shared-memory read instead of two
+// dependent global loads (offsets, then row).  The operator comes slot-major in colour order
+// (base_slots_kernel: vT, cT, bT), so the phase's loads are coalesced -- one SM's L1 serves
+// them all, and row-major rows cost a wavefront per lane.  STAGED (levels whose operator fits,
+// up to ~790 float64 rows) copies every slot into shared memory first, so the 8 x iters phases
+// read no global memory; it builds that copy from the row-major operator itself.
+template <class T, bool STAGED>
+__global__ void __launch_bounds__(1024) relax_colors_shared_kernel(const int32_t* cols, const T* vals, const T* b,
+                                                                   const T* vT, const uint16_t* cT, const T* bT, T* x,
                                                                    const int32_t* rows, const int32_t* group_off,
                                                                    int iters, int forward, T* hist, int64_t n) {
   extern __shared__ __align__(16) unsigned char relax_smem[];
   T* xs = reinterpret_cast<T*>(relax_smem);
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) xs[i] = x[i];
+  T* vs = xs + n + 1;                  // STAGED: 27 n values, slot-major
+  T* bs = vs + (STAGED ? 27 * n : 0);  // STAGED: n right-hand sides
+  int32_t* rows_s = reinterpret_cast<int32_t*>(bs + (STAGED ? n : 0));
+  int32_t* off_s = rows_s + n;
+  uint16_t* cs = reinterpret_cast<uint16_t*>(off_s + 9);  // STAGED: 27 n columns, slot-major
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    xs[i] = x[i];
+    rows_s[i] = rows[i];
+    if (STAGED) bs[i] = b[rows[i]];
+  }
+  if (STAGED)
+    for (int64_t e = threadIdx.x; e < 27 * n; e += blockDim.x) {
+      const int64_t j = e / 27, k = e - 27 * j;
+      const int64_t src = int64_t(rows[j]) * kSlots + k;
+      vs[k * n + j] = vals[src];
+      cs[k * n + j] = uint16_t(min(unsigned(cols[src]), unsigned(n)));
+    }
+  if (threadIdx.x <= 8) off_s[threadIdx.x] = group_off[threadIdx.x];
   if (threadIdx.x == 0) xs[n] = T(0);  // the entry absent slots read
   __syncthreads();
   for (int it = 0; it < iters; ++it)
     for (int cc = 0; cc < 8; ++cc) {
       int g = forward ? cc : 7 - cc;
-      for (int j = group_off[g] + threadIdx.x; j < group_off[g + 1]; j += blockDim.x)
-        gs_row_shared(cols, vals, b, xs, rows[j], hist ? hist + 2 * (int64_t(it) * n + rows[j]) : nullptr,
-                      unsigned(n));
+      for (int j = off_s[g] + threadIdx.x; j < off_s[g + 1]; j += blockDim.x) {
+        T* rec = hist ? hist + 2 * (int64_t(it) * n + rows_s[j]) : nullptr;
+        if (STAGED)
+          gs_row_slots(vs + j, cs + j, n, bs[j], xs, rows_s[j], rec);
+        else
+          gs_row_slots(vT + j, cT + j, n, __ldg(bT + j), xs, rows_s[j], rec);
+      }
       __syncthreads();
     }
   for (int64_t i = threadIdx.x; i < n; i += blockDim.x) x[i] = xs[i];
 }
 
-constexpr size_t kRelaxSharedBytes = 200 * 1024;
+constexpr size_t kRelaxSharedBytes = 227 * 1024;  // the opt-in limit of one CTA
 
 // One colour-relaxation call on a small level: shared-memory x when it fits.  1024 threads
 // (41 registers each): a depth-4 colour group of ~600 rows is one pass instead of two.
 template <class T>
 static void relax_colors(const int32_t* cols, const T* vals, const T* b, T* x, const int32_t* rows,
                          const int32_t* group_off, int iters, int forward, T* hist, int64_t n, cudaStream_t s) {
-  const size_t bytes = size_t(n + 1) * sizeof(T);  // x and a +0 entry
-  // PSR_BASE_RELAX=global keeps x in global memory at any size (test override: the path of
-  // base levels too large for shared memory, on small cases).
+  const size_t bytes = BaseRelaxLayout<T, false>::bytes(n), staged_bytes = BaseRelaxLayout<T, true>::bytes(n);
+  // PSR_BASE_RELAX=global keeps x in global memory at any size, =shared never stages the
+  // operator rows (test overrides: the paths of larger base levels, on small cases).
   const char* mode = std::getenv("PSR_BASE_RELAX");
   const bool force_global = mode && mode[0] == 'g';
-  if (n > 0 && bytes <= kRelaxSharedBytes && !force_global) {
-    static bool configured = false;
-    if (!configured) {
-      PSR_CUDA(cudaFuncSetAttribute(relax_colors_shared_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    int(kRelaxSharedBytes)));
-      configured = true;
-    }
-    relax_colors_shared_kernel<T><<<1, 1024, bytes, s>>>(cols, vals, b, x, rows, group_off, iters, forward, hist, n);
+  const bool allow_staged = !(mode && mode[0] == 's');
+  // per row visit: 27 columns and values, b, x read and written, row id, and the tape record
+  const double visits = double(n) * iters;
+  KernelClock clock(kClkBaseRelax, visits * (27.0 * (4 + sizeof(T)) + 3 * sizeof(T) + 4 + (hist ? 2 * sizeof(T) : 0)),
+                    visits, s);
+  static bool configured = false;
+  if (!configured) {
+    PSR_CUDA(cudaFuncSetAttribute(relax_colors_shared_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(kRelaxSharedBytes)));
+    PSR_CUDA(cudaFuncSetAttribute(relax_colors_shared_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(kRelaxSharedBytes)));
+    configured = true;
+  }
+  if (n > 0 && n < 65535 && staged_bytes <= kRelaxSharedBytes && !force_global && allow_staged) {
+    relax_colors_shared_kernel<T, true><<<1, 1024, staged_bytes, s>>>(cols, vals, b, nullptr, nullptr, nullptr, x,
+                                                                      rows, group_off, iters, forward, hist, n);
+  } else if (n > 0 && n < 65535 && bytes <= kRelaxSharedBytes && !force_global) {
+    DBuf<T> vT(27 * n, s), bT(n, s);
+    DBuf<uint16_t> cT(27 * n, s);
+    base_slots_kernel<T><<<blocks_for(27 * n), kThreads, 0, s>>>(cols, vals, b, rows, n, vT.p, cT.p, bT.p);
+    PSR_LAUNCH_CHECK();
+    relax_colors_shared_kernel<T, false><<<1, 1024, bytes, s>>>(cols, vals, b, vT.p, cT.p, bT.p, x, rows, group_off,
+                                                                iters, forward, hist, n);
   } else {
     relax_colors_kernel<T><<<1, 512, 0, s>>>(cols, vals, b, x, rows, group_off, iters, forward, hist, n);
   }
@@ -1260,6 +1358,8 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
     DBuf<double> table(int64_t(res + 1) * width * 2, s);
     normal_table_kernel<<<blocks_for(res + 1), kThreads, 0, s>>>(test_d, normal_d, first, width, table.p);
     PSR_LAUNCH_CHECK();
+    // test key and load per row; key and 4 values per normal record
+    KernelClock clock(kClkNormalStencil, n * 16.0 + nrec * (8.0 + 4 * sizeof(T)), double(n), s);
     if (h.dense && width == 4)
       normal_stencil_dense_kernel<T, 4><<<blocks_for(n), kThreads, 0, s>>>(keys_at(test_d), n, test_d, normal_d, h,
                                                                           noff, nvals, table.p, first, out.p);
@@ -1389,6 +1489,9 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
         using I = decltype(i_tag);
         S* sv = reinterpret_cast<S*>(svals.p);
         I* si = reinterpret_cast<I*>(sidx.p);
+        // key, float64 load, schedule position, operator row, index row, b, screening cell ranges
+        const double row_bytes = 8 + 8 + 4 + kSlots * sizeof(S) + 32 * sizeof(I) + sizeof(T) + (screened ? 64 : 0);
+        KernelClock clock(kClkAssembleSliced, n * row_bytes + (screened ? P.m * 4.0 * sizeof(T) : 0.0), double(n), s);
         if (screened)
           assemble_sliced_kernel<T, S, I, true><<<blocks_for(n, 128), 128, 0, s>>>(
               keys_at(d), n, d, bcv, level_offsets[d], table.p, pv, loads[d].p, sched.inv.p, sched.off.p, sv, si, b.p,
@@ -1518,6 +1621,12 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
         ccols.alloc(kSlots * n, s);
         cvals.alloc(kSlots * n, s);  // every slot written by the cross kernel
       }
+      // key, schedule position, b read and written, screening cell ranges, tape row (columns,
+      // values), the binned points and the coarser cumulative solution
+      KernelClock cross_clock(kClkCrossApply,
+                              n * (8.0 + 4 + 2 * sizeof(T) + (screened ? 64 : 0) + (tp ? kSlots * (4.0 + sizeof(T)) : 0)) +
+                                  (screened ? P.m * 4.0 * sizeof(T) : 0.0) + count_at(d - 1) * double(sizeof(T)),
+                              double(n), s);
       if (screened)
         cross_apply_kernel<T, true><<<blocks_for(n, 128), 128, 0, s>>>(keys_at(d), n, d, bcv, level_offsets[d - 1],
                                                                         ctable.p, pv, cumulative.p, b.p, sched.inv.p,
@@ -1531,39 +1640,43 @@ void solve_levels(const TreeData& tree, const DensityData<T>& D, const NormalDat
         tp->sliced[d].cvals = std::move(cvals);
       }
       PSR_LAUNCH_CHECK();
+      cross_clock.stop();
       if (sink && sink->on) {  // kept in key order, like every other stage
         DBuf<T> kb(n, s);
         unpermute_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(sched.perm.p, n, b.p, kb.p);
         PSR_LAUNCH_CHECK();
         sink->put("rhs_" + std::to_string(d), kb.p, n, s);
       }
-      float ms = 0;
-      float* msp = stats ? &ms : nullptr;
+      RelaxDeferred deferred;
+      RelaxDeferred* dp = nullptr;
+      if (stats) {
+        deferred = stats->defer(s);
+        dp = &deferred;
+      }
+      float* msp = nullptr;
       DBuf<T> hist;
       if (tp) hist.alloc(int64_t(p.iters) * n, s);
       if (mixed) {
         if (sched.wide)
           relax_strips_scheduled<float, T, int32_t>(sched, reinterpret_cast<const float*>(svals.p),
                                                     reinterpret_cast<const int32_t*>(sidx.p), b.p, x, p.iters, s, msp,
-                                                    hist.p);
+                                                    hist.p, false, false, dp);
         else
           relax_strips_scheduled<float, T, int16_t>(sched, reinterpret_cast<const float*>(svals.p),
                                                     reinterpret_cast<const int16_t*>(sidx.p), b.p, x, p.iters, s, msp,
-                                                    hist.p);
+                                                    hist.p, false, false, dp);
       } else {
         if (sched.wide)
           relax_strips_scheduled<T, T, int32_t>(sched, reinterpret_cast<const T*>(svals.p),
                                                 reinterpret_cast<const int32_t*>(sidx.p), b.p, x, p.iters, s, msp,
-                                                hist.p);
+                                                hist.p, false, false, dp);
         else
           relax_strips_scheduled<T, T, int16_t>(sched, reinterpret_cast<const T*>(svals.p),
                                                 reinterpret_cast<const int16_t*>(sidx.p), b.p, x, p.iters, s, msp,
-                                                hist.p);
+                                                hist.p, false, false, dp);
       }
-      if (stats) {
-        stats->relax_ms += ms;
+      if (stats) {  // relax_ms and level_relax_ms are filled by stats->finish()
         stats->row_visits += n * p.iters;
-        stats->level_relax_ms.push_back(ms);
         stats->finest_row_visits = n * p.iters;
         stats->launches += 1;
       }

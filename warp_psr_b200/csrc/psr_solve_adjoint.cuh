@@ -999,6 +999,11 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
   };
 
   const int top = tp.top;
+  // The reverse sweeps' error codes merge into one device word, read once after the sliced
+  // levels (one host synchronisation for all of them).
+  DBuf<int> relax_error(1, s);
+  relax_error.zero();
+  RelaxDeferred deferred{relax_error.p, nullptr};
   // ---- sliced levels, finest first
   for (int d = top; d > base; --d) {
     const int64_t n = count_at(d);
@@ -1026,7 +1031,7 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
       PSR_LAUNCH_CHECK();
       mark(kBwMirror);
       relax_strips_scheduled<S, T, I>(st.sched, tv.p, reinterpret_cast<const I*>(st.sidx.p), sb.p, M.p, p.iters, s,
-                                      nullptr, mu.p, true, true);
+                                      nullptr, mu.p, true, true, &deferred);
       mark(kBwSweep);
     };
     if (tp.mixed) {
@@ -1078,6 +1083,14 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
         rA.alloc(27 * n, s);
         L.row_gA = rA.p;
       }
+      // per row: sorted key, permutation, index row, reverse and forward visit records, g_b,
+      // the 27 operator adjoints, the cross tape row; the coarser cumulative adjoint read and
+      // written
+      KernelClock rows_clock(kClkLevelRowsReverse,
+                             n * (8.0 + 4 + 32 * sizeof(I) + 2.0 * p.iters * sizeof(T) + sizeof(T) +
+                                  (tp.screened ? 27 * sizeof(T) : 0) + kSlots * (4.0 + sizeof(T))) +
+                                 2.0 * count_at(d - 1) * sizeof(T),
+                             double(n), s);
       if (p.iters == 8 && L.ccols) {
         level_rows_reverse_kernel<T, I, 8><<<blocks_for(n, 128), 128, 0, s>>>(
             st.sched.skeys.p, n, st.sched.perm.p, L.off, L.sidx, L.xhist, L.mu, L.g_b, L.ccols, L.cvals,
@@ -1086,8 +1099,14 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
         level_reverse_kernel<T, S, I, true, 0><<<blocks_for(n, 128), 128, 0, s>>>(L);
       }
       PSR_LAUNCH_CHECK();
+      rows_clock.stop();
       if (tp.screened && tp.points[d].m) {
         const int64_t m = tp.points[d].m;
+        // per point: position and weight read, their adjoints written; per row: g_b and the
+        // 27 operator adjoints; the coarser cumulative solution
+        KernelClock points_clock(kClkScreeningReverse,
+                                 m * 8.0 * sizeof(T) + n * 28.0 * sizeof(T) + count_at(d - 1) * double(sizeof(T)),
+                                 double(m), s);
         screening_points_reverse_kernel<T><<<blocks_for(m, 128), 128, 0, s>>>(
             L.P, m, d, bcv, level_offsets[d], g_b.p, rA.p, 27, tp.cum[d - 1].p, level_offsets[d - 1], g_pos[d].p,
             g_w[d].p);
@@ -1106,6 +1125,7 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
     PSR_LAUNCH_CHECK();
     mark(kBwOperator);
   }
+  throw_relax_error(read_scalar(relax_error.p, s));
 
   // ---- base multigrid
   {
@@ -1256,6 +1276,8 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
       DBuf<double> table(int64_t(res + 1) * width * 2, s);
       normal_table_kernel<<<blocks_for(res + 1), kThreads, 0, s>>>(test_d, normal_d, first, width, table.p);
       PSR_LAUNCH_CHECK();
+      // per normal record: key, 3 value adjoints read and written; per test function: its adjoint
+      KernelClock clock(kClkNormalStencilReverse, m * (8.0 + 6 * sizeof(T)) + nt * 8.0, double(m), s);
       normal_stencil_reverse_kernel<T><<<blocks_for(m), kThreads, 0, s>>>(
           nkeys, m, test_d, normal_d, bcv, level_offsets[test_d], g_test, table.p, width, first, g_vals);
       PSR_LAUNCH_CHECK();
