@@ -51,15 +51,43 @@ __global__ void bounds_partial_kernel(const T* __restrict__ pos, int64_t n, T* p
 }
 
 // samples.py:54-88 — bounding cube, scale and the cofactor normal scale.
+// Bounds over the per-block partials, reduced by one block of kBoundsThreads threads (min and
+// max are exact in any grouping, as in the per-block reduction that made the partials).
+constexpr int kBoundsThreads = 256;
 template <class T>
-__global__ void transform_kernel(const T* partial, int blocks, T scale, T* transform, int* status) {
-  if (threadIdx.x != 0) return;
-  T lo[3] = {T(INFINITY), T(INFINITY), T(INFINITY)}, hi[3] = {T(-INFINITY), T(-INFINITY), T(-INFINITY)};
-  for (int b = 0; b < blocks; ++b)
+__device__ void reduce_partials(const T* partial, int blocks, T lo[3], T hi[3]) {
+  __shared__ T s_lo[3][kBoundsThreads], s_hi[3][kBoundsThreads];
+  T l[3] = {T(INFINITY), T(INFINITY), T(INFINITY)}, h[3] = {T(-INFINITY), T(-INFINITY), T(-INFINITY)};
+  for (int b = threadIdx.x; b < blocks; b += blockDim.x)
     for (int a = 0; a < 3; ++a) {
-      lo[a] = dmin(lo[a], partial[6 * b + a]);
-      hi[a] = dmax(hi[a], partial[6 * b + 3 + a]);
+      l[a] = dmin(l[a], partial[6 * b + a]);
+      h[a] = dmax(h[a], partial[6 * b + 3 + a]);
     }
+  for (int a = 0; a < 3; ++a) {
+    s_lo[a][threadIdx.x] = l[a];
+    s_hi[a][threadIdx.x] = h[a];
+  }
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int a = 0; a < 3; ++a) {
+        s_lo[a][threadIdx.x] = dmin(s_lo[a][threadIdx.x], s_lo[a][threadIdx.x + st]);
+        s_hi[a][threadIdx.x] = dmax(s_hi[a][threadIdx.x], s_hi[a][threadIdx.x + st]);
+      }
+    __syncthreads();
+  }
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = s_lo[a][0];
+    hi[a] = s_hi[a][0];
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBoundsThreads) transform_kernel(const T* partial, int blocks, T scale, T* transform,
+                                                                   int* status) {
+  T lo[3], hi[3];
+  reduce_partials(partial, blocks, lo, hi);
+  if (threadIdx.x != 0) return;
   T width = dmax(hi[0] - lo[0], dmax(hi[1] - lo[1], hi[2] - lo[2])) * scale;
   if (!isfinite(width) || width <= T(0)) {
     status[0] += 1;
@@ -144,14 +172,10 @@ __global__ void groups_kernel(const uint64_t* __restrict__ keys, const int32_t* 
 
 // Adjoint bookkeeping: bounding box and the lowest input index attaining each bound.
 template <class T>
-__global__ void bounds_final_kernel(const T* partial, int blocks, T* bounds) {
+__global__ void __launch_bounds__(kBoundsThreads) bounds_final_kernel(const T* partial, int blocks, T* bounds) {
+  T lo[3], hi[3];
+  reduce_partials(partial, blocks, lo, hi);
   if (threadIdx.x != 0) return;
-  T lo[3] = {T(INFINITY), T(INFINITY), T(INFINITY)}, hi[3] = {T(-INFINITY), T(-INFINITY), T(-INFINITY)};
-  for (int b = 0; b < blocks; ++b)
-    for (int a = 0; a < 3; ++a) {
-      lo[a] = dmin(lo[a], partial[6 * b + a]);
-      hi[a] = dmax(hi[a], partial[6 * b + 3 + a]);
-    }
   for (int a = 0; a < 3; ++a) {
     bounds[a] = lo[a];
     bounds[3 + a] = hi[a];
@@ -202,12 +226,12 @@ SampleGroups<T> prepare_samples(const T* pos, const T* nrm, int64_t n, int depth
   G.transform.zero();
   bounds_partial_kernel<T><<<blocks, kThreads, 0, s>>>(pos, n, partial.p, status.p);
   PSR_LAUNCH_CHECK();
-  transform_kernel<T><<<1, 32, 0, s>>>(partial.p, blocks, T(scale), G.transform.p, status.p);
+  transform_kernel<T><<<1, kBoundsThreads, 0, s>>>(partial.p, blocks, T(scale), G.transform.p, status.p);
   PSR_LAUNCH_CHECK();
   if (read_scalar(status.p, s)) throw Error(3, "Nonfinite positions or degenerate/overflowing bounding cube");
   if (keep) {
     G.bounds.alloc(6, s);
-    bounds_final_kernel<T><<<1, 32, 0, s>>>(partial.p, blocks, G.bounds.p);
+    bounds_final_kernel<T><<<1, kBoundsThreads, 0, s>>>(partial.p, blocks, G.bounds.p);
     PSR_LAUNCH_CHECK();
     G.bound_owner.alloc(6, s);
     PSR_CUDA(cudaMemsetAsync(G.bound_owner.p, 0x7f, 6 * sizeof(int32_t), s));
@@ -619,19 +643,26 @@ __global__ void average_contrib_kernel(const int32_t* order, int64_t n, const T*
 }
 
 // Fixed 1024-item chunks summed serially (in T, input order) — the order the oracle
-// restates — then the chunk totals serially.
+// restates — then the chunk totals serially.  One block per chunk copies the chunk's 3 x 1024
+// values into shared memory with coalesced loads, then one thread adds them in order (a
+// serial loop over global memory waits an L2 round trip per item).
+constexpr int kAverageChunk = 1024, kAverageThreads = 128;
 template <class T>
-__global__ void average_chunks_kernel(const T* contrib, int64_t n, T* partial) {
-  int64_t chunk = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  int64_t begin = chunk * 1024;
+__global__ void __launch_bounds__(kAverageThreads) average_chunks_kernel(const T* contrib, int64_t n, T* partial) {
+  __shared__ T s_c[3 * kAverageChunk];
+  const int64_t chunk = blockIdx.x;
+  const int64_t begin = chunk * kAverageChunk;
   if (begin >= n) return;
-  int64_t end = begin + 1024 < n ? begin + 1024 : n;
+  const int count = int(begin + kAverageChunk < n ? kAverageChunk : n - begin);
+  for (int e = threadIdx.x; e < 3 * count; e += blockDim.x) s_c[e] = contrib[3 * begin + e];
+  __syncthreads();
+  if (threadIdx.x != 0) return;
   T part[3] = {T(0), T(0), T(0)};
-  for (int64_t i = begin; i < end; ++i) {
-    T c2 = contrib[3 * i + 2];
+  for (int i = 0; i < count; ++i) {
+    T c2 = s_c[3 * i + 2];
     if (c2 > T(0)) {
-      part[0] = part[0] + contrib[3 * i];
-      part[1] = part[1] + contrib[3 * i + 1];
+      part[0] = part[0] + s_c[3 * i];
+      part[1] = part[1] + s_c[3 * i + 1];
       part[2] = part[2] + c2;
     }
   }
@@ -639,11 +670,19 @@ __global__ void average_chunks_kernel(const T* contrib, int64_t n, T* partial) {
 }
 
 template <class T>
-__global__ void average_finish_kernel(const T* partial, int64_t chunks, T* average) {
-  if (threadIdx.x != 0) return;
+__global__ void __launch_bounds__(kAverageThreads) average_finish_kernel(const T* partial, int64_t chunks, T* average) {
+  __shared__ T s_p[3 * kAverageChunk];
   T total[3] = {T(0), T(0), T(0)};
-  for (int64_t c = 0; c < chunks; ++c)
-    for (int a = 0; a < 3; ++a) total[a] = total[a] + partial[3 * c + a];
+  for (int64_t c0 = 0; c0 < chunks; c0 += kAverageChunk) {  // tiles of chunk totals, in order
+    const int count = int(c0 + kAverageChunk < chunks ? kAverageChunk : chunks - c0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < 3 * count; e += blockDim.x) s_p[e] = partial[3 * c0 + e];
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int c = 0; c < count; ++c)
+        for (int a = 0; a < 3; ++a) total[a] = total[a] + s_p[3 * c + a];
+  }
+  if (threadIdx.x != 0) return;
   average[0] = average[1] = average[2] = T(0);
   if (total[2] > T(0)) {
     average[0] = total[0] / total[2];
@@ -701,15 +740,15 @@ NormalData<T> build_normals(const SampleGroups<T>& g, const DensityData<T>& D, i
       PSR_LAUNCH_CHECK();
     }
   }
-  int64_t chunks = (n + 1023) / 1024;
+  int64_t chunks = (n + kAverageChunk - 1) / kAverageChunk;
   DBuf<T> partial(3 * chunks, s), contrib(3 * n, s);
   average_contrib_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(order.p, n, g.normal_sums.p, g.weights.p, D.dw.p,
                                                                contrib.p);
   PSR_LAUNCH_CHECK();
-  average_chunks_kernel<T><<<blocks_for(chunks, 64), 64, 0, s>>>(contrib.p, n, partial.p);
+  if (chunks) average_chunks_kernel<T><<<unsigned(chunks), kAverageThreads, 0, s>>>(contrib.p, n, partial.p);
   PSR_LAUNCH_CHECK();
   N.average.alloc(3, s);
-  average_finish_kernel<T><<<1, 32, 0, s>>>(partial.p, chunks, N.average.p);
+  average_finish_kernel<T><<<1, kAverageThreads, 0, s>>>(partial.p, chunks, N.average.p);
   PSR_LAUNCH_CHECK();
   DBuf<int64_t> off(maximum + 2, s);
   depth_offsets_kernel<<<1, 32, 0, s>>>(N.keys.p, N.count, maximum + 2, off.p);

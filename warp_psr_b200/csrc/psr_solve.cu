@@ -251,12 +251,32 @@ __global__ void __launch_bounds__(256, 6) normal_stencil_kernel(const int64_t* k
   out[i] = value;
 }
 
+// The first three components of a normal record (4 values, 16- or 32-byte aligned) with
+// one vector load and one scalar load (double) or one vector load (float).
+__device__ __forceinline__ void load_normal3(const double* v, double& a, double& b, double& c) {
+  const double2 ab = __ldg(reinterpret_cast<const double2*>(v));
+  a = ab.x;
+  b = ab.y;
+  c = __ldg(v + 2);
+}
+__device__ __forceinline__ void load_normal3(const float* v, float& a, float& b, float& c) {
+  const float4 r = __ldg(reinterpret_cast<const float4*>(v));
+  a = r.x;
+  b = r.y;
+  c = r.z;
+}
+
 // The same with the dense column table and a compile-time window W: for each x the W
 // columns' ranges are read together and their lower bounds of z0 advance in lock step, and
 // the up to W keys after each bound (increasing z, so in the z-loop's order) are loaded
-// together.  The additions run in the same (x, y, z) order: same result.
+// together.  The row's 1-D integrals along y and z (2 W table entries each) are loaded once
+// into registers; a column's normals in the window become a bit mask over the W z offsets
+// (keys ascend, so the t-th set bit is the t-th key after the bound), which keeps every
+// register index a constant.  The kernel is bound by L1 throughput (scattered 8-byte loads),
+// so fewer loads per row is what counts.  The additions run in the same (x, y, z) order with
+// the same products: same result.
 template <class T, int W>
-__global__ void __launch_bounds__(256, W == 4 ? 5 : 4) normal_stencil_dense_kernel(const int64_t* keys, int64_t n, int test_depth,
+__global__ void __launch_bounds__(256, W == 4 ? 4 : 2) normal_stencil_dense_kernel(const int64_t* keys, int64_t n, int test_depth,
                                                                       int normal_depth, ColumnView cv, int64_t noff,
                                                                       const T* nvals, const double* table, int first,
                                                                       double* out) {
@@ -270,11 +290,18 @@ __global__ void __launch_bounds__(256, W == 4 ? 5 : 4) normal_stencil_dense_kern
   const int side = lim + 1;
   const int z0 = ctr[2] + first;
   const int2* dense = cv.dense + dense_column_base(normal_depth);
+  const double2* tab = reinterpret_cast<const double2*>(table);  // entry (coordinate * W + offset)
+  double2 ty[W], tz[W];
+#pragma unroll
+  for (int o = 0; o < W; ++o) {
+    ty[o] = __ldg(tab + c[1] * W + o);
+    tz[o] = __ldg(tab + c[2] * W + o);
+  }
   double value = 0.0;
   for (int x = 0; x < W; ++x) {
     const int nx = ctr[0] + x + first;
     if (nx < 0 || nx >= lim) continue;
-    const double* ix = table + (c[0] * W + x) * 2;
+    const double2 tx = __ldg(tab + c[0] * W + x);
     int32_t lo[W], hi[W], end[W];
 #pragma unroll
     for (int y = 0; y < W; ++y) {
@@ -308,20 +335,22 @@ __global__ void __launch_bounds__(256, W == 4 ? 5 : 4) normal_stencil_dense_kern
     }
 #pragma unroll
     for (int y = 0; y < W; ++y) {
-      const double* iy = table + (c[1] * W + y) * 2;
-      int dz[W];
-#pragma unroll
-      for (int e = 0; e < W; ++e)
-        dz[e] = lo[y] + e < end[y] ? int(__ldg(cv.keys + lo[y] + e) & 65535) - z0 : W;
+      uint32_t mask = 0;  // bit t: a normal at z0 + t (keys after lo[y] ascend in z)
 #pragma unroll
       for (int e = 0; e < W; ++e) {
-        if (dz[e] >= W) break;  // past the window (z ascending)
-        if (z0 + dz[e] >= lim) continue;
-        const double* iz = table + (c[2] * W + dz[e]) * 2;
-        const T* v = nvals + 4 * (int64_t(lo[y] + e) - noff);
-        value += double(v[0]) * ix[1] * iy[0] * iz[0];
-        value += double(v[1]) * ix[0] * iy[1] * iz[0];
-        value += double(v[2]) * ix[0] * iy[0] * iz[1];
+        const int dz = lo[y] + e < end[y] ? int(__ldg(cv.keys + lo[y] + e) & 65535) - z0 : W;
+        if (dz < W) mask |= 1u << dz;
+      }
+#pragma unroll
+      for (int t = 0; t < W; ++t) {
+        if (!((mask >> t) & 1u)) continue;
+        if (z0 + t >= lim) continue;
+        const int64_t idx = int64_t(lo[y]) + __popc(mask & ((1u << t) - 1u));
+        T v0, v1, v2;
+        load_normal3(nvals + 4 * (idx - noff), v0, v1, v2);
+        value += double(v0) * tx.y * ty[y].x * tz[t].x;
+        value += double(v1) * tx.x * ty[y].y * tz[t].x;
+        value += double(v2) * tx.x * ty[y].x * tz[t].y;
       }
     }
   }
@@ -552,6 +581,47 @@ __device__ __forceinline__ double screening_row(const PointsView<T>& P, const in
   return rhs;
 }
 
+// screening_row for trial functions at the row's own depth, with compile-time slots.  A
+// point of the row's k8-th support cell c - o (o = (k8/4, k8/2%2, k8%2)) lies in that cell's
+// floor bin (points_kernel bins with the same clamp(floor(p 2^d)) as screening_row), so
+// screening_row's f is 1 - o for every such point and its eight trial functions are the
+// slots (1 - o) + e, all inside the 3x3x3 window.  With both loops unrolled every acc index is
+// a constant and acc stays in registers instead of local memory.  Same contributions, same
+// order, same arithmetic as screening_row.
+template <class T>
+__device__ __forceinline__ double screening_row_same(const PointsView<T>& P, const int c[3], int d, uint32_t present,
+                                                     double acc[27], int2* rout) {
+  double rhs = 0.0;
+#pragma unroll
+  for (int k8 = 0; k8 < 8; ++k8) {
+    const int o0 = k8 / 4, o1 = (k8 / 2) % 2, o2 = k8 % 2;
+    int2 range = make_int2(0, 0);
+    const int cell[3] = {c[0] - o0, c[1] - o1, c[2] - o2};
+    if (dmin(cell[0], dmin(cell[1], cell[2])) >= 0 && dmax(cell[0], dmax(cell[1], cell[2])) < (1 << d)) {
+      int32_t u = P.bins.find(basis_key(d, cell[0], cell[1], cell[2]));
+      if (u >= 0) range = make_int2(P.bstart[u], P.bstart[u + 1]);
+    }
+    if (rout) rout[k8] = range;
+    for (int32_t j = range.x; j < range.y; ++j) {
+      T p[3] = {P.spos[3 * j], P.spos[3 * j + 1], P.spos[3 * j + 2]};
+      T weight = P.sw[j];
+      if (weight == T(0)) continue;
+      T phi = hat3(p, c, d);
+      rhs += double(phi * weight);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int s0 = 1 - o0 + e / 4, s1 = 1 - o1 + (e / 2) % 2, s2 = 1 - o2 + e % 2;
+        const int k = s0 * 9 + s1 * 3 + s2;
+        if (!((present >> k) & 1)) continue;
+        const int q[3] = {c[0] - 1 + s0, c[1] - 1 + s1, c[2] - 1 + s2};
+        T trial = hat3(p, q, d);
+        acc[k] += double(phi * trial * weight);
+      }
+    }
+  }
+  return rhs;
+}
+
 // ------------------------------------------------------------------ A5/A7 level assembly
 // Same-level operator rows (stiffness.py:38-108 + screening) and b = T(load) + 0.5*T(point load).
 template <class T, bool SCREEN>
@@ -567,10 +637,7 @@ __global__ void assemble_level_kernel(const int64_t* keys, int64_t n, int d, Col
   double acc[27];
   for (int k = 0; k < 27; ++k) acc[k] = 0.0;
   double pl = 0.0;
-  if (SCREEN) {
-    int q0[3] = {c[0] - 1, c[1] - 1, c[2] - 1};
-    pl = screening_row(P, c, d, d, q0, present, acc);
-  }
+  if (SCREEN) pl = screening_row_same(P, c, d, present, acc, nullptr);
   for (int k = 0; k < 27; ++k) {
     T v = T(0);
     if (col[k] >= 0) {
@@ -593,7 +660,7 @@ __global__ void assemble_level_kernel(const int64_t* keys, int64_t n, int d, Col
 // indices inside their (slice, colour) group (slot 27 = the row's own index), and
 // b = T(load) + 0.5*T(point load).
 template <class T, class S, class I, bool SCREEN>
-__global__ void __launch_bounds__(128, 12) assemble_sliced_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t off,
+__global__ void __launch_bounds__(128, 4) assemble_sliced_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t off,
                                        const double* table, PointsView<T> P, const double* load, const int32_t* inv,
                                        const int32_t* group_off, S* svals, I* sidx, T* sb,
                                        int2* ranges_out = nullptr) {
@@ -604,15 +671,14 @@ __global__ void __launch_bounds__(128, 12) assemble_sliced_kernel(const int64_t*
   int32_t col[27];
   uint32_t present = neighbours27(cv, d, c, off, col);
   double acc[27];
+#pragma unroll
   for (int k = 0; k < 27; ++k) acc[k] = 0.0;
   double pl = 0.0;
-  if (SCREEN) {
-    int q0[3] = {c[0] - 1, c[1] - 1, c[2] - 1};
-    pl = screening_row(P, c, d, d, q0, present, acc, nullptr, ranges_out ? ranges_out + 8 * i : nullptr);
-  }
+  if (SCREEN) pl = screening_row_same(P, c, d, present, acc, ranges_out ? ranges_out + 8 * i : nullptr);
   const int64_t p = inv[i];
   __align__(16) S v[28];  // written to global memory as 16-byte vectors
   __align__(16) I idx[32];
+#pragma unroll
   for (int k = 0; k < 27; ++k) {
     v[k] = S(0);
     idx[k] = idx_absent<I>();

@@ -932,6 +932,93 @@ __global__ void __launch_bounds__(256, 5) normal_stencil_reverse_kernel(const in
   for (int ax = 0; ax < 3; ++ax) g_vals[4 * j + ax] = g_vals[4 * j + ax] + T(acc[ax]);
 }
 
+// normal_stencil_reverse_kernel for test functions at the normals' own depth, with the dense
+// column table and a compile-time window W: the test functions whose window holds normal a
+// are w0 + [0, W)^3 with w0 = a - first - W + 1, and the one at window index u along an axis
+// uses table entry ((w0 + u) W + W - 1 - u), so each axis' W entries are loaded once into
+// registers.  Per x the W columns' lower bounds advance in lock step (as in the forward
+// stencil), and a column's test functions in the window become a bit mask over the W z
+// offsets (keys ascend).  Additions in the same (x, y, z) order with the same products as
+// normal_stencil_reverse_kernel: same result.
+template <class T, int W>
+__global__ void __launch_bounds__(256, 3) normal_stencil_reverse_same_kernel(const int64_t* nkeys, int64_t m, int depth,
+                                                                             ColumnView tcv, int64_t toff,
+                                                                             const double* g_test, const double* table,
+                                                                             int first, T* g_vals) {
+  const int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (j >= m) return;
+  int a[3];
+  key_coords(nkeys[j], a);
+  const int tl = 1 << depth, side = tl + 1;
+  const int w0[3] = {a[0] - first - W + 1, a[1] - first - W + 1, a[2] - first - W + 1};
+  const int zlo = max(w0[2], 0);
+  const double2* tab = reinterpret_cast<const double2*>(table);
+  double2 ty[W], tz[W];
+#pragma unroll
+  for (int u = 0; u < W; ++u) {
+    const int yi = w0[1] + u, zi = w0[2] + u;
+    ty[u] = yi >= 0 && yi <= tl ? __ldg(tab + yi * W + (W - 1 - u)) : make_double2(0.0, 0.0);
+    tz[u] = zi >= 0 && zi <= tl ? __ldg(tab + zi * W + (W - 1 - u)) : make_double2(0.0, 0.0);
+  }
+  const int2* dense = tcv.dense + dense_column_base(depth);
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int u = 0; u < W; ++u) {
+    const int xi = w0[0] + u;
+    if (xi < 0 || xi > tl) continue;
+    const double2 tx = __ldg(tab + xi * W + (W - 1 - u));
+    int32_t lo[W], hi[W], end[W];
+#pragma unroll
+    for (int v = 0; v < W; ++v) {
+      const int yi = w0[1] + v;
+      lo[v] = 0;
+      end[v] = 0;
+      if (yi >= 0 && yi <= tl) {
+        const int2 e = __ldg(dense + int64_t(xi) * side + yi);
+        if (e.x >= 0) {
+          lo[v] = e.x;
+          end[v] = e.x + e.y;
+        }
+      }
+      hi[v] = end[v];
+    }
+    for (int step = 0; step < 32; ++step) {
+      bool active = false;
+#pragma unroll
+      for (int v = 0; v < W; ++v) active |= lo[v] < hi[v];
+      if (!active) break;
+#pragma unroll
+      for (int v = 0; v < W; ++v) {
+        if (lo[v] < hi[v]) {
+          const int32_t mid = (lo[v] + hi[v]) >> 1;
+          if (int(__ldg(tcv.keys + mid) & 65535) < zlo)
+            lo[v] = mid + 1;
+          else
+            hi[v] = mid;
+        }
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < W; ++v) {
+      uint32_t mask = 0;  // bit t: a test function at w0[2] + t
+#pragma unroll
+      for (int e = 0; e < W; ++e) {
+        const int dz = lo[v] + e < end[v] ? int(__ldg(tcv.keys + lo[v] + e) & 65535) - w0[2] : W;
+        if (dz < W) mask |= 1u << dz;
+      }
+#pragma unroll
+      for (int t = 0; t < W; ++t) {
+        if (!((mask >> t) & 1u)) continue;
+        const int64_t r = int64_t(lo[v]) + __popc(mask & ((1u << t) - 1u));
+        const double g = __ldg(g_test + (r - toff));
+        acc[0] += g * tx.y * ty[v].x * tz[t].x;
+        acc[1] += g * tx.x * ty[v].y * tz[t].x;
+        acc[2] += g * tx.x * ty[v].x * tz[t].y;
+      }
+    }
+  }
+  for (int ax = 0; ax < 3; ++ax) g_vals[4 * j + ax] = g_vals[4 * j + ax] + T(acc[ax]);
+}
+
 // Transpose of prolong_normals_kernel: own record and the 8 coarse parents.
 template <class T>
 __global__ void prolong_normals_reverse_kernel(const int64_t* keys, int64_t n, int d, HashView nh, HashView bh,
@@ -1278,8 +1365,12 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
       PSR_LAUNCH_CHECK();
       // per normal record: key, 3 value adjoints read and written; per test function: its adjoint
       KernelClock clock(kClkNormalStencilReverse, m * (8.0 + 6 * sizeof(T)) + nt * 8.0, double(m), s);
-      normal_stencil_reverse_kernel<T><<<blocks_for(m), kThreads, 0, s>>>(
-          nkeys, m, test_d, normal_d, bcv, level_offsets[test_d], g_test, table.p, width, first, g_vals);
+      if (test_d == normal_d && width == 4 && bcv.dense)
+        normal_stencil_reverse_same_kernel<T, 4><<<blocks_for(m), kThreads, 0, s>>>(
+            nkeys, m, test_d, bcv, level_offsets[test_d], g_test, table.p, first, g_vals);
+      else
+        normal_stencil_reverse_kernel<T><<<blocks_for(m), kThreads, 0, s>>>(
+            nkeys, m, test_d, normal_d, bcv, level_offsets[test_d], g_test, table.p, width, first, g_vals);
       PSR_LAUNCH_CHECK();
     };
     // finer chain: loads[d] = same[d] + finer_d + parent[d], finer_{d-1} = child[d-1] + P^T finer_d
