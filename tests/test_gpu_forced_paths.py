@@ -64,3 +64,27 @@ def test_forced_paths_reconstruct_identically(monkeypatch, precision, name, valu
         ref = oracle.OracleResult(p.astype(dt), n.astype(dt), **options(kat["params"]))
         np.testing.assert_array_equal(forced.field.keys.cpu().numpy(), ref.keys)
         np.testing.assert_array_equal(forced.field.coefficients.cpu().numpy(), ref.coefficients)
+
+
+@pytest.mark.parametrize("precision", ["input", "mixed"])
+def test_window_reverse_normal_stencils_match_generic(monkeypatch, precision):
+    """The reverse normal-load stencils for same-depth and one-coarser test functions (lock-step
+    window kernels) give the generic kernel's gradients (PSR_NORMAL_REVERSE=generic forces the
+    generic kernel for every window).  The comparison is to rounding, not bitwise: other
+    stages of the reverse pass add with float64 atomics (the cross-term adjoint), so two
+    passes over the same inputs already differ in the last bits."""
+    from warp_psr_b200 import clouds, reconstruct_differentiable
+    p0, n0 = clouds.sphere(20000)
+    q = torch.tensor(p0[::97], dtype=torch.float64, device="cuda")
+    grads = []
+    for mode in (None, "generic"):
+        if mode:
+            monkeypatch.setenv("PSR_NORMAL_REVERSE", mode)
+        P = torch.tensor(p0, dtype=torch.float64, device="cuda", requires_grad=True)
+        N = torch.tensor(n0, dtype=torch.float64, device="cuda", requires_grad=True)
+        res = reconstruct_differentiable(P, N, depth=7, full_depth=4, point_weight=2.0, precision=precision)
+        v, _, _ = res.evaluate(q, centered=True)
+        torch.nan_to_num(v).square().sum().backward()
+        grads.append((P.grad.cpu().numpy(), N.grad.cpu().numpy()))
+    for a, b in zip(grads[0], grads[1]):
+        np.testing.assert_allclose(a, b, rtol=1e-10, atol=1e-12 * np.abs(b).max())

@@ -137,14 +137,24 @@ __global__ void isovalue_blocks_kernel(const T* values, const T* weights, int64_
 }
 
 template <class T>
-__global__ void isovalue_finish_kernel(const double* partial, int64_t blocks, T* out) {
-  if (threadIdx.x != 0) return;
+__global__ void __launch_bounds__(128) isovalue_finish_kernel(const double* partial, int64_t blocks, T* out) {
+  // block totals summed serially in order by one thread, from tiles staged in shared memory
+  // with coalesced loads (a loop over global memory waits an L2 round trip per total)
+  constexpr int kTile = 1024;
+  __shared__ double s_p[2 * kTile];
   double total = 0.0, mass = 0.0;
-  for (int64_t b = 0; b < blocks; ++b) {
-    total += partial[2 * b];
-    mass += partial[2 * b + 1];
+  for (int64_t b0 = 0; b0 < blocks; b0 += kTile) {
+    const int count = int(b0 + kTile < blocks ? kTile : blocks - b0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < 2 * count; e += blockDim.x) s_p[e] = partial[2 * b0 + e];
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int b = 0; b < count; ++b) {
+        total += s_p[2 * b];
+        mass += s_p[2 * b + 1];
+      }
   }
-  out[0] = T(total / mass);
+  if (threadIdx.x == 0) out[0] = T(total / mass);
 }
 
 template <class T>
@@ -155,7 +165,7 @@ void isovalue(const T* values, const T* weights, int64_t n, T* out, cudaStream_t
     isovalue_blocks_kernel<T><<<unsigned(blocks), 256, 0, s>>>(values, weights, n, partial.p);
     PSR_LAUNCH_CHECK();
   }
-  isovalue_finish_kernel<T><<<1, 32, 0, s>>>(partial.p, blocks, out);
+  isovalue_finish_kernel<T><<<1, 128, 0, s>>>(partial.p, blocks, out);
   PSR_LAUNCH_CHECK();
 }
 
@@ -244,7 +254,7 @@ static void isovalue_static(const T* values, const T* weights, int64_t n, T* out
   // `blocks` of them, so no slot has to start at zero.
   isovalue_blocks_kernel<T><<<unsigned(blocks), 256, 0, s>>>(values, weights, n, partial);
   PSR_LAUNCH_CHECK();
-  isovalue_finish_kernel<T><<<1, 32, 0, s>>>(partial, blocks, out);
+  isovalue_finish_kernel<T><<<1, 128, 0, s>>>(partial, blocks, out);
   PSR_LAUNCH_CHECK();
 }
 

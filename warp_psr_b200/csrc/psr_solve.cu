@@ -276,7 +276,7 @@ __device__ __forceinline__ void load_normal3(const float* v, float& a, float& b,
 // so fewer loads per row is what counts.  The additions run in the same (x, y, z) order with
 // the same products: same result.
 template <class T, int W>
-__global__ void __launch_bounds__(256, W == 4 ? 4 : 2) normal_stencil_dense_kernel(const int64_t* keys, int64_t n, int test_depth,
+__global__ void __launch_bounds__(256, W == 4 ? 4 : 3) normal_stencil_dense_kernel(const int64_t* keys, int64_t n, int test_depth,
                                                                       int normal_depth, ColumnView cv, int64_t noff,
                                                                       const T* nvals, const double* table, int first,
                                                                       double* out) {
@@ -291,10 +291,13 @@ __global__ void __launch_bounds__(256, W == 4 ? 4 : 2) normal_stencil_dense_kern
   const int z0 = ctr[2] + first;
   const int2* dense = cv.dense + dense_column_base(normal_depth);
   const double2* tab = reinterpret_cast<const double2*>(table);  // entry (coordinate * W + offset)
-  double2 ty[W], tz[W];
+  // W = 6 keeps only z's entries in registers (y's are read per window column): with both,
+  // the wide window needs more registers than 3 blocks per SM allow.
+  constexpr int WY = W <= 4 ? W : 1;
+  double2 ty[WY], tz[W];
 #pragma unroll
   for (int o = 0; o < W; ++o) {
-    ty[o] = __ldg(tab + c[1] * W + o);
+    if (W <= 4) ty[o < WY ? o : 0] = __ldg(tab + c[1] * W + o);
     tz[o] = __ldg(tab + c[2] * W + o);
   }
   double value = 0.0;
@@ -335,6 +338,7 @@ __global__ void __launch_bounds__(256, W == 4 ? 4 : 2) normal_stencil_dense_kern
     }
 #pragma unroll
     for (int y = 0; y < W; ++y) {
+      const double2 tyy = W <= 4 ? ty[y < WY ? y : 0] : __ldg(tab + c[1] * W + y);
       uint32_t mask = 0;  // bit t: a normal at z0 + t (keys after lo[y] ascend in z)
 #pragma unroll
       for (int e = 0; e < W; ++e) {
@@ -348,9 +352,9 @@ __global__ void __launch_bounds__(256, W == 4 ? 4 : 2) normal_stencil_dense_kern
         const int64_t idx = int64_t(lo[y]) + __popc(mask & ((1u << t) - 1u));
         T v0, v1, v2;
         load_normal3(nvals + 4 * (idx - noff), v0, v1, v2);
-        value += double(v0) * tx.y * ty[y].x * tz[t].x;
-        value += double(v1) * tx.x * ty[y].y * tz[t].x;
-        value += double(v2) * tx.x * ty[y].x * tz[t].y;
+        value += double(v0) * tx.y * tyy.x * tz[t].x;
+        value += double(v1) * tx.x * tyy.y * tz[t].x;
+        value += double(v2) * tx.x * tyy.x * tz[t].y;
       }
     }
   }
@@ -660,7 +664,7 @@ __global__ void assemble_level_kernel(const int64_t* keys, int64_t n, int d, Col
 // indices inside their (slice, colour) group (slot 27 = the row's own index), and
 // b = T(load) + 0.5*T(point load).
 template <class T, class S, class I, bool SCREEN>
-__global__ void __launch_bounds__(128, 4) assemble_sliced_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t off,
+__global__ void __launch_bounds__(128, 5) assemble_sliced_kernel(const int64_t* keys, int64_t n, int d, ColumnView cv, int64_t off,
                                        const double* table, PointsView<T> P, const double* load, const int32_t* inv,
                                        const int32_t* group_off, S* svals, I* sidx, T* sb,
                                        int2* ranges_out = nullptr) {
@@ -668,8 +672,22 @@ __global__ void __launch_bounds__(128, 4) assemble_sliced_kernel(const int64_t* 
   if (i >= n) return;
   int c[3];
   key_coords(keys[i], c);
-  int32_t col[27];
-  uint32_t present = neighbours27(cv, d, c, off, col);
+  // The neighbours' schedule indices first: the 27 columns are then dead before the
+  // screening loop, which needs the registers for its 27 sums (present bit k <=> col[k] >= 0).
+  __align__(16) I idx[32];
+  uint32_t present;
+  {
+    int32_t col[27];
+    present = neighbours27(cv, d, c, off, col);
+#pragma unroll
+    for (int k = 0; k < 27; ++k) {
+      idx[k] = idx_absent<I>();
+      if (col[k] >= 0) {
+        int g = 4 * (c[2] + k % 3 - 1) + ((c[0] + k / 9 - 1) & 1) + 2 * ((c[1] + (k / 3) % 3 - 1) & 1);
+        idx[k] = I(inv[col[k]] - group_off[g]);
+      }
+    }
+  }
   double acc[27];
 #pragma unroll
   for (int k = 0; k < 27; ++k) acc[k] = 0.0;
@@ -677,19 +695,15 @@ __global__ void __launch_bounds__(128, 4) assemble_sliced_kernel(const int64_t* 
   if (SCREEN) pl = screening_row_same(P, c, d, present, acc, ranges_out ? ranges_out + 8 * i : nullptr);
   const int64_t p = inv[i];
   __align__(16) S v[28];  // written to global memory as 16-byte vectors
-  __align__(16) I idx[32];
 #pragma unroll
   for (int k = 0; k < 27; ++k) {
     v[k] = S(0);
-    idx[k] = idx_absent<I>();
-    if (col[k] >= 0) {
+    if ((present >> k) & 1) {
       const double* x = table + (c[0] * 3 + k / 9) * 2;
       const double* y = table + (c[1] * 3 + (k / 3) % 3) * 2;
       const double* z = table + (c[2] * 3 + k % 3) * 2;
       double stiff = x[1] * y[0] * z[0] + x[0] * y[1] * z[0] + x[0] * y[0] * z[1];
       v[k] = S(T(SCREEN ? stiff + acc[k] : stiff));
-      int g = 4 * (c[2] + k % 3 - 1) + ((c[0] + k / 9 - 1) & 1) + 2 * ((c[1] + (k / 3) % 3 - 1) & 1);
-      idx[k] = I(inv[col[k]] - group_off[g]);
     }
   }
   v[27] = S(0);

@@ -932,43 +932,53 @@ __global__ void __launch_bounds__(256, 5) normal_stencil_reverse_kernel(const in
   for (int ax = 0; ax < 3; ++ax) g_vals[4 * j + ax] = g_vals[4 * j + ax] + T(acc[ax]);
 }
 
-// normal_stencil_reverse_kernel for test functions at the normals' own depth, with the dense
-// column table and a compile-time window W: the test functions whose window holds normal a
-// are w0 + [0, W)^3 with w0 = a - first - W + 1, and the one at window index u along an axis
-// uses table entry ((w0 + u) W + W - 1 - u), so each axis' W entries are loaded once into
-// registers.  Per x the W columns' lower bounds advance in lock step (as in the forward
-// stencil), and a column's test functions in the window become a bit mask over the W z
-// offsets (keys ascend).  Additions in the same (x, y, z) order with the same products as
-// normal_stencil_reverse_kernel: same result.
-template <class T, int W>
-__global__ void __launch_bounds__(256, 3) normal_stencil_reverse_same_kernel(const int64_t* nkeys, int64_t m, int depth,
-                                                                             ColumnView tcv, int64_t toff,
-                                                                             const double* g_test, const double* table,
-                                                                             int first, T* g_vals) {
+// normal_stencil_reverse_kernel with the dense column table and a compile-time window, for
+// test functions at the normals' own depth (W = 4, K = 4) or one depth coarser (CHILD: W = 6,
+// centre 2i, K = 3).  The test functions whose window holds normal a are w0 + [0, K)^3, with
+// w0 = a - first - W + 1 (same depth) or ceil((a - first - W + 1) / 2) (CHILD); the one at
+// window index u along an axis (coordinate i = w0 + u) uses table entry (i W + a - centre(i) -
+// first), so each axis' K entries are loaded once into registers.  Per x the K columns'
+// lower bounds advance in lock step (as in the forward stencil), and a column's test
+// functions in the window become a bit mask over the K z offsets (keys ascend).  Additions in
+// the same (x, y, z) order with the same products as normal_stencil_reverse_kernel: same
+// result.
+template <class T, int W, int K, bool CHILD>
+__global__ void __launch_bounds__(256, 3) normal_stencil_reverse_window_kernel(const int64_t* nkeys, int64_t m,
+                                                                               int test_depth, ColumnView tcv,
+                                                                               int64_t toff, const double* g_test,
+                                                                               const double* table, int first,
+                                                                               T* g_vals) {
   const int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (j >= m) return;
   int a[3];
   key_coords(nkeys[j], a);
-  const int tl = 1 << depth, side = tl + 1;
-  const int w0[3] = {a[0] - first - W + 1, a[1] - first - W + 1, a[2] - first - W + 1};
+  const int tl = 1 << test_depth, side = tl + 1;
+  int w0[3];
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) w0[ax] = CHILD ? (a[ax] - first - W + 2) >> 1 : a[ax] - first - W + 1;
   const int zlo = max(w0[2], 0);
   const double2* tab = reinterpret_cast<const double2*>(table);
-  double2 ty[W], tz[W];
+  // table entry of window index u along axis ax (zero when the coordinate is outside the grid)
+  auto entry = [&](int ax, int u) {
+    const int i = w0[ax] + u;
+    const int off = a[ax] - (CHILD ? 2 * i : i) - first;
+    return i >= 0 && i <= tl ? __ldg(tab + i * W + off) : make_double2(0.0, 0.0);
+  };
+  double2 ty[K], tz[K];
 #pragma unroll
-  for (int u = 0; u < W; ++u) {
-    const int yi = w0[1] + u, zi = w0[2] + u;
-    ty[u] = yi >= 0 && yi <= tl ? __ldg(tab + yi * W + (W - 1 - u)) : make_double2(0.0, 0.0);
-    tz[u] = zi >= 0 && zi <= tl ? __ldg(tab + zi * W + (W - 1 - u)) : make_double2(0.0, 0.0);
+  for (int u = 0; u < K; ++u) {
+    ty[u] = entry(1, u);
+    tz[u] = entry(2, u);
   }
-  const int2* dense = tcv.dense + dense_column_base(depth);
+  const int2* dense = tcv.dense + dense_column_base(test_depth);
   double acc[3] = {0.0, 0.0, 0.0};
-  for (int u = 0; u < W; ++u) {
+  for (int u = 0; u < K; ++u) {
     const int xi = w0[0] + u;
     if (xi < 0 || xi > tl) continue;
-    const double2 tx = __ldg(tab + xi * W + (W - 1 - u));
-    int32_t lo[W], hi[W], end[W];
+    const double2 tx = entry(0, u);
+    int32_t lo[K], hi[K], end[K];
 #pragma unroll
-    for (int v = 0; v < W; ++v) {
+    for (int v = 0; v < K; ++v) {
       const int yi = w0[1] + v;
       lo[v] = 0;
       end[v] = 0;
@@ -984,10 +994,10 @@ __global__ void __launch_bounds__(256, 3) normal_stencil_reverse_same_kernel(con
     for (int step = 0; step < 32; ++step) {
       bool active = false;
 #pragma unroll
-      for (int v = 0; v < W; ++v) active |= lo[v] < hi[v];
+      for (int v = 0; v < K; ++v) active |= lo[v] < hi[v];
       if (!active) break;
 #pragma unroll
-      for (int v = 0; v < W; ++v) {
+      for (int v = 0; v < K; ++v) {
         if (lo[v] < hi[v]) {
           const int32_t mid = (lo[v] + hi[v]) >> 1;
           if (int(__ldg(tcv.keys + mid) & 65535) < zlo)
@@ -998,15 +1008,15 @@ __global__ void __launch_bounds__(256, 3) normal_stencil_reverse_same_kernel(con
       }
     }
 #pragma unroll
-    for (int v = 0; v < W; ++v) {
+    for (int v = 0; v < K; ++v) {
       uint32_t mask = 0;  // bit t: a test function at w0[2] + t
 #pragma unroll
-      for (int e = 0; e < W; ++e) {
-        const int dz = lo[v] + e < end[v] ? int(__ldg(tcv.keys + lo[v] + e) & 65535) - w0[2] : W;
-        if (dz < W) mask |= 1u << dz;
+      for (int e = 0; e < K; ++e) {
+        const int dz = lo[v] + e < end[v] ? int(__ldg(tcv.keys + lo[v] + e) & 65535) - w0[2] : K;
+        if (dz < K) mask |= 1u << dz;
       }
 #pragma unroll
-      for (int t = 0; t < W; ++t) {
+      for (int t = 0; t < K; ++t) {
         if (!((mask >> t) & 1u)) continue;
         const int64_t r = int64_t(lo[v]) + __popc(mask & ((1u << t) - 1u));
         const double g = __ldg(g_test + (r - toff));
@@ -1365,8 +1375,15 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
       PSR_LAUNCH_CHECK();
       // per normal record: key, 3 value adjoints read and written; per test function: its adjoint
       KernelClock clock(kClkNormalStencilReverse, m * (8.0 + 6 * sizeof(T)) + nt * 8.0, double(m), s);
-      if (test_d == normal_d && width == 4 && bcv.dense)
-        normal_stencil_reverse_same_kernel<T, 4><<<blocks_for(m), kThreads, 0, s>>>(
+      // PSR_NORMAL_REVERSE=generic: the generic kernel for every window (test override: the
+      // window kernels must give its result bit for bit)
+      const char* mode = std::getenv("PSR_NORMAL_REVERSE");
+      const bool generic = mode && mode[0] == 'g';
+      if (!generic && test_d == normal_d && width == 4 && first == -2 && bcv.dense)
+        normal_stencil_reverse_window_kernel<T, 4, 4, false><<<blocks_for(m), kThreads, 0, s>>>(
+            nkeys, m, test_d, bcv, level_offsets[test_d], g_test, table.p, first, g_vals);
+      else if (!generic && test_d + 1 == normal_d && width == 6 && first == -3 && bcv.dense)
+        normal_stencil_reverse_window_kernel<T, 6, 3, true><<<blocks_for(m), kThreads, 0, s>>>(
             nkeys, m, test_d, bcv, level_offsets[test_d], g_test, table.p, first, g_vals);
       else
         normal_stencil_reverse_kernel<T><<<blocks_for(m), kThreads, 0, s>>>(
