@@ -933,16 +933,17 @@ __global__ void __launch_bounds__(256, 5) normal_stencil_reverse_kernel(const in
 }
 
 // normal_stencil_reverse_kernel with the dense column table and a compile-time window, for
-// test functions at the normals' own depth (W = 4, K = 4) or one depth coarser (CHILD: W = 6,
-// centre 2i, K = 3).  The test functions whose window holds normal a are w0 + [0, K)^3, with
-// w0 = a - first - W + 1 (same depth) or ceil((a - first - W + 1) / 2) (CHILD); the one at
-// window index u along an axis (coordinate i = w0 + u) uses table entry (i W + a - centre(i) -
-// first), so each axis' K entries are loaded once into registers.  Per x the K columns'
-// lower bounds advance in lock step (as in the forward stencil), and a column's test
-// functions in the window become a bit mask over the K z offsets (keys ascend).  Additions in
-// the same (x, y, z) order with the same products as normal_stencil_reverse_kernel: same
-// result.
-template <class T, int W, int K, bool CHILD>
+// test functions at the normals' own depth (MODE 0: W = 4, K = 4), one depth coarser
+// (MODE 1: W = 6, centre 2i, K = 3) or one depth finer (MODE 2: W = 4, centre i >> 1,
+// K = 8).  The test functions whose window holds normal a are w0 + [0, K)^3, with w0 =
+// a - first - W + 1, ceil((a - first - W + 1) / 2) or 2 (a - first - W + 1); the one at
+// window index u along an axis (coordinate i = w0 + u) uses table entry (i W + a -
+// centre(i) - first), so the K entries along z (and y, for K <= 4) are loaded once into
+// registers.  Per x the K columns' lower bounds advance in lock step (as in the forward
+// stencil), and a column's test functions in the window become a bit mask over the K z
+// offsets (keys ascend).  Additions in the same (x, y, z) order with the same products as
+// normal_stencil_reverse_kernel: same result.
+template <class T, int W, int K, int MODE>
 __global__ void __launch_bounds__(256, 3) normal_stencil_reverse_window_kernel(const int64_t* nkeys, int64_t m,
                                                                                int test_depth, ColumnView tcv,
                                                                                int64_t toff, const double* g_test,
@@ -955,19 +956,21 @@ __global__ void __launch_bounds__(256, 3) normal_stencil_reverse_window_kernel(c
   const int tl = 1 << test_depth, side = tl + 1;
   int w0[3];
 #pragma unroll
-  for (int ax = 0; ax < 3; ++ax) w0[ax] = CHILD ? (a[ax] - first - W + 2) >> 1 : a[ax] - first - W + 1;
+  for (int ax = 0; ax < 3; ++ax)
+    w0[ax] = MODE == 1 ? (a[ax] - first - W + 2) >> 1 : MODE == 2 ? 2 * (a[ax] - first - W + 1) : a[ax] - first - W + 1;
   const int zlo = max(w0[2], 0);
   const double2* tab = reinterpret_cast<const double2*>(table);
   // table entry of window index u along axis ax (zero when the coordinate is outside the grid)
   auto entry = [&](int ax, int u) {
     const int i = w0[ax] + u;
-    const int off = a[ax] - (CHILD ? 2 * i : i) - first;
+    const int off = a[ax] - (MODE == 1 ? 2 * i : MODE == 2 ? i >> 1 : i) - first;
     return i >= 0 && i <= tl ? __ldg(tab + i * W + off) : make_double2(0.0, 0.0);
   };
-  double2 ty[K], tz[K];
+  constexpr int KY = K <= 4 ? K : 1;  // y entries in registers only for narrow windows
+  double2 ty[KY], tz[K];
 #pragma unroll
   for (int u = 0; u < K; ++u) {
-    ty[u] = entry(1, u);
+    if (K <= 4) ty[u < KY ? u : 0] = entry(1, u);
     tz[u] = entry(2, u);
   }
   const int2* dense = tcv.dense + dense_column_base(test_depth);
@@ -1009,6 +1012,7 @@ __global__ void __launch_bounds__(256, 3) normal_stencil_reverse_window_kernel(c
     }
 #pragma unroll
     for (int v = 0; v < K; ++v) {
+      const double2 tyv = K <= 4 ? ty[v < KY ? v : 0] : entry(1, v);
       uint32_t mask = 0;  // bit t: a test function at w0[2] + t
 #pragma unroll
       for (int e = 0; e < K; ++e) {
@@ -1020,9 +1024,9 @@ __global__ void __launch_bounds__(256, 3) normal_stencil_reverse_window_kernel(c
         if (!((mask >> t) & 1u)) continue;
         const int64_t r = int64_t(lo[v]) + __popc(mask & ((1u << t) - 1u));
         const double g = __ldg(g_test + (r - toff));
-        acc[0] += g * tx.y * ty[v].x * tz[t].x;
-        acc[1] += g * tx.x * ty[v].y * tz[t].x;
-        acc[2] += g * tx.x * ty[v].x * tz[t].y;
+        acc[0] += g * tx.y * tyv.x * tz[t].x;
+        acc[1] += g * tx.x * tyv.y * tz[t].x;
+        acc[2] += g * tx.x * tyv.x * tz[t].y;
       }
     }
   }
@@ -1380,10 +1384,13 @@ void solve_backward(void* tape_ptr, const TreeData& tree, const DensityData<T>& 
       const char* mode = std::getenv("PSR_NORMAL_REVERSE");
       const bool generic = mode && mode[0] == 'g';
       if (!generic && test_d == normal_d && width == 4 && first == -2 && bcv.dense)
-        normal_stencil_reverse_window_kernel<T, 4, 4, false><<<blocks_for(m), kThreads, 0, s>>>(
+        normal_stencil_reverse_window_kernel<T, 4, 4, 0><<<blocks_for(m), kThreads, 0, s>>>(
             nkeys, m, test_d, bcv, level_offsets[test_d], g_test, table.p, first, g_vals);
       else if (!generic && test_d + 1 == normal_d && width == 6 && first == -3 && bcv.dense)
-        normal_stencil_reverse_window_kernel<T, 6, 3, true><<<blocks_for(m), kThreads, 0, s>>>(
+        normal_stencil_reverse_window_kernel<T, 6, 3, 1><<<blocks_for(m), kThreads, 0, s>>>(
+            nkeys, m, test_d, bcv, level_offsets[test_d], g_test, table.p, first, g_vals);
+      else if (!generic && test_d == normal_d + 1 && width == 4 && first == -2 && bcv.dense)
+        normal_stencil_reverse_window_kernel<T, 4, 8, 2><<<blocks_for(m), kThreads, 0, s>>>(
             nkeys, m, test_d, bcv, level_offsets[test_d], g_test, table.p, first, g_vals);
       else
         normal_stencil_reverse_kernel<T><<<blocks_for(m), kThreads, 0, s>>>(
