@@ -1612,14 +1612,21 @@ void build_strip_schedule(const int64_t* keys, int64_t rows, int depth, StripSch
   PSR_LAUNCH_CHECK();
   permute_keys_kernel<<<blocks_for(rows), kThreads, 0, s>>>(S.perm.p, rows, keys, S.skeys.p);
   PSR_LAUNCH_CHECK();
-  DBuf<int> gmax(1, s);
-  gmax.zero();
-  max_group_kernel<<<blocks_for(groups), kThreads, 0, s>>>(S.off.p, groups, gmax.p);
-  PSR_LAUNCH_CHECK();
-  // Group-relative neighbour indices fit 16 bits unless a (slice, colour) group is huge.
-  // PSR_INDEX_WIDTH=32 takes the 32-bit rows regardless (test override: the huge-group path
-  // on small levels).
-  S.wide = read_scalar(gmax.p, s) >= 32767;
+  // Group-relative neighbour indices fit 16 bits unless a (slice, colour) group is huge.  A
+  // group holds one x and one y parity of a slice, at most (2^(d-1) + 1)^2 rows (and never
+  // more than the level), so below depth 9 the bound settles it without reading the largest
+  // group back (a host synchronisation).  PSR_INDEX_WIDTH=32 takes the 32-bit rows regardless
+  // (test override: the huge-group path on small levels).
+  const int64_t side = (int64_t(1) << std::max(depth - 1, 0)) + 1;
+  if (std::min<int64_t>(rows, side * side) < 32767) {
+    S.wide = false;
+  } else {
+    DBuf<int> gmax(1, s);
+    gmax.zero();
+    max_group_kernel<<<blocks_for(groups), kThreads, 0, s>>>(S.off.p, groups, gmax.p);
+    PSR_LAUNCH_CHECK();
+    S.wide = read_scalar(gmax.p, s) >= 32767;
+  }
   if (const char* env = std::getenv("PSR_INDEX_WIDTH"))
     if (std::atoi(env) == 32) S.wide = true;
 }
