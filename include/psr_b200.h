@@ -129,7 +129,8 @@ int psr_kernel_launches(int64_t* count);
  * reports, per kernel, the launches, summed device ms, summed algorithmic bytes (what the
  * launch must read and write once) and summed units (rows, row visits, points), then clears
  * the totals.  Up to `capacity` entries are written; *count receives how many kernels have
- * totals. */
+ * totals.  While nobody reads them, at most 4096 launches' events are held: beyond that the
+ * older half is folded into the totals (waiting for those launches). */
 typedef struct psr_kernel_clock {
   const char* kernel;
   const char* unit;

@@ -3,6 +3,7 @@
 #include "../../include/psr_b200.h"
 #include "psr_internal.cuh"
 
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -49,6 +50,25 @@ bool kernel_clocks_on() {
 void kernel_clock_push(int kind, double bytes, double units, cudaEvent_t a, cudaEvent_t b) {
   std::lock_guard<std::mutex> lock(clocks::g_clock_mutex);
   clocks::g_clock_pending.push_back(PendingClock{kind, bytes, units, a, b});
+  // Bound the events held while nobody reads the clocks: fold the older half into the
+  // totals (waiting for those launches; a diagnostic mode only).
+  if (clocks::g_clock_pending.size() >= 4096) {
+    const size_t half = clocks::g_clock_pending.size() / 2;
+    for (size_t i = 0; i < half; ++i) {
+      PendingClock& c = clocks::g_clock_pending[i];
+      float ms = 0;
+      if (cudaEventSynchronize(c.b) == cudaSuccess && cudaEventElapsedTime(&ms, c.a, c.b) == cudaSuccess) {
+        clocks::ClockTotals& t = clocks::g_clock_totals[c.kind];
+        t.launches += 1;
+        t.ms += ms;
+        t.bytes += c.bytes;
+        t.units += c.units;
+      }
+      cudaEventDestroy(c.a);
+      cudaEventDestroy(c.b);
+    }
+    clocks::g_clock_pending.erase(clocks::g_clock_pending.begin(), clocks::g_clock_pending.begin() + half);
+  }
 }
 
 __global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, longlong2* slots, uint64_t mask,
@@ -179,16 +199,17 @@ void validate(const psr_params* p) {
     throw Error(PSR_EINVAL, "precision must be PSR_PRECISION_INPUT or PSR_PRECISION_MIXED");
 }
 
-void tune_pool() {
-  static bool done = false;
-  if (done) return;
+void tune_pool() {  // once per device: each device has its own default pool
+  static std::atomic<uint64_t> done{0};
   int dev = 0;
   PSR_CUDA(cudaGetDevice(&dev));
+  const uint64_t bit = dev < 64 ? uint64_t(1) << dev : 0;
+  if (bit && (done.load() & bit)) return;
   cudaMemPool_t pool;
   PSR_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
   uint64_t threshold = ~uint64_t(0);
   PSR_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
-  done = true;
+  done.fetch_or(bit);
 }
 
 __global__ void upcast_kernel(const float* in, int64_t n, double* out) {

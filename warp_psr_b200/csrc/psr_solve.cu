@@ -6,6 +6,7 @@
 // loads).  Stiffness values come from 1-D hat-integral tables (float64), the point
 // screening is accumulated in float64 per row exactly as screening_stencils.py:34-71, and
 // the result is rounded once to the solve precision.
+#include <atomic>
 #include "psr_internal.cuh"
 
 #include <algorithm>
@@ -1086,13 +1087,16 @@ static void relax_colors(const int32_t* cols, const T* vals, const T* b, T* x, c
   const double visits = double(n) * iters;
   KernelClock clock(kClkBaseRelax, visits * (27.0 * (4 + sizeof(T)) + 3 * sizeof(T) + 4 + (hist ? 2 * sizeof(T) : 0)),
                     visits, s);
-  static bool configured = false;
-  if (!configured) {
+  static std::atomic<uint64_t> configured{0};  // per device: the attribute is set per device
+  int dev = 0;
+  PSR_CUDA(cudaGetDevice(&dev));
+  const uint64_t bit = dev < 64 ? uint64_t(1) << dev : 0;
+  if (!bit || !(configured.load() & bit)) {
     PSR_CUDA(cudaFuncSetAttribute(relax_colors_shared_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(kRelaxSharedBytes)));
     PSR_CUDA(cudaFuncSetAttribute(relax_colors_shared_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(kRelaxSharedBytes)));
-    configured = true;
+    configured.fetch_or(bit);
   }
   if (n > 0 && n < 65535 && staged_bytes <= kRelaxSharedBytes && !force_global && allow_staged) {
     relax_colors_shared_kernel<T, true><<<1, 1024, staged_bytes, s>>>(cols, vals, b, nullptr, nullptr, nullptr, x,
