@@ -1195,10 +1195,7 @@ static bool relax_pipeline(const StripSchedule& S, const T* svals, const I* sidx
                            bool record_increment, RelaxDeferred* defer) {
   const char* mode = std::getenv("PSR_RELAX_KERNEL");
   const bool forced = mode && std::string(mode) == "pipeline";
-  if (!forced) return false;  // opt-in until validated on hardware
-  if (!forced && (std::getenv("PSR_RELAX_STRIPS") || std::getenv("PSR_RELAX_ROW_CAP") ||
-                  std::getenv("PSR_RELAX_FOOTPRINT_LIMIT") || std::getenv("PSR_RELAX_STALL_TEST")))
-    return false;
+  if (!forced) return false;  // opt-in: measured slower than the dynamic scheduler
   const int depth = S.depth, n = 1 << depth, strips = kPipeCtas;
   const int per16 = 16 / int(sizeof(V));
   if (int64_t(iters) * kPipeCtas > device_sms()) return false;
