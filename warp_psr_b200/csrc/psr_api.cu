@@ -88,6 +88,23 @@ __global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, l
   }
 }
 
+__global__ void hash_insert_counted_kernel(const int64_t* __restrict__ src, int64_t n_max, const int32_t* count,
+                                           longlong2* slots, uint64_t mask) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n_max || i >= int64_t(*count)) return;
+  int64_t key = src[i];
+  uint64_t h = HashView::mix(uint64_t(key)) & mask;
+  while (true) {  // the table holds more than twice n_max slots: a free one is always found
+    unsigned long long prev = atomicCAS(reinterpret_cast<unsigned long long*>(&slots[h].x), ~0ULL,
+                                        static_cast<unsigned long long>(key));
+    if (prev == ~0ULL || prev == static_cast<unsigned long long>(key)) {
+      slots[h].y = i;
+      return;
+    }
+    h = (h + 1) & mask;
+  }
+}
+
 // Column heads of sorted keys: (depth, x, y) changes.
 __global__ void column_insert_kernel(const int64_t* __restrict__ keys, int64_t n, longlong2* slots, uint64_t mask) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;

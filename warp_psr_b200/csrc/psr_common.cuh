@@ -191,6 +191,9 @@ struct HashView {
 
 __global__ void hash_insert_kernel(const int64_t* __restrict__ src, int64_t n, longlong2* slots, uint64_t mask,
                                    int32_t value_offset);
+// hash_insert_kernel over the first *count keys (a device count, at most n_max).
+__global__ void hash_insert_counted_kernel(const int64_t* __restrict__ src, int64_t n_max, const int32_t* count,
+                                           longlong2* slots, uint64_t mask);
 
 struct HashMap {
   DBuf<longlong2> slots;
@@ -206,6 +209,21 @@ struct HashMap {
     PSR_CUDA(cudaMemsetAsync(slots.p, 0xff, cap * sizeof(longlong2), s));
     if (n > 0) {
       hash_insert_kernel<<<blocks_for(n), kThreads, 0, s>>>(src, n, slots.p, mask, value_offset);
+      PSR_LAUNCH_CHECK();
+    }
+  }
+  // Build from the first *d_count keys of src, a count known only on the device (at most
+  // n_max): the table is sized for n_max, so the count needs no host read-back.  Key i maps
+  // to i.
+  void build_counted(const int64_t* src, int64_t n_max, const int32_t* d_count, cudaStream_t s) {
+    count = n_max;
+    uint64_t cap = 16;
+    while (cap < uint64_t(2 * n_max + 1)) cap <<= 1;
+    mask = cap - 1;
+    slots.alloc(int64_t(cap), s);
+    PSR_CUDA(cudaMemsetAsync(slots.p, 0xff, cap * sizeof(longlong2), s));
+    if (n_max > 0) {
+      hash_insert_counted_kernel<<<blocks_for(n_max), kThreads, 0, s>>>(src, n_max, d_count, slots.p, mask);
       PSR_LAUNCH_CHECK();
     }
   }

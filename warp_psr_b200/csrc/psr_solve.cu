@@ -1433,22 +1433,24 @@ static PointsData<T> make_points(const DensityData<T>& D, const NormalData<T>& N
     bin_order_points_kernel<T><<<blocks_for(m), kThreads, 0, s>>>(P.ids.p, m, P.pos.p, P.w.p, P.spos.p, P.sw.p);
     PSR_LAUNCH_CHECK();
   }
+  // Unique bins: at most m.  The arrays and the bin hash are sized for m and the hash takes
+  // the count from the device, so the count is never read back (a host synchronisation).
   DBuf<int32_t> heads(m, s), prefix(m, s);
-  int64_t u = 0;
   if (m) {
     bin_heads_kernel<<<blocks_for(m), kThreads, 0, s>>>(sbk.p, m, heads.p);
     PSR_LAUNCH_CHECK();
     inclusive_sum(heads.p, prefix.p, m, s);
-    u = read_scalar(prefix.p + m - 1, s);
   }
-  P.nbins = u;
-  P.bkeys.alloc(u, s);
-  P.bstart.alloc(u + 1, s);
+  P.nbins = m;  // an upper bound; the bins are the first prefix[m - 1] entries
+  P.bkeys.alloc(m, s);
+  P.bstart.alloc(m + 1, s);
   if (m) {
     bin_fill_kernel<<<blocks_for(m + 1), kThreads, 0, s>>>(sbk.p, heads.p, prefix.p, m, d, P.bkeys.p, P.bstart.p);
     PSR_LAUNCH_CHECK();
+    P.bins.build_counted(P.bkeys.p, m, prefix.p + m - 1, s);
+  } else {
+    P.bins.build(P.bkeys.p, 0, s);
   }
-  P.bins.build(P.bkeys.p, u, s);
   return P;
 }
 
