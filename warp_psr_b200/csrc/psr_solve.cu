@@ -916,19 +916,21 @@ __device__ __forceinline__ void gs_row(const int32_t* __restrict__ cols, const T
   if (diagonal != T(0)) st_x(x, row, xi + r * (V(1.0) / V(diagonal)));
 }
 
-// Eight-colour relaxation of a small level by one CTA (relaxation.py:261-271).  With `hist`
-// (adjoint tape) visit `it` of row i stores (old x, r) at hist[2 * (it * n + i)].
+// One colour phase of the base levels' eight-colour relaxation (relaxation.py:261-271), spread
+// over the whole GPU: the rows of colour group g (positions group_off[g] .. group_off[g + 1] of the colour-ordered
+// list), one per thread, x in global memory.  Rows of one colour are never each other's
+// neighbours, so they update independently, exactly as the threads of
+// relax_colors_shared_kernel do between two of its barriers; consecutive launches order the
+// phases.  With `hist` (adjoint tape) visit `it` of row i stores (old x, r) at
+// hist[2 * (it * n + i)].  The grid covers all n rows (a group never has more), threads past the
+// group return at once.
 template <class T>
-__global__ void __launch_bounds__(512) relax_colors_kernel(const int32_t* cols, const T* vals, const T* b, T* x,
-                                                            const int32_t* rows, const int32_t* group_off, int iters,
-                                                            int forward, T* hist = nullptr, int64_t n = 0) {
-  for (int it = 0; it < iters; ++it)
-    for (int cc = 0; cc < 8; ++cc) {
-      int g = forward ? cc : 7 - cc;
-      for (int j = group_off[g] + threadIdx.x; j < group_off[g + 1]; j += blockDim.x)
-        gs_row(cols, vals, b, x, rows[j], hist ? hist + 2 * (int64_t(it) * n + rows[j]) : nullptr);
-      __syncthreads();
-    }
+__global__ void relax_phase_kernel(const int32_t* cols, const T* vals, const T* b, T* x, const int32_t* rows,
+                                   const int32_t* group_off, int g, int it, T* hist, int64_t n) {
+  const int64_t j = group_off[g] + blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (j >= group_off[g + 1]) return;
+  const int32_t row = rows[j];
+  gs_row(cols, vals, b, x, row, hist ? hist + 2 * (int64_t(it) * n + row) : nullptr);
 }
 
 // The same relaxation with x held in shared memory for the whole call (levels whose x fits):
@@ -1108,8 +1110,15 @@ static void relax_colors(const int32_t* cols, const T* vals, const T* b, T* x, c
     PSR_LAUNCH_CHECK();
     relax_colors_shared_kernel<T, false><<<1, 1024, bytes, s>>>(cols, vals, b, vT.p, cT.p, bT.p, x, rows, group_off,
                                                                 iters, forward, hist, n);
-  } else {
-    relax_colors_kernel<T><<<1, 512, 0, s>>>(cols, vals, b, x, rows, group_off, iters, forward, hist, n);
+  } else if (n > 0) {
+    // x does not fit one CTA's shared memory: one launch per colour phase, each spread over
+    // the GPU (a single CTA would pull every row of the level through one SM's L1).
+    for (int it = 0; it < iters; ++it)
+      for (int cc = 0; cc < 8; ++cc) {
+        relax_phase_kernel<T><<<blocks_for(n), kThreads, 0, s>>>(cols, vals, b, x, rows, group_off,
+                                                                 forward ? cc : 7 - cc, it, hist, n);
+        PSR_LAUNCH_CHECK();
+      }
   }
   PSR_LAUNCH_CHECK();
 }
