@@ -133,13 +133,13 @@ __global__ void classify_kernel(const T* __restrict__ pos, const T* __restrict__
   keys[i] = key;
 }
 
-// head[i] = 1 where a new valid segment of `keys >> shift` starts.
-__global__ void heads_kernel(const uint64_t* __restrict__ keys, int64_t n, uint64_t sentinel, int shift,
-                             int32_t* heads) {
+// head[i] = 1 where a new valid segment of `keys >> shift` starts (32- or 64-bit keys).
+template <class K>
+__global__ void heads_kernel(const K* __restrict__ keys, int64_t n, uint64_t sentinel, int shift, int32_t* heads) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
-  uint64_t k = keys[i] >> shift;
-  heads[i] = (keys[i] < sentinel && (i == 0 || (keys[i - 1] >> shift) != k)) ? 1 : 0;
+  const uint64_t k = uint64_t(keys[i]) >> shift;
+  heads[i] = (uint64_t(keys[i]) < sentinel && (i == 0 || (uint64_t(keys[i - 1]) >> shift) != k)) ? 1 : 0;
 }
 
 template <class T>
@@ -203,12 +203,13 @@ __global__ void input_group_kernel(const uint64_t* __restrict__ keys, const int3
 }
 
 // Marks segment heads of sorted keys and returns the number of segments.
-static int64_t segment_heads(const uint64_t* keys, int64_t n, uint64_t sentinel, int shift, DBuf<int32_t>& heads,
+template <class K>
+static int64_t segment_heads(const K* keys, int64_t n, uint64_t sentinel, int shift, DBuf<int32_t>& heads,
                              DBuf<int32_t>& prefix, cudaStream_t s) {
   heads.alloc(n, s);
   prefix.alloc(n, s);
   if (n == 0) return 0;
-  heads_kernel<<<blocks_for(n), kThreads, 0, s>>>(keys, n, sentinel, shift, heads.p);
+  heads_kernel<K><<<blocks_for(n), kThreads, 0, s>>>(keys, n, sentinel, shift, heads.p);
   PSR_LAUNCH_CHECK();
   inclusive_sum(heads.p, prefix.p, n, s);
   return read_scalar(prefix.p + n - 1, s);
@@ -333,9 +334,9 @@ __global__ void morton_kernel(const int64_t* keys, int64_t n, int d, uint64_t* c
 }
 
 // density.py:74-107 — 27 degree-2 splat records per occupied cell, in morton order.
-template <class T>
+template <class T, class K>
 __global__ void density_splat_kernel(const int64_t* keys, const T* values, const int32_t* order, int64_t m, int d,
-                                     T scale, uint64_t* rkeys, int32_t* rids, T* rvals) {
+                                     T scale, K* rkeys, int32_t* rids, T* rvals) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= m) return;
   int64_t j = order[i];
@@ -356,23 +357,23 @@ __global__ void density_splat_kernel(const int64_t* keys, const T* values, const
     int64_t r = 27 * i + k;
     rids[r] = int32_t(r);
     if (dmin(t[0], dmin(t[1], t[2])) >= 0 && dmax(t[0], dmax(t[1], t[2])) < n) {
-      rkeys[r] = (uint64_t(t[0]) << (2 * D)) | (uint64_t(t[1]) << D) | uint64_t(t[2]);
+      rkeys[r] = K((uint64_t(t[0]) << (2 * D)) | (uint64_t(t[1]) << D) | uint64_t(t[2]));
       rvals[r] = T(double(weight) * b[0][x] * b[1][y] * b[2][z]);
     } else {
-      rkeys[r] = sentinel;
+      rkeys[r] = K(sentinel);
       rvals[r] = T(0);
     }
   }
 }
 
-template <class T>
-__global__ void scalar_reduce_kernel(const uint64_t* keys, const int32_t* order, const int32_t* heads,
+template <class T, class K>
+__global__ void scalar_reduce_kernel(const K* keys, const int32_t* order, const int32_t* heads,
                                      const int32_t* prefix, int64_t n, const T* values, int d, int D,
                                      int64_t* out_keys, T* out_values) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n || !heads[i]) return;
   int64_t g = prefix[i] - 1;
-  uint64_t k = keys[i];
+  const K k = keys[i];
   T acc = T(0);
   for (int64_t j = i; j < n && keys[j] == k; ++j) acc = acc + values[order[j]];
   uint64_t mask = (uint64_t(1) << D) - 1;
@@ -447,11 +448,12 @@ __global__ void depths_kernel(const T* dens, int64_t G, int kernel_depth, T targ
 }
 
 // Adjoint bookkeeping: map every sorted record to its segment (unique key) index.
-__global__ void segment_slot_kernel(const int32_t* order, const int32_t* prefix, const uint64_t* skeys, int64_t n,
+template <class K>
+__global__ void segment_slot_kernel(const int32_t* order, const int32_t* prefix, const K* skeys, int64_t n,
                                     uint64_t sentinel, int shift, int32_t* slot) {
   int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (j >= n) return;
-  slot[order[j]] = (skeys[j] >> shift) < (sentinel >> shift) ? prefix[j] - 1 : -1;
+  slot[order[j]] = (uint64_t(skeys[j]) >> shift) < (sentinel >> shift) ? prefix[j] - 1 : -1;
 }
 
 template <class T>
@@ -508,31 +510,45 @@ DensityData<T> build_density(const SampleGroups<T>& g, int depth, int kernel_dep
     PSR_LAUNCH_CHECK();
     sort_pairs(codes.p, scodes.p, ids.p, order.p, m, d > 0 ? 3 * d : 1, s);
     int64_t r = 27 * m;
-    DBuf<uint64_t> rkeys(r, s), skeys(r, s);
     DBuf<int32_t> rids(r, s), rorder(r, s);
     DBuf<T> rvals(r, s);
-    density_splat_kernel<T><<<blocks_for(m), kThreads, 0, s>>>(D.agg_keys[d].p, D.agg_values[d].p, order.p, m, d,
-                                                               D.scale, rkeys.p, rids.p, rvals.p);
-    PSR_LAUNCH_CHECK();
     int Db = d > 0 ? d : 1;
-    sort_pairs(rkeys.p, skeys.p, rids.p, rorder.p, r, 3 * Db + 1, s);
     DBuf<int32_t> heads, prefix;
-    int64_t u = segment_heads(skeys.p, r, uint64_t(1) << (3 * Db), 0, heads, prefix, s);
-    DBuf<int64_t> lkeys(u, s);
-    DBuf<T> lvals(u, s);
-    scalar_reduce_kernel<T><<<blocks_for(r), kThreads, 0, s>>>(skeys.p, rorder.p, heads.p, prefix.p, r, rvals.p, d,
-                                                               Db, lkeys.p, lvals.p);
-    PSR_LAUNCH_CHECK();
+    DBuf<int64_t> lkeys;
+    DBuf<T> lvals;
+    int64_t u = 0;
+    // Record keys of 3 Db + 1 bits: 32-bit keys while they fit (a third less data through the
+    // sort's passes), else 64-bit.  Same keys, same stable order either way.
+    auto splat_reduce = [&](auto key_tag) {
+      using K = decltype(key_tag);
+      DBuf<K> rkeys(r, s), skeys(r, s);
+      density_splat_kernel<T, K><<<blocks_for(m), kThreads, 0, s>>>(D.agg_keys[d].p, D.agg_values[d].p, order.p, m,
+                                                                    d, D.scale, rkeys.p, rids.p, rvals.p);
+      PSR_LAUNCH_CHECK();
+      sort_pairs(rkeys.p, skeys.p, rids.p, rorder.p, r, 3 * Db + 1, s);
+      u = segment_heads(skeys.p, r, uint64_t(1) << (3 * Db), 0, heads, prefix, s);
+      lkeys.alloc(u, s);
+      lvals.alloc(u, s);
+      scalar_reduce_kernel<T, K><<<blocks_for(r), kThreads, 0, s>>>(skeys.p, rorder.p, heads.p, prefix.p, r, rvals.p,
+                                                                    d, Db, lkeys.p, lvals.p);
+      PSR_LAUNCH_CHECK();
+      if (keep) {
+        D.splat_slot[d].alloc(r, s);
+        segment_slot_kernel<<<blocks_for(r), kThreads, 0, s>>>(rorder.p, prefix.p, skeys.p, r,
+                                                               uint64_t(1) << (3 * Db), 0, D.splat_slot[d].p);
+        PSR_LAUNCH_CHECK();
+      }
+    };
+    if (3 * Db + 1 <= 32)
+      splat_reduce(uint32_t());
+    else
+      splat_reduce(uint64_t());
     HashMap hm;
     hm.build(lkeys.p, u, s);
     density_eval_kernel<T><<<blocks_for(G), kThreads, 0, s>>>(hm.view(), lvals.p, g.sums.p, g.weights.p, G, d,
                                                               kernel_depth + 1, dens.p);
     PSR_LAUNCH_CHECK();
     if (keep) {
-      D.splat_slot[d].alloc(r, s);
-      segment_slot_kernel<<<blocks_for(r), kThreads, 0, s>>>(rorder.p, prefix.p, skeys.p, r, uint64_t(1) << (3 * Db),
-                                                             0, D.splat_slot[d].p);
-      PSR_LAUNCH_CHECK();
       D.splat_order[d] = std::move(order);
       D.level_values[d] = std::move(lvals);
       D.level_hash[d] = std::move(hm);
@@ -555,9 +571,9 @@ __global__ void first_keys_kernel(const int32_t* first, int64_t n, uint32_t* key
 
 // normals.py:46-104 — 54 records per group: two 27-node degree-2 splats on the same
 // node `top` (issue #12), weighted by dx and 1-dx.
-template <class T>
+template <class T, class K>
 __global__ void normal_splat_kernel(const int32_t* order, int64_t n, const T* sums, const T* nsums, const T* weights,
-                                    const T* dw, int minimum, int maximum, uint64_t* rkeys, int32_t* rids, T* rvals) {
+                                    const T* dw, int minimum, int maximum, K* rkeys, int32_t* rids, T* rvals) {
   // one thread per record (54 per sample): neighbouring threads write neighbouring records
   const int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (r >= 54 * n) return;
@@ -565,7 +581,7 @@ __global__ void normal_splat_kernel(const int32_t* order, int64_t n, const T* su
   const int k = int(r % 54);
   int D = maximum > 0 ? maximum : 1;
   uint64_t sentinel = uint64_t(1) << (3 * D + 4);
-  rkeys[r] = sentinel;
+  rkeys[r] = K(sentinel);
   rids[r] = int32_t(r);
   int64_t src = order[i];
   T w = weights[src];
@@ -601,20 +617,20 @@ __global__ void normal_splat_kernel(const int32_t* order, int64_t n, const T* su
     if (dmin(t[0], dmin(t[1], t[2])) >= 0 && dmax(t[0], dmax(t[1], t[2])) < nn) {
       T bw = T(b[0][x] * b[1][y] * b[2][z]);
       const int64_t dst = r;
-      rkeys[dst] = (uint64_t(top) << (3 * D)) | (uint64_t(t[0]) << (2 * D)) | (uint64_t(t[1]) << D) | uint64_t(t[2]);
+      rkeys[dst] = K((uint64_t(top) << (3 * D)) | (uint64_t(t[0]) << (2 * D)) | (uint64_t(t[1]) << D) | uint64_t(t[2]));
       for (int a = 0; a < 3; ++a) rvals[3 * dst + a] = nm[a] * sw / (h * h * h) * fraction * bw;
     }
   }
 }
 
-template <class T>
-__global__ void normal_reduce_kernel(const uint64_t* keys, const int32_t* order, const int32_t* heads,
+template <class T, class K>
+__global__ void normal_reduce_kernel(const K* keys, const int32_t* order, const int32_t* heads,
                                      const int32_t* prefix, int64_t n, const T* values, int D, int64_t* out_keys,
                                      T* out_values) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n || !heads[i]) return;
   int64_t g = prefix[i] - 1;
-  uint64_t k = keys[i];
+  const uint64_t k = keys[i];
   T acc[3] = {T(0), T(0), T(0)};
   for (int64_t j = i; j < n && keys[j] == k; ++j) {
     int64_t r = order[j];
@@ -718,27 +734,37 @@ NormalData<T> build_normals(const SampleGroups<T>& g, const DensityData<T>& D, i
   int64_t r = 54 * n;
   int Db = maximum > 0 ? maximum : 1;
   {
-    DBuf<uint64_t> rkeys(r, s), skeys(r, s);
     DBuf<int32_t> rids(r, s), rorder(r, s);
     DBuf<T> rvals(3 * r, s);
-    normal_splat_kernel<T><<<blocks_for(54 * n), kThreads, 0, s>>>(order.p, n, g.sums.p, g.normal_sums.p, g.weights.p,
-                                                              D.dw.p, minimum, maximum, rkeys.p, rids.p, rvals.p);
-    PSR_LAUNCH_CHECK();
-    sort_pairs(rkeys.p, skeys.p, rids.p, rorder.p, r, 3 * Db + 5, s);
-    DBuf<int32_t> heads, prefix;
-    int64_t u = segment_heads(skeys.p, r, uint64_t(1) << (3 * Db + 4), 0, heads, prefix, s);
-    N.count = u;
-    N.keys.alloc(u, s);
-    N.values.alloc(4 * u, s);
-    normal_reduce_kernel<T><<<blocks_for(r), kThreads, 0, s>>>(skeys.p, rorder.p, heads.p, prefix.p, r, rvals.p, Db,
-                                                               N.keys.p, N.values.p);
-    PSR_LAUNCH_CHECK();
-    if (keep) {
-      N.record_slot.alloc(r, s);
-      segment_slot_kernel<<<blocks_for(r), kThreads, 0, s>>>(rorder.p, prefix.p, skeys.p, r,
-                                                             uint64_t(1) << (3 * Db + 4), 0, N.record_slot.p);
+    // Record keys of 3 Db + 5 bits: 32-bit keys up to depth 9 (a third less data through the
+    // sort's passes), else 64-bit.  Same keys, same stable order either way.
+    auto splat_reduce = [&](auto key_tag) {
+      using K = decltype(key_tag);
+      DBuf<K> rkeys(r, s), skeys(r, s);
+      normal_splat_kernel<T, K><<<blocks_for(54 * n), kThreads, 0, s>>>(order.p, n, g.sums.p, g.normal_sums.p,
+                                                                        g.weights.p, D.dw.p, minimum, maximum,
+                                                                        rkeys.p, rids.p, rvals.p);
       PSR_LAUNCH_CHECK();
-    }
+      sort_pairs(rkeys.p, skeys.p, rids.p, rorder.p, r, 3 * Db + 5, s);
+      DBuf<int32_t> heads, prefix;
+      int64_t u = segment_heads(skeys.p, r, uint64_t(1) << (3 * Db + 4), 0, heads, prefix, s);
+      N.count = u;
+      N.keys.alloc(u, s);
+      N.values.alloc(4 * u, s);
+      normal_reduce_kernel<T, K><<<blocks_for(r), kThreads, 0, s>>>(skeys.p, rorder.p, heads.p, prefix.p, r,
+                                                                    rvals.p, Db, N.keys.p, N.values.p);
+      PSR_LAUNCH_CHECK();
+      if (keep) {
+        N.record_slot.alloc(r, s);
+        segment_slot_kernel<<<blocks_for(r), kThreads, 0, s>>>(rorder.p, prefix.p, skeys.p, r,
+                                                               uint64_t(1) << (3 * Db + 4), 0, N.record_slot.p);
+        PSR_LAUNCH_CHECK();
+      }
+    };
+    if (3 * Db + 5 <= 32)
+      splat_reduce(uint32_t());
+    else
+      splat_reduce(uint64_t());
   }
   int64_t chunks = (n + kAverageChunk - 1) / kAverageChunk;
   DBuf<T> partial(3 * chunks, s), contrib(3 * n, s);
