@@ -211,17 +211,24 @@ def run_ours(args, rank, world):
         return summary, P.grad, N.grad
 
     def timed(fn, k):
+        # Python's cyclic garbage collector is run before and paused during the timed steps,
+        # as timeit does: its pauses are the interpreter's, not the step's work.
         total = 0.0
         last = None
-        for _ in range(k):
-            flush.fill_(1)
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            last = fn()
-            b.record(stream)
-            b.synchronize()
-            total += a.elapsed_time(b)
+        gc.collect()
+        gc.disable()
+        try:
+            for _ in range(k):
+                flush.fill_(1)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                last = fn()
+                b.record(stream)
+                b.synchronize()
+                total += a.elapsed_time(b)
+        finally:
+            gc.enable()
         return total / k, last
 
     # The clock sampler (an nvidia-smi process) starts before the warm-up, so that its start
@@ -243,6 +250,7 @@ def run_ours(args, rank, world):
         clocks.__exit__(None, None, None)
     launches = _lib.kernel_launches() - launches0
     bw_stage_ms = {k: round(statistics.mean(b[k] for b in bw_stages), 3) for k in bw_stages[0]} if bw_stages else {}
+    bw_stage_sums = [round(sum(b.values()), 2) for b in bw_stages]  # per timed step: host pauses show as gaps
     fwd_ms = statistics.mean(x[0] for x in split)
     bwd_ms = statistics.mean(x[1] for x in split)
     split_steps = list(split)  # (forward, backward) ms of each timed step
@@ -364,7 +372,8 @@ def run_ours(args, rank, world):
                                "positions and normals",
                    "points": POINTS, "coefficients": result["coefficients"],
                    "basis_counts": result["basis_counts"], "precision": args.precision,
-                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
+                   "python_gc": "collected before and paused during the timed steps, as timeit does"},
         "roofline": {"bound": "hbm", "kernel": f"strip_gs_kernel, finest level (ordered relaxation, depth {CONFIG['depth']})",
                      "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4) if achieved else None, "peak_kind": peak_kind,
@@ -382,7 +391,7 @@ def run_ours(args, rank, world):
                 "d2h_bytes_per_step": int(p_pin.numel() * 4 * 2)},
         "split_ms": {"forward_differentiable": round(fwd_ms, 3), "backward": round(bwd_ms, 3),
                      "adjoint_over_forward": round(bwd_ms / fwd_ms, 3), "forward_plain": round(plain_ms, 3),
-                     "backward_stages": bw_stage_ms,
+                     "backward_stages": bw_stage_ms, "backward_stage_sum_per_step": bw_stage_sums,
                      "per_step": [[round(a, 2), round(b, 2)] for a, b in split_steps]},
         "fp64_step": fp64_step,
         "coefficient_sweeps_per_s": {"step": round(all_visits / (ms / 1e3), 1),
