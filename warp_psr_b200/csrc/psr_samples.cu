@@ -571,11 +571,70 @@ __global__ void first_keys_kernel(const int32_t* first, int64_t n, uint32_t* key
 
 // normals.py:46-104 — 54 records per group: two 27-node degree-2 splats on the same
 // node `top` (issue #12), weighted by dx and 1-dx.
+// The per-group part of the normal splat: the unit normal times the weight, the splat depth
+// and its two fractions, the cell and the 3 x 3 quadratic B-spline weights.
+template <class T>
+struct SplatGroup {
+  T nm[3], dx, h, sw;
+  double b[3][3];
+  int c[3], top, nn, valid, second;
+};
+
+// One thread per record (54 per sample): neighbouring threads write neighbouring records.  A
+// block's records span at most six samples; their per-sample values (two divisions and a
+// square root per component, the B-spline weights) are computed once per sample by the
+// block's first threads into shared memory instead of once per record.  Same arithmetic:
+// same records.
 template <class T, class K>
-__global__ void normal_splat_kernel(const int32_t* order, int64_t n, const T* sums, const T* nsums, const T* weights,
-                                    const T* dw, int minimum, int maximum, K* rkeys, int32_t* rids, T* rvals) {
-  // one thread per record (54 per sample): neighbouring threads write neighbouring records
-  const int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+__global__ void __launch_bounds__(kThreads) normal_splat_kernel(const int32_t* order, int64_t n, const T* sums,
+                                                                const T* nsums, const T* weights, const T* dw,
+                                                                int minimum, int maximum, K* rkeys, int32_t* rids,
+                                                                T* rvals) {
+  constexpr int kGroups = (kThreads + 53) / 54 + 1;  // samples a block's records can touch
+  __shared__ SplatGroup<T> sg[kGroups];
+  const int64_t r0 = blockIdx.x * int64_t(blockDim.x);
+  const int64_t i0 = r0 / 54;
+  if (threadIdx.x < kGroups) {
+    const int64_t i = i0 + threadIdx.x;
+    SplatGroup<T>& G = sg[threadIdx.x];
+    G.valid = 0;
+    if (i < n && i * 54 < r0 + blockDim.x) {
+      int64_t src = order[i];
+      T w = weights[src];
+      T nm[3] = {nsums[3 * src] / w, nsums[3 * src + 1] / w, nsums[3 * src + 2] / w};
+      T length = sqrt(nm[0] * nm[0] + nm[1] * nm[1] + nm[2] * nm[2]);
+      if (length > T(0)) {
+        for (int a = 0; a < 3; ++a) G.nm[a] = nm[a] / length * w;
+        T p[3] = {sums[3 * src] / w, sums[3 * src + 1] / w, sums[3 * src + 2] / w};
+        T depth = dmin(dmax(dw[2 * src], T(minimum)), T(maximum));
+        int top = int(ceil(depth));
+        T dx = T(1.0) - (T(top) - depth);
+        if (top <= minimum) {
+          top = minimum;
+          dx = T(1.0);
+        }
+        if (top > maximum) {
+          top = maximum;
+          dx = T(1.0);
+        }
+        int nn = 1 << top;
+        T h = T(1.0) / T(nn);
+        for (int a = 0; a < 3; ++a) {
+          G.c[a] = ceil_cell(p[a], nn);
+          quadratic(double((p[a] - T(G.c[a]) * h) / h), G.b[a]);
+        }
+        G.top = top;
+        G.nn = nn;
+        G.dx = dx;
+        G.h = h;
+        G.second = fabs(1.0 - double(dx)) > 1e-06;
+        G.sw = dw[2 * src + 1];
+        G.valid = 1;
+      }
+    }
+  }
+  __syncthreads();
+  const int64_t r = r0 + threadIdx.x;
   if (r >= 54 * n) return;
   const int64_t i = r / 54;
   const int k = int(r % 54);
@@ -583,43 +642,18 @@ __global__ void normal_splat_kernel(const int32_t* order, int64_t n, const T* su
   uint64_t sentinel = uint64_t(1) << (3 * D + 4);
   rkeys[r] = K(sentinel);
   rids[r] = int32_t(r);
-  int64_t src = order[i];
-  T w = weights[src];
-  T nm[3] = {nsums[3 * src] / w, nsums[3 * src + 1] / w, nsums[3 * src + 2] / w};
-  T length = sqrt(nm[0] * nm[0] + nm[1] * nm[1] + nm[2] * nm[2]);
-  if (!(length > T(0))) return;
-  for (int a = 0; a < 3; ++a) nm[a] = nm[a] / length * w;
-  T p[3] = {sums[3 * src] / w, sums[3 * src + 1] / w, sums[3 * src + 2] / w};
-  T depth = dmin(dmax(dw[2 * src], T(minimum)), T(maximum));
-  int top = int(ceil(depth));
-  T dx = T(1.0) - (T(top) - depth);
-  if (top <= minimum) {
-    top = minimum;
-    dx = T(1.0);
-  }
-  if (top > maximum) {
-    top = maximum;
-    dx = T(1.0);
-  }
-  int nn = 1 << top;
-  T h = T(1.0) / T(nn);
-  int c[3] = {ceil_cell(p[0], nn), ceil_cell(p[1], nn), ceil_cell(p[2], nn)};
-  double b[3][3];
-  for (int a = 0; a < 3; ++a) quadratic(double((p[a] - T(c[a]) * h) / h), b[a]);
-  bool second = fabs(1.0 - double(dx)) > 1e-06;
-  T sw = dw[2 * src + 1];
-  {
-    if (k >= 27 && !second) return;
-    T fraction = k < 27 ? dx : T(1.0) - dx;
-    int q = k % 27;
-    int x = q / 9, y = q / 3 % 3, z = q % 3;
-    int t[3] = {c[0] + x - 1, c[1] + y - 1, c[2] + z - 1};
-    if (dmin(t[0], dmin(t[1], t[2])) >= 0 && dmax(t[0], dmax(t[1], t[2])) < nn) {
-      T bw = T(b[0][x] * b[1][y] * b[2][z]);
-      const int64_t dst = r;
-      rkeys[dst] = K((uint64_t(top) << (3 * D)) | (uint64_t(t[0]) << (2 * D)) | (uint64_t(t[1]) << D) | uint64_t(t[2]));
-      for (int a = 0; a < 3; ++a) rvals[3 * dst + a] = nm[a] * sw / (h * h * h) * fraction * bw;
-    }
+  const SplatGroup<T>& G = sg[i - i0];
+  if (!G.valid) return;
+  if (k >= 27 && !G.second) return;
+  T fraction = k < 27 ? G.dx : T(1.0) - G.dx;
+  int q = k % 27;
+  int x = q / 9, y = q / 3 % 3, z = q % 3;
+  int t[3] = {G.c[0] + x - 1, G.c[1] + y - 1, G.c[2] + z - 1};
+  if (dmin(t[0], dmin(t[1], t[2])) >= 0 && dmax(t[0], dmax(t[1], t[2])) < G.nn) {
+    T bw = T(G.b[0][x] * G.b[1][y] * G.b[2][z]);
+    const T h = G.h;
+    rkeys[r] = K((uint64_t(G.top) << (3 * D)) | (uint64_t(t[0]) << (2 * D)) | (uint64_t(t[1]) << D) | uint64_t(t[2]));
+    for (int a = 0; a < 3; ++a) rvals[3 * r + a] = G.nm[a] * G.sw / (h * h * h) * fraction * bw;
   }
 }
 
