@@ -219,6 +219,7 @@ def run_ours(args, rank, world):
         gc.disable()
         try:
             for _ in range(k):
+                last = None  # the previous step's outputs are released before the next step
                 flush.fill_(1)
                 a = torch.cuda.Event(enable_timing=True)
                 b = torch.cuda.Event(enable_timing=True)
