@@ -63,3 +63,14 @@ def test_cpu_tensors_are_rejected():
     p = torch.rand((16, 3))
     with pytest.raises(ValueError, match="CUDA device"):
         reconstruct(p, p, depth=4, full_depth=2)
+
+
+def test_kernel_clocks_without_pending_launches_need_no_device():
+    """With no clocked launch pending, psr_kernel_clocks reports no kernels and makes no CUDA
+    call; the struct it fills matches the header's field order."""
+    from warp_psr_b200 import _lib
+    assert _lib.kernel_clocks() == []
+    names = [f[0] for f in _lib.KernelClock._fields_]
+    header = (ROOT / "include" / "psr_b200.h").read_text()
+    body = header[header.index("typedef struct psr_kernel_clock {"):header.index("} psr_kernel_clock;")]
+    assert names == re.findall(r"\b(\w+);", body)
